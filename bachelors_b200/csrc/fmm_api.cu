@@ -1,0 +1,456 @@
+// C ABI of libfmmcuda.so (declared in include/fmmcuda.h): plan lifetime, input staging,
+// phase sequencing, timing and error reporting.
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "fmm_internal.cuh"
+
+namespace fmm {
+
+// addingKernel (FMMCUDADLL/kernels.cuh:6-11): c = a + b
+__global__ void kAdd(const float* a, const float* b, float* c, int64_t n)
+{
+   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+   if(i < n) c[i] = a[i] + b[i];
+}
+
+fmm_status directFp64Subset(Plan& P, double current, const double* tgtDev, int k, double* outDev, cudaStream_t st);
+
+namespace {
+thread_local std::string g_lastError;
+}
+
+fmm_status setError(fmm_status s, const char* fmt, ...)
+{
+   char buf[1024];
+   va_list ap;
+   va_start(ap, fmt);
+   vsnprintf(buf, sizeof(buf), fmt, ap);
+   va_end(ap);
+   g_lastError = buf;
+   return s;
+}
+
+fmm_status Plan::ensureNodes(int64_t cap, cudaStream_t st)
+{
+   if(cap <= nodeCap) return FMM_OK;
+   // grow every per-node array, keeping the contents
+   const size_t es[12] = {8, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4};
+   for(int b = 0; b < 12; b++)
+   {
+      DevBuf nb;
+      FMM_TRY(nb.reserve(es[b] * cap));
+      if(nodeBufs[b].ptr && nodeCap > 0)
+         FMM_CUDA(cudaMemcpyAsync(nb.ptr, nodeBufs[b].ptr, es[b] * nodeCap, cudaMemcpyDeviceToDevice, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+      nodeBufs[b].release();
+      nodeBufs[b] = nb;
+   }
+   nodeCap = cap;
+   tree.key = (uint64_t*)nodeBufs[0].ptr;
+   tree.level = (int*)nodeBufs[1].ptr;
+   tree.ix = (int*)nodeBufs[2].ptr;
+   tree.iy = (int*)nodeBufs[3].ptr;
+   tree.iz = (int*)nodeBufs[4].ptr;
+   tree.s0 = (int*)nodeBufs[5].ptr;
+   tree.s1 = (int*)nodeBufs[6].ptr;
+   tree.t0 = (int*)nodeBufs[7].ptr;
+   tree.t1 = (int*)nodeBufs[8].ptr;
+   tree.parent = (int*)nodeBufs[9].ptr;
+   tree.child0 = (int*)nodeBufs[10].ptr;
+   tree.nchild = (int*)nodeBufs[11].ptr;
+   return FMM_OK;
+}
+
+fmm_status Plan::ensureLists(int64_t cap)
+{
+   if(cap <= listCap) return FMM_OK;
+   const size_t per[8] = {COLCAP, 1, ACAP, 1, XCAP, 1, 316, 1};
+   for(int b = 0; b < 8; b++) FMM_TRY(listBufs[b].reserve(sizeof(int) * per[b] * cap));
+   listCap = cap;
+   lists.col = (int*)listBufs[0].ptr;
+   lists.ncol = (int*)listBufs[1].ptr;
+   lists.acoarse = (int*)listBufs[2].ptr;
+   lists.na = (int*)listBufs[3].ptr;
+   lists.xl = (int*)listBufs[4].ptr;
+   lists.nx = (int*)listBufs[5].ptr;
+   lists.vtab = (int*)listBufs[6].ptr;
+   lists.nv = (int*)listBufs[7].ptr;
+   return FMM_OK;
+}
+
+}  // namespace fmm
+
+using namespace fmm;
+
+struct fmm_plan
+{
+   Plan P;
+};
+
+namespace {
+
+struct DeviceGuard
+{
+   int prev = -1;
+   explicit DeviceGuard(int dev)
+   {
+      cudaGetDevice(&prev);
+      if(prev != dev) cudaSetDevice(dev);
+   }
+   ~DeviceGuard()
+   {
+      int cur = -1;
+      cudaGetDevice(&cur);
+      if(prev >= 0 && cur != prev) cudaSetDevice(prev);
+   }
+};
+
+fmm_status copyIn(DevBuf& buf, const void* src, size_t bytes, int onDevice, cudaStream_t st, void** out)
+{
+   FMM_TRY(buf.reserve(bytes));
+   if(bytes) FMM_CUDA(cudaMemcpyAsync(buf.ptr, src, bytes, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+   *out = buf.ptr;
+   return FMM_OK;
+}
+
+fmm_status copyOut(void* dst, const DevBuf& buf, size_t bytes, int onDevice, cudaStream_t st)
+{
+   if(!dst || !bytes) return FMM_OK;
+   FMM_CUDA(cudaMemcpyAsync(dst, buf.ptr, bytes, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+   if(!onDevice) FMM_CUDA(cudaStreamSynchronize(st));
+   return FMM_OK;
+}
+
+double elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+   float ms = 0;
+   if(cudaEventElapsedTime(&ms, a, b) != cudaSuccess) { cudaGetLastError(); return 0; }
+   return ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fmm_version(void) { return "bachelors_b200 fmmcuda 0.1 (sm_100a)"; }
+
+const char* fmm_last_error_string(void) { return g_lastError.c_str(); }
+
+void fmm_default_config(fmm_config* cfg)
+{
+   if(!cfg) return;
+   std::memset(cfg, 0, sizeof(*cfg));
+   cfg->order = 10;
+   cfg->leaf_capacity = 64;
+   cfg->precision = FMM_FP32;
+   cfg->m2l_mode = FMM_M2L_SIMT;
+   cfg->m2l_truncate = 0;
+   cfg->device = 0;
+   cfg->root_half_width = 0;
+}
+
+fmm_status fmm_plan_create(const fmm_config* cfg, fmm_plan** plan)
+{
+   if(!cfg || !plan) return setError(FMM_E_INVALID, "fmm_plan_create: null argument");
+   *plan = nullptr;
+   if(cfg->order < 1 || cfg->order > MAXORDER)
+      return setError(FMM_E_INVALID, "order %d outside 1..%d", cfg->order, MAXORDER);
+   if(cfg->leaf_capacity < 1) return setError(FMM_E_INVALID, "leaf_capacity must be >= 1");
+   if(cfg->precision != FMM_FP32 && cfg->precision != FMM_FP64)
+      return setError(FMM_E_INVALID, "unknown precision %d", cfg->precision);
+   if(cfg->m2l_mode < FMM_M2L_SIMT || cfg->m2l_mode > FMM_M2L_TF32)
+      return setError(FMM_E_INVALID, "unknown m2l_mode %d", cfg->m2l_mode);
+   int ndev = 0;
+   cudaError_t e = cudaGetDeviceCount(&ndev);
+   if(e != cudaSuccess || ndev == 0)
+   {
+      cudaGetLastError();
+      return setError(FMM_E_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+   }
+   if(cfg->device < 0 || cfg->device >= ndev) return setError(FMM_E_INVALID, "device %d out of range", cfg->device);
+   DeviceGuard g(cfg->device);
+   fmm_plan* h = new fmm_plan();
+   Plan& P = h->P;
+   P.cfg = *cfg;
+   P.p = cfg->order;
+   P.L = nharm(P.p);
+   P.Lp = padded(P.L);
+   P.fp64 = cfg->precision == FMM_FP64;
+   fmm_status s = P.rootb.reserve(sizeof(RootBox));
+   if(s == FMM_OK) s = P.errb.reserve(sizeof(int));
+   if(s != FMM_OK) { delete h; return s; }
+   if(s == FMM_OK) s = initOffsetTables();
+   if(s != FMM_OK) { delete h; return s; }
+   P.root = (RootBox*)P.rootb.ptr;
+   P.err = (int*)P.errb.ptr;
+   for(int i = 0; i < 8; i++) cudaEventCreate(&P.ev[i]);
+   P.eventsMade = true;
+   *plan = h;
+   return FMM_OK;
+}
+
+fmm_status fmm_plan_destroy(fmm_plan* plan)
+{
+   if(!plan) return FMM_OK;
+   Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   DevBuf* bufs[] = {&P.srcXYZb, &P.srcWb, &P.srcJb, &P.tgtXYZb, &P.rootb, &P.sKeys, &P.tKeys, &P.sIdx, &P.tIdx,
+                     &P.sPos, &P.sQ, &P.tPos, &P.cubTmp, &P.scratch, &P.lvlBounds, &P.lvlCnt, &P.lvlOff,
+                     &P.p2pOff, &P.p2pList, &P.errb, &P.mult, &P.local, &P.outB, &P.outA, &P.opM2M64,
+                     &P.opL2L64, &P.opM2L64, &P.opM2Mw, &P.opL2Lw, &P.opM2Lw, &P.opM2Lbf};
+   for(DevBuf* b : bufs) b->release();
+   for(auto& b : P.nodeBufs) b.release();
+   for(auto& b : P.listBufs) b.release();
+   if(P.eventsMade)
+      for(int i = 0; i < 8; i++) cudaEventDestroy(P.ev[i]);
+   delete plan;
+   return FMM_OK;
+}
+
+fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const void* J, int64_t n, int on_device,
+                           void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   if(n < 0 || n > (int64_t(1) << 31) - 1) return setError(FMM_E_INVALID, "source count %lld out of range", (long long)n);
+   if(n > 0 && (!xyz || !w)) return setError(FMM_E_INVALID, "null source coordinates or weights");
+   Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_TRY(copyIn(P.srcXYZb, xyz, es * 3 * n, on_device, st, &P.srcXYZ));
+   FMM_TRY(copyIn(P.srcWb, w, es * n, on_device, st, &P.srcW));
+   P.hasJ = J != nullptr;
+   if(P.hasJ) FMM_TRY(copyIn(P.srcJb, J, es * 3 * n, on_device, st, &P.srcJ));
+   if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
+   P.n = n;
+   P.treeReady = P.upReady = P.downReady = false;
+   return FMM_OK;
+}
+
+fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_device, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   if(m < 0 || m > (int64_t(1) << 31) - 1) return setError(FMM_E_INVALID, "target count %lld out of range", (long long)m);
+   if(m > 0 && !xyz) return setError(FMM_E_INVALID, "null target coordinates");
+   Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_TRY(copyIn(P.tgtXYZb, xyz, es * 3 * m, on_device, st, &P.tgtXYZ));
+   if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
+   P.m = m;
+   P.treeReady = P.upReady = P.downReady = false;
+   return FMM_OK;
+}
+
+fmm_status fmm_build_tree(fmm_plan* plan, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(P.n + P.m == 0) return setError(FMM_E_INVALID, "no sources or targets set");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   cudaEventRecord(P.ev[0], st);
+   FMM_TRY(P.fp64 ? buildTreeT<double>(P, st) : buildTreeT<float>(P, st));
+   cudaEventRecord(P.ev[1], st);
+   P.treeReady = true;
+   P.upReady = P.downReady = false;
+   return FMM_OK;
+}
+
+fmm_status fmm_upward(fmm_plan* plan, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!P.treeReady) return setError(FMM_E_INVALID, "fmm_upward: tree not built");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.fp64 ? upwardT<double>(P, st) : upwardT<float>(P, st));
+   cudaEventRecord(P.ev[2], st);
+   P.upReady = true;
+   P.downReady = false;
+   return FMM_OK;
+}
+
+fmm_status fmm_downward(fmm_plan* plan, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!P.upReady) return setError(FMM_E_INVALID, "fmm_downward: multipoles are not ready");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.fp64 ? downwardT<double>(P, st) : downwardT<float>(P, st));
+   cudaEventRecord(P.ev[4], st);
+   P.downReady = true;
+   return FMM_OK;
+}
+
+fmm_status fmm_evaluate(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device,
+                        void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!P.downReady) return setError(FMM_E_INVALID, "fmm_evaluate: local expansions are not ready");
+   if(want < 1 || want > 3) return setError(FMM_E_INVALID, "want must be 1, 2 or 3");
+   if(((want & 1) && !out_B) || ((want & 2) && !out_A)) return setError(FMM_E_INVALID, "null output buffer");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   size_t bytes = es * 3 * std::max<int64_t>(P.m, 1);
+   bool directB = on_device && (want & 1);
+   bool directA = on_device && (want & 2);
+   // write straight into device outputs; stage host outputs through plan buffers
+   DevBuf ob, oa;
+   if(directB) { ob.ptr = out_B; ob.bytes = bytes; }
+   else if(want & 1) { FMM_TRY(P.outB.reserve(bytes)); ob = P.outB; }
+   if(directA) { oa.ptr = out_A; oa.bytes = bytes; }
+   else if(want & 2) { FMM_TRY(P.outA.reserve(bytes)); oa = P.outA; }
+   DevBuf saveB = P.outB, saveA = P.outA;
+   P.outB = ob;
+   P.outA = oa;
+   fmm_status s = P.fp64 ? evaluateT<double>(P, current, want, st) : evaluateT<float>(P, current, want, st);
+   P.outB = saveB;
+   P.outA = saveA;
+   FMM_TRY(s);
+   cudaEventRecord(P.ev[5], st);
+   if(!on_device)
+   {
+      if(want & 1) FMM_TRY(copyOut(out_B, P.outB, es * 3 * P.m, 0, st));
+      if(want & 2) FMM_TRY(copyOut(out_A, P.outA, es * 3 * P.m, 0, st));
+   }
+   return FMM_OK;
+}
+
+fmm_status fmm_solve(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device, void* stream)
+{
+   FMM_TRY(fmm_build_tree(plan, stream));
+   FMM_TRY(fmm_upward(plan, stream));
+   FMM_TRY(fmm_downward(plan, stream));
+   FMM_TRY(fmm_evaluate(plan, current, want, out_B, out_A, on_device, stream));
+   return FMM_OK;
+}
+
+fmm_status fmm_direct(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(want < 1 || want > 3) return setError(FMM_E_INVALID, "want must be 1, 2 or 3");
+   if(((want & 1) && !out_B) || ((want & 2) && !out_A)) return setError(FMM_E_INVALID, "null output buffer");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   if(!P.treeReady) FMM_TRY(fmm_build_tree(plan, stream));
+   size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   size_t bytes = es * 3 * std::max<int64_t>(P.m, 1);
+   FMM_TRY(P.outB.reserve(bytes));
+   FMM_TRY(P.outA.reserve(bytes));
+   FMM_TRY(P.fp64 ? directT<double>(P, current, want, st) : directT<float>(P, current, want, st));
+   if(want & 1) FMM_TRY(copyOut(out_B, P.outB, es * 3 * P.m, on_device, st));
+   if(want & 2) FMM_TRY(copyOut(out_A, P.outA, es * 3 * P.m, on_device, st));
+   return FMM_OK;
+}
+
+fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* tgt, int64_t k, double* out_B)
+{
+   if(!plan || (k > 0 && (!tgt || !out_B))) return setError(FMM_E_INVALID, "null argument");
+   Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = 0;
+   if(!P.treeReady) FMM_TRY(fmm_build_tree(plan, nullptr));
+   DevBuf t, o;
+   FMM_TRY(t.reserve(sizeof(double) * 3 * std::max<int64_t>(k, 1)));
+   fmm_status s = o.reserve(sizeof(double) * 3 * std::max<int64_t>(k, 1));
+   if(s != FMM_OK) { t.release(); return s; }
+   cudaMemcpyAsync(t.ptr, tgt, sizeof(double) * 3 * k, cudaMemcpyHostToDevice, st);
+   s = directFp64Subset(P, current, (const double*)t.ptr, int(k), (double*)o.ptr, st);
+   if(s == FMM_OK)
+   {
+      cudaError_t e = cudaMemcpyAsync(out_B, o.ptr, sizeof(double) * 3 * k, cudaMemcpyDeviceToHost, st);
+      if(e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if(e != cudaSuccess) s = setError(FMM_E_CUDA, "fmm_direct_fp64_subset: %s", cudaGetErrorString(e));
+   }
+   t.release();
+   o.release();
+   return s;
+}
+
+fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats)
+{
+   if(!plan || !stats) return setError(FMM_E_INVALID, "null argument");
+   const Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   fmm_stats s{};
+   s.ms_tree = elapsed(P.ev[0], P.ev[1]);
+   s.ms_upward = elapsed(P.ev[1], P.ev[2]);
+   s.ms_m2l = elapsed(P.ev[2], P.ev[3]);
+   s.ms_downward = elapsed(P.ev[2], P.ev[4]);
+   s.ms_near = elapsed(P.ev[4], P.ev[5]);
+   s.ms_total = elapsed(P.ev[0], P.ev[5]);
+   s.nodes = P.tree.nNodes;
+   s.levels = P.tree.nLevels;
+   s.p2p_pairs = P.nP2P;
+   s.v_pairs = P.nV;
+   s.n_sources = P.n;
+   s.n_targets = P.m;
+   *stats = s;
+   return FMM_OK;
+}
+
+fmm_status fmm_get_operator(fmm_plan* plan, int kind, int index, double* out)
+{
+   if(!plan || !out) return setError(FMM_E_INVALID, "null argument");
+   Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   if(kind < 0 || kind > 2) return setError(FMM_E_INVALID, "kind must be 0, 1 or 2");
+   const int L = P.L;
+   int slot = index;
+   if(kind == 2)
+   {
+      int ox = index % 7 - 3, oy = (index / 7) % 7 - 3, oz = index / 49 - 3;
+      if(index < 0 || index >= NOFF || (abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1))
+         return setError(FMM_E_INVALID, "offset index %d is not an M2L offset", index);
+      int k = 0;
+      for(int o = 0; o < index; o++)
+      {
+         int ax = o % 7 - 3, ay = (o / 7) % 7 - 3, az = o / 49 - 3;
+         if(!(abs(ax) <= 1 && abs(ay) <= 1 && abs(az) <= 1)) k++;
+      }
+      slot = k;
+   }
+   else if(index < 0 || index > 7) return setError(FMM_E_INVALID, "octant must be 0..7");
+   FMM_TRY(buildOperators(P, 0));
+   const DevBuf& b = kind == 0 ? P.opM2M64 : kind == 1 ? P.opL2L64 : P.opM2L64;
+   FMM_CUDA(cudaMemcpy(out, (const double*)b.ptr + int64_t(slot) * L * L, sizeof(double) * L * L,
+                       cudaMemcpyDeviceToHost));
+   return FMM_OK;
+}
+
+
+fmm_status fmm_add_vectors(const float* a, const float* b, float* c, int64_t n)
+{
+   if(n < 0 || (n > 0 && (!a || !b || !c))) return setError(FMM_E_INVALID, "fmm_add_vectors: bad arguments");
+   if(n == 0) return FMM_OK;
+   DevBuf da, db, dc;
+   fmm_status s = da.reserve(sizeof(float) * n);
+   if(s == FMM_OK) s = db.reserve(sizeof(float) * n);
+   if(s == FMM_OK) s = dc.reserve(sizeof(float) * n);
+   if(s == FMM_OK)
+   {
+      cudaError_t e = cudaMemcpy(da.ptr, a, sizeof(float) * n, cudaMemcpyHostToDevice);
+      if(e == cudaSuccess) e = cudaMemcpy(db.ptr, b, sizeof(float) * n, cudaMemcpyHostToDevice);
+      if(e == cudaSuccess)
+      {
+         kAdd<<<int((n + 255) / 256), 256>>>((const float*)da.ptr, (const float*)db.ptr, (float*)dc.ptr, n);
+         e = cudaGetLastError();
+      }
+      if(e == cudaSuccess) e = cudaMemcpy(c, dc.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost);
+      if(e != cudaSuccess) s = setError(FMM_E_CUDA, "fmm_add_vectors: %s", cudaGetErrorString(e));
+   }
+   da.release();
+   db.release();
+   dc.release();
+   return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// Host-side plan state and error plumbing shared by the library's translation units.
+#pragma once
+#include <algorithm>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "../../include/fmmcuda.h"
+#include "fmm_common.cuh"
+
+namespace fmm {
+
+fmm_status setError(fmm_status s, const char* fmt, ...);
+
+#define FMM_TRY(expr)                                   \
+   do                                                   \
+   {                                                    \
+      fmm_status _s = (expr);                           \
+      if(_s != FMM_OK) return _s;                       \
+   } while(0)
+
+#define FMM_CUDA(expr)                                                                          \
+   do                                                                                           \
+   {                                                                                            \
+      cudaError_t _e = (expr);                                                                  \
+      if(_e != cudaSuccess)                                                                     \
+         return ::fmm::setError(_e == cudaErrorMemoryAllocation ? FMM_E_OOM : FMM_E_CUDA,        \
+                                "%s:%d %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(_e)); \
+   } while(0)
+
+#define FMM_CHECK_LAUNCH() FMM_CUDA(cudaGetLastError())
+
+// device error flags set by list builders and bounded waits
+enum : int {
+   ERR_LIST_A = 1,
+   ERR_LIST_X = 2,
+   ERR_LIST_COL = 4,
+   ERR_LIST_V = 8,
+   ERR_DFS = 16,
+   ERR_TIMEOUT = 32,
+};
+
+extern __constant__ int d_m2lIndex[NOFF];   // offset index (0..342) -> M2L slot (0..315) or -1
+extern __constant__ int d_m2lOffset[316];   // M2L slot -> offset index
+
+// A growable device allocation.
+struct DevBuf
+{
+   void* ptr = nullptr;
+   size_t bytes = 0;
+   fmm_status reserve(size_t want)
+   {
+      if(want <= bytes) return FMM_OK;
+      if(ptr) cudaFree(ptr);
+      ptr = nullptr;
+      bytes = 0;
+      size_t b = std::max<size_t>(want, 256);
+      cudaError_t e = cudaMalloc(&ptr, b);
+      if(e != cudaSuccess)
+      {
+         cudaGetLastError();
+         return setError(FMM_E_OOM, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+      }
+      bytes = b;
+      return FMM_OK;
+   }
+   void release()
+   {
+      if(ptr) cudaFree(ptr);
+      ptr = nullptr;
+      bytes = 0;
+   }
+};
+
+struct RootBox
+{
+   double center[3];
+   double H;
+   double lo[3];
+   double scale;
+};
+
+struct Lists
+{
+   int* col;      // [node][COLCAP]
+   int* ncol;
+   int* acoarse;  // [node][ACAP]
+   int* na;
+   int* xl;       // [node][XCAP]
+   int* nx;
+   int* vtab;     // [node][316], source node or -1
+   int* nv;
+};
+
+struct Plan
+{
+   fmm_config cfg;
+   int p = 0, L = 0, Lp = 0;
+   bool fp64 = false;
+   // inputs (device copies, element type float or double)
+   DevBuf srcXYZb, srcWb, srcJb, tgtXYZb;
+   void* srcXYZ = nullptr; void* srcW = nullptr; void* srcJ = nullptr; void* tgtXYZ = nullptr;
+   bool hasJ = false;
+   int64_t n = 0, m = 0;
+   // tree
+   RootBox* root = nullptr;
+   DevBuf rootb, sKeys, tKeys, sIdx, tIdx, sPos, sQ, tPos, cubTmp, scratch, lvlBounds, lvlCnt, lvlOff;
+   DevBuf nodeBufs[12];
+   int64_t nodeCap = 0;
+   Tree tree{};
+   DevBuf listBufs[8];
+   int64_t listCap = 0;
+   Lists lists{};
+   DevBuf p2pOff, p2pList;
+   int nP2P = 0;
+   int64_t nV = 0;
+   int* err = nullptr;
+   DevBuf errb;
+   // expansions [node][3][Lp] and outputs
+   DevBuf mult, local, outB, outA;
+   // operator tables (scaled basis): FP64 masters and the working-precision copies
+   DevBuf opM2M64, opL2L64, opM2L64;     // [8][L][L], [8][L][L], [316][L][L] FP64 row-major
+   DevBuf opM2Mw, opL2Lw, opM2Lw;        // transposed working copies, see fmm_kernels.cu
+   DevBuf opM2Lbf;                       // bf16 hi/lo split for the tensor-core M2L
+   int opOrder = -1;
+   // state
+   bool treeReady = false, upReady = false, downReady = false;
+   fmm_stats stats{};
+   cudaEvent_t ev[8];
+   bool eventsMade = false;
+
+   fmm_status ensureNodes(int64_t cap, cudaStream_t st = 0);
+   fmm_status ensureLists(int64_t cap);
+};
+
+template <class T> fmm_status buildTreeT(Plan& P, cudaStream_t st);
+template <class T> fmm_status upwardT(Plan& P, cudaStream_t st);
+template <class T> fmm_status downwardT(Plan& P, cudaStream_t st);
+template <class T> fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st);
+template <class T> fmm_status directT(Plan& P, double current, int want, cudaStream_t st);
+fmm_status buildOperators(Plan& P, cudaStream_t st);
+fmm_status initOffsetTables();
+fmm_status m2lTensorCore(Plan& P, cudaStream_t st);
+
+}  // namespace fmm

@@ -1,0 +1,789 @@
+// FMM kernels for sm_100a: translation-operator tables (FP64), P2M, M2M, M2L (CUDA-core
+// form), L2L, and the fused L2P + direct near field.
+//
+// Every expansion is stored box-size scaled: a node of side h keeps M~_l = M_l / h^l and
+// L~_l = L_l h^(l+1). With that scaling the M2M, L2L and M2L operators do not depend on the
+// level: 8 M2M and 8 L2L operators (one per child octant) and 316 M2L operators (one per
+// offset o in [-3,3]^3 outside [-1,1]^3), all built once per order in FP64.
+//
+// Reference counterparts (FMM/FMMGPU/):
+//   P2M   math::calcIntegralContribution                     integration.cpp:137-161
+//   M2M   MultipoleTranslator::translateMultipoleWithComplex  multipole_translator.cpp:3-32,111-125,143-146
+//   M2L   multipoleToLocalWithComplex (l + lambda <= p)       multipole_translator.cpp:148-199
+//   L2L   translateLocalWithComplex                          multipole_translator.cpp:201-255
+//   L2P   CalculationPointOctreeNode::calcA / calcRot        calculation_point_octree.cpp:192-275
+//         (B from analytic gradients here, finite differences there)
+//   near  bioSavartLaplaceFunction                           integration.cpp:113-120
+#include <cuda_bf16.h>
+
+#include "fmm_internal.cuh"
+
+namespace fmm {
+
+__constant__ int d_m2lIndex[NOFF];
+__constant__ int d_m2lOffset[316];
+
+// Constant memory is per device context: fill it once on every device that uses the library.
+fmm_status initOffsetTables()
+{
+   static bool done[64] = {false};
+   int dev = 0;
+   FMM_CUDA(cudaGetDevice(&dev));
+   if(dev < 64 && done[dev]) return FMM_OK;
+   int idx[NOFF], off[316];
+   int k = 0;
+   for(int oz = -3; oz <= 3; oz++)
+      for(int oy = -3; oy <= 3; oy++)
+         for(int ox = -3; ox <= 3; ox++)
+         {
+            int o = offsetIndex(ox, oy, oz);
+            if(abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1) idx[o] = -1;
+            else { idx[o] = k; off[k] = o; k++; }
+         }
+   FMM_CUDA(cudaMemcpyToSymbol(d_m2lIndex, idx, sizeof(idx)));
+   FMM_CUDA(cudaMemcpyToSymbol(d_m2lOffset, off, sizeof(off)));
+   if(dev < 64) done[dev] = true;
+   return FMM_OK;
+}
+
+// ====================================================================================
+// Operator tables. Entry (i, j) of a translation in the real basis, derived from the
+// reference's complex form res(l,m) = sum a(lambda,mu) G(l,m,lambda,mu) between the
+// realToComplex / complexToReal conversions (harmonics.cpp:340-379), with exact 1/sqrt2.
+// ====================================================================================
+struct C2 { double re, im; };
+
+__device__ inline C2 cplxOf(const double* H, int n, int k)
+{
+   const double s = 0.70710678118654752440;
+   if(k == 0) return {H[hidx(n, 0)], 0.0};
+   int a = abs(k);
+   return {s * H[hidx(n, a)], (k > 0 ? s : -s) * H[hidx(n, -a)]};
+}
+
+__device__ inline double signPow(int t) { int e = (-t) / 2; return (e & 1) ? -1.0 : 1.0; }
+
+// kind 0 = M2M, 1 = L2L, 2 = M2L. H = real harmonics of the translation (regular for
+// M2M / L2L, irregular to order `lim` for M2L).
+__device__ C2 translationG(int kind, int l, int m, int lam, int mu, const double* H, int lim)
+{
+   if(kind == 0)
+   {
+      int dl = l - lam, dm = m - mu;
+      if(dl < 0 || abs(dm) > dl) return {0, 0};
+      C2 b = cplxOf(H, dl, dm);
+      double f = signPow(abs(m) - abs(m - mu) - abs(mu));
+      return {b.re * f, b.im * f};
+   }
+   if(kind == 1)
+   {
+      int dl = lam - l, dm = m - mu;
+      if(dl < 0 || abs(dm) > dl) return {0, 0};
+      C2 b = cplxOf(H, dl, dm);
+      double f = signPow(abs(mu) - abs(m - mu) - abs(m)) * (((lam + l) & 1) ? -1.0 : 1.0);
+      return {b.re * f, b.im * f};
+   }
+   int dl = l + lam, dm = m - mu;
+   if(dl > lim) return {0, 0};
+   C2 b = cplxOf(H, dl, dm);
+   double f = signPow(abs(m - mu) - abs(m) - abs(mu)) * ((lam & 1) ? -1.0 : 1.0);
+   return {b.re * f, b.im * f};
+}
+
+__device__ double operatorEntry(int kind, int i, int j, const double* H, int lim)
+{
+   const double s = 0.70710678118654752440;
+   int l = int(sqrt(double(i))); while(l * l > i) l--; while((l + 1) * (l + 1) <= i) l++;
+   int mi = i - l * l - l;
+   int lam = int(sqrt(double(j))); while(lam * lam > j) lam--; while((lam + 1) * (lam + 1) <= j) lam++;
+   int mj = j - lam * lam - lam;
+   // complex input of the unit real vector e_j
+   int mus[2]; C2 as[2]; int nin;
+   if(mj == 0) { mus[0] = 0; as[0] = {1, 0}; nin = 1; }
+   else if(mj > 0) { mus[0] = mj; as[0] = {s, 0}; mus[1] = -mj; as[1] = {s, 0}; nin = 2; }
+   else { mus[0] = -mj; as[0] = {0, s}; mus[1] = mj; as[1] = {0, -s}; nin = 2; }
+   auto res = [&](int m) {
+      C2 r = {0, 0};
+      for(int e = 0; e < nin; e++)
+      {
+         C2 g = translationG(kind, l, m, lam, mus[e], H, lim);
+         r.re += as[e].re * g.re - as[e].im * g.im;
+         r.im += as[e].re * g.im + as[e].im * g.re;
+      }
+      return r;
+   };
+   if(mi == 0) return res(0).re;
+   if(mi > 0) return s * (res(mi).re + res(-mi).re);
+   return s * (res(-mi).im - res(mi).im);
+}
+
+// One block per operator. op < 8: M2M octant, op < 16: L2L octant, else M2L slot.
+__global__ void kBuildOperators(int p, int lim, int first, int count, double* m2m, double* l2l, double* m2l)
+{
+   extern __shared__ double Hs[];
+   int op = first + blockIdx.x;
+   if(blockIdx.x >= count) return;
+   int L = nharm(p);
+   int kind = op < 8 ? 0 : (op < 16 ? 1 : 2);
+   if(threadIdx.x == 0)
+   {
+      if(kind < 2)
+      {
+         int oct = op & 7;
+         double t[3] = {((oct & 1) - 0.5) * 0.5, (((oct >> 1) & 1) - 0.5) * 0.5, (((oct >> 2) & 1) - 0.5) * 0.5};
+         if(kind == 1) { t[0] = -t[0]; t[1] = -t[1]; t[2] = -t[2]; }
+         realRegular<double>(p, t[0], t[1], t[2], Hs);
+      }
+      else
+      {
+         int o = d_m2lOffset[op - 16];
+         int ox = o % 7 - 3, oy = (o / 7) % 7 - 3, oz = o / 49 - 3;
+         realIrregular<double>(lim, double(ox), double(oy), double(oz), Hs);
+      }
+   }
+   __syncthreads();
+   double* out = kind == 0 ? m2m + int64_t(op) * L * L : kind == 1 ? l2l + int64_t(op - 8) * L * L
+                                                                   : m2l + int64_t(op - 16) * L * L;
+   for(int e = threadIdx.x; e < L * L; e += blockDim.x)
+   {
+      int i = e / L, j = e % L;
+      double v = operatorEntry(kind, i, j, Hs, lim);
+      int li = int(sqrt(double(i))); while(li * li > i) li--; while((li + 1) * (li + 1) <= i) li++;
+      int lj = int(sqrt(double(j))); while(lj * lj > j) lj--; while((lj + 1) * (lj + 1) <= j) lj++;
+      if(kind == 0) v = ldexp(v, -lj);        // scaled M2M: columns times 2^-lambda
+      else if(kind == 1) v = ldexp(v, -(li + 1));  // scaled L2L: rows times 2^-(l+1)
+      out[e] = v;
+   }
+}
+
+// Working copies: transposed [op][j (input)][k (output, padded to Lp)] in T.
+template <class T>
+__global__ void kTransposeOps(const double* __restrict__ src, int nops, int L, int Lp, T* dst)
+{
+   int64_t total = int64_t(nops) * L * Lp;
+   for(int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
+   {
+      int k = int(e % Lp);
+      int64_t r = e / Lp;
+      int j = int(r % L);
+      int op = int(r / L);
+      dst[e] = k < L ? T(src[(int64_t(op) * L + k) * L + j]) : T(0);
+   }
+}
+
+fmm_status buildOperators(Plan& P, cudaStream_t st)
+{
+   if(P.opOrder == P.p) return FMM_OK;
+   FMM_TRY(initOffsetTables());
+   const int p = P.p, L = P.L, Lp = P.Lp;
+   const int lim = P.cfg.m2l_truncate ? p : 2 * p;
+   FMM_TRY(P.opM2M64.reserve(sizeof(double) * 8 * L * L));
+   FMM_TRY(P.opL2L64.reserve(sizeof(double) * 8 * L * L));
+   FMM_TRY(P.opM2L64.reserve(sizeof(double) * 316 * L * L));
+   size_t shm = sizeof(double) * nharm(std::max(lim, p));
+   kBuildOperators<<<16 + 316, 256, shm, st>>>(p, lim, 0, 16 + 316, (double*)P.opM2M64.ptr, (double*)P.opL2L64.ptr,
+                                               (double*)P.opM2L64.ptr);
+   FMM_CHECK_LAUNCH();
+   size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_TRY(P.opM2Mw.reserve(es * 8 * L * Lp));
+   FMM_TRY(P.opL2Lw.reserve(es * 8 * L * Lp));
+   FMM_TRY(P.opM2Lw.reserve(es * 316 * L * Lp));
+   if(P.fp64)
+   {
+      kTransposeOps<double><<<1024, 256, 0, st>>>((const double*)P.opM2M64.ptr, 8, L, Lp, (double*)P.opM2Mw.ptr);
+      kTransposeOps<double><<<1024, 256, 0, st>>>((const double*)P.opL2L64.ptr, 8, L, Lp, (double*)P.opL2Lw.ptr);
+      kTransposeOps<double><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, 316, L, Lp, (double*)P.opM2Lw.ptr);
+   }
+   else
+   {
+      kTransposeOps<float><<<1024, 256, 0, st>>>((const double*)P.opM2M64.ptr, 8, L, Lp, (float*)P.opM2Mw.ptr);
+      kTransposeOps<float><<<1024, 256, 0, st>>>((const double*)P.opL2L64.ptr, 8, L, Lp, (float*)P.opL2Lw.ptr);
+      kTransposeOps<float><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, 316, L, Lp, (float*)P.opM2Lw.ptr);
+   }
+   FMM_CHECK_LAUNCH();
+   P.opOrder = p;
+   return FMM_OK;
+}
+
+// ====================================================================================
+// Geometry helpers
+// ====================================================================================
+__device__ __forceinline__ void nodeCenter(const RootBox& rb, int level, int ix, int iy, int iz, double c[3], double& h)
+{
+   h = 2.0 * rb.H / double(int64_t(1) << level);
+   c[0] = rb.center[0] - rb.H + (double(ix) + 0.5) * h;
+   c[1] = rb.center[1] - rb.H + (double(iy) + 0.5) * h;
+   c[2] = rb.center[2] - rb.H + (double(iz) + 0.5) * h;
+}
+
+// ====================================================================================
+// P2M: one block per leaf holding sources. Each thread writes the harmonics of one point
+// into a shared-memory row; then each thread reduces a set of coefficients over the rows.
+// ====================================================================================
+template <class T, int CH>
+__global__ void __launch_bounds__(CH) kP2M(Tree t, const RootBox* __restrict__ rootp,
+                                           const typename Vec4<T>::type* __restrict__ pos,
+                                           const typename Vec4<T>::type* __restrict__ q, int p, int Lp, T* __restrict__ M)
+{
+   extern __shared__ unsigned char smraw[];
+   const int node = blockIdx.x;
+   if(t.nchild[node] != 0) return;
+   const int s0 = t.s0[node], s1 = t.s1[node];
+   const int L = nharm(p);
+   const int LS = L | 1;  // odd row stride: conflict-free column access
+   T* R = (T*)smraw;                   // [CH][LS]
+   T* Q = R + CH * LS;                 // [CH][3]
+   const RootBox rb = *rootp;
+   double c[3], h;
+   nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], c, h);
+   const double ih = 1.0 / h;
+   constexpr int SLOTS = (nharm(MAXORDER) + CH - 1) / CH;
+   T acc[SLOTS][3];
+#pragma unroll
+   for(int s = 0; s < SLOTS; s++) acc[s][0] = acc[s][1] = acc[s][2] = T(0);
+   for(int base = s0; base < s1; base += CH)
+   {
+      const int cnt = min(CH, s1 - base);
+      if(threadIdx.x < cnt)
+      {
+         const auto x = pos[base + threadIdx.x];
+         const auto w = q[base + threadIdx.x];
+         T ux = T((double(x.x) - c[0]) * ih), uy = T((double(x.y) - c[1]) * ih), uz = T((double(x.z) - c[2]) * ih);
+         realRegular<T>(p, ux, uy, uz, R + threadIdx.x * LS);
+         Q[3 * threadIdx.x] = w.x; Q[3 * threadIdx.x + 1] = w.y; Q[3 * threadIdx.x + 2] = w.z;
+      }
+      __syncthreads();
+#pragma unroll
+      for(int s = 0; s < SLOTS; s++)
+      {
+         int k = threadIdx.x + s * CH;
+         if(k < L)
+            for(int i = 0; i < cnt; i++)
+            {
+               T r = R[i * LS + k];
+               acc[s][0] += Q[3 * i] * r;
+               acc[s][1] += Q[3 * i + 1] * r;
+               acc[s][2] += Q[3 * i + 2] * r;
+            }
+      }
+      __syncthreads();
+   }
+   T* out = M + int64_t(node) * 3 * Lp;
+#pragma unroll
+   for(int s = 0; s < SLOTS; s++)
+   {
+      int k = threadIdx.x + s * CH;
+      if(k < Lp)
+         for(int d = 0; d < 3; d++) out[d * Lp + k] = k < L ? acc[s][d] : T(0);
+   }
+}
+
+// ====================================================================================
+// M2M, one level: one block per node of the level with children; the parent sums the
+// translated multipoles of its children. Output coefficient k of degree l only needs input
+// coefficients j < (l+1)^2.
+// ====================================================================================
+template <class T>
+__global__ void __launch_bounds__(256) kM2M(Tree t, int a, int b, int p, int Lp, const T* __restrict__ opw,
+                                            T* __restrict__ M)
+{
+   extern __shared__ unsigned char smraw[];
+   T* Ms = (T*)smraw;  // [8][3][Lp]
+   const int node = a + blockIdx.x;
+   if(node >= b) return;
+   const int nc = t.nchild[node];
+   if(nc == 0 || t.s1[node] == t.s0[node]) return;
+   const int L = nharm(p);
+   const int c0 = t.child0[node];
+   for(int e = threadIdx.x; e < nc * 3 * Lp; e += blockDim.x) Ms[e] = M[int64_t(c0) * 3 * Lp + e];
+   __syncthreads();
+   for(int k = threadIdx.x; k < Lp; k += blockDim.x)
+   {
+      T acc[3] = {T(0), T(0), T(0)};
+      if(k < L)
+      {
+         int l = int(sqrtf(float(k)));
+         while(l * l > k) l--;
+         while((l + 1) * (l + 1) <= k) l++;
+         const int jmax = (l + 1) * (l + 1);
+         for(int c = 0; c < nc; c++)
+         {
+            const int ch = c0 + c;
+            if(t.s1[ch] == t.s0[ch]) continue;
+            const int oct = int(t.key[ch] & 7);
+            const T* op = opw + int64_t(oct) * L * Lp + k;
+            const T* mc = Ms + c * 3 * Lp;
+            for(int j = 0; j < jmax; j++)
+            {
+               const T o = op[int64_t(j) * Lp];
+               acc[0] += o * mc[j];
+               acc[1] += o * mc[Lp + j];
+               acc[2] += o * mc[2 * Lp + j];
+            }
+         }
+      }
+      T* out = M + int64_t(node) * 3 * Lp;
+      out[k] = acc[0]; out[Lp + k] = acc[1]; out[2 * Lp + k] = acc[2];
+   }
+}
+
+// ====================================================================================
+// L2L, one level: one block per node of the level holding targets; adds the parent's
+// translated local expansion. Output coefficient of degree l needs inputs of degree >= l.
+// ====================================================================================
+template <class T>
+__global__ void __launch_bounds__(256) kL2L(Tree t, int a, int b, int p, int Lp, const T* __restrict__ opw,
+                                            T* __restrict__ Lc)
+{
+   extern __shared__ unsigned char smraw[];
+   T* Ps = (T*)smraw;  // [3][Lp]
+   const int node = a + blockIdx.x;
+   if(node >= b) return;
+   if(t.t1[node] == t.t0[node]) return;
+   const int L = nharm(p);
+   const int par = t.parent[node];
+   for(int e = threadIdx.x; e < 3 * Lp; e += blockDim.x) Ps[e] = Lc[int64_t(par) * 3 * Lp + e];
+   __syncthreads();
+   const int oct = int(t.key[node] & 7);
+   T* out = Lc + int64_t(node) * 3 * Lp;
+   for(int k = threadIdx.x; k < L; k += blockDim.x)
+   {
+      int l = int(sqrtf(float(k)));
+      while(l * l > k) l--;
+      while((l + 1) * (l + 1) <= k) l++;
+      T acc[3] = {T(0), T(0), T(0)};
+      const T* op = opw + int64_t(oct) * L * Lp + k;
+      for(int j = l * l; j < L; j++)
+      {
+         const T o = op[int64_t(j) * Lp];
+         acc[0] += o * Ps[j];
+         acc[1] += o * Ps[Lp + j];
+         acc[2] += o * Ps[2 * Lp + j];
+      }
+      out[k] += acc[0]; out[Lp + k] += acc[1]; out[2 * Lp + k] += acc[2];
+   }
+}
+
+// ====================================================================================
+// M2L on the CUDA cores. A block owns TT consecutive target nodes (3 TT rows: node x
+// component) and all output coefficients; for each of the 316 offsets it gathers the source
+// rows named by the dense V table and multiplies by the operator, K-chunk by K-chunk through
+// shared memory. Thread (rg, cg): rows 12 rg .. 12 rg + 11, columns cg + 64 n.
+// ====================================================================================
+constexpr int M2L_TT = 16;
+constexpr int M2L_ROWS = 3 * M2L_TT;   // 48
+constexpr int M2L_CG = 64;
+constexpr int M2L_NC = 5;              // 5 x 64 = 320 >= Lp for p <= 16
+
+template <class T, int M2L_KC>
+__global__ void __launch_bounds__(256) kM2LSimt(int firstNode, int nNodes, const int* __restrict__ vtab,
+                                                const int* __restrict__ nv, int p, int Lp,
+                                                const T* __restrict__ opw, const T* __restrict__ M,
+                                                T* __restrict__ Lc)
+{
+   __shared__ T As[M2L_KC][M2L_ROWS];
+   __shared__ T Bs[M2L_KC][M2L_CG * M2L_NC];
+   __shared__ int srcRow[M2L_TT];
+   __shared__ int anyPresent;
+   const int L = nharm(p);
+   const int tid = threadIdx.x;
+   const int rg = tid / M2L_CG;   // 0..3
+   const int cg = tid % M2L_CG;   // 0..63
+   const int tgt0 = firstNode + blockIdx.x * M2L_TT;
+   T acc[12][M2L_NC];
+#pragma unroll
+   for(int r = 0; r < 12; r++)
+#pragma unroll
+      for(int n = 0; n < M2L_NC; n++) acc[r][n] = T(0);
+   for(int o = 0; o < 316; o++)
+   {
+      __syncthreads();
+      if(tid == 0) anyPresent = 0;
+      __syncthreads();
+      if(tid < M2L_TT)
+      {
+         int node = tgt0 + tid;
+         int s = -1;
+         if(node < firstNode + nNodes && nv[node] > 0) s = vtab[int64_t(node) * 316 + o];
+         srcRow[tid] = s;
+         if(s >= 0) anyPresent = 1;
+      }
+      __syncthreads();
+      if(!anyPresent) continue;
+      const T* op = opw + int64_t(o) * L * Lp;
+      for(int k0 = 0; k0 < L; k0 += M2L_KC)
+      {
+         __syncthreads();
+         // gather A: rows = (target, component), columns = input coefficients k0..k0+KC
+         for(int e = tid; e < M2L_KC * M2L_ROWS; e += 256)
+         {
+            int kk = e % M2L_KC, row = e / M2L_KC;
+            int s = srcRow[row / 3];
+            int k = k0 + kk;
+            As[kk][row] = (s >= 0 && k < L) ? M[(int64_t(s) * 3 + row % 3) * Lp + k] : T(0);
+         }
+         for(int e = tid; e < M2L_KC * M2L_CG * M2L_NC; e += 256)
+         {
+            int col = e % (M2L_CG * M2L_NC), kk = e / (M2L_CG * M2L_NC);
+            int k = k0 + kk;
+            Bs[kk][col] = (k < L && col < Lp) ? op[int64_t(k) * Lp + col] : T(0);
+         }
+         __syncthreads();
+#pragma unroll 4
+         for(int kk = 0; kk < M2L_KC; kk++)
+         {
+            T a[12], bv[M2L_NC];
+#pragma unroll
+            for(int r = 0; r < 12; r++) a[r] = As[kk][12 * rg + r];
+#pragma unroll
+            for(int n = 0; n < M2L_NC; n++) bv[n] = Bs[kk][cg + M2L_CG * n];
+#pragma unroll
+            for(int r = 0; r < 12; r++)
+#pragma unroll
+               for(int n = 0; n < M2L_NC; n++) acc[r][n] += a[r] * bv[n];
+         }
+      }
+   }
+#pragma unroll
+   for(int r = 0; r < 12; r++)
+   {
+      int row = 12 * rg + r;
+      int node = tgt0 + row / 3;
+      if(node >= firstNode + nNodes) continue;
+#pragma unroll
+      for(int n = 0; n < M2L_NC; n++)
+      {
+         int col = cg + M2L_CG * n;
+         if(col < Lp) Lc[(int64_t(node) * 3 + row % 3) * Lp + col] = col < L ? acc[r][n] : T(0);
+      }
+   }
+}
+
+// ====================================================================================
+// L2P + near field: one block per target leaf. The local expansion is turned into the
+// expansion of B = curl A (order p - 1) in shared memory, evaluated per target by the
+// harmonic recurrence, then the direct sum over the leaf's source list is added.
+//
+// Real-basis derivatives used for the curl (R = regular harmonics, standard convention):
+//   d/dz R_l^{+-m} = -R_{l-1}^{+-m}
+//   d/dx, d/dy move m by one; see gradCoeff below.
+// ====================================================================================
+template <class T>
+__device__ inline T coefAt(const T* Lv, int l, int m)
+{
+   return (abs(m) <= l) ? Lv[hidx(l, m)] : T(0);
+}
+
+// Coefficient of R_{l'}^{mu} in d/dx_j (sum_k L_k R_k), j = 0 (x), 1 (y), 2 (z); l = l' + 1.
+template <class T>
+__device__ inline T gradCoeff(const T* Lv, int j, int lp, int mu)
+{
+   const int l = lp + 1;
+   const T h = T(0.5), r2 = T(0.70710678118654752440);
+   if(j == 2) return -coefAt(Lv, l, mu);
+   if(j == 0)
+   {
+      if(mu == 0) return -r2 * coefAt(Lv, l, 1);
+      if(mu == 1) return -h * coefAt(Lv, l, 2) + r2 * coefAt(Lv, l, 0);
+      if(mu >= 2) return -h * coefAt(Lv, l, mu + 1) + h * coefAt(Lv, l, mu - 1);
+      if(mu == -1) return -h * coefAt(Lv, l, -2);
+      return -h * coefAt(Lv, l, mu - 1) + h * coefAt(Lv, l, mu + 1);
+   }
+   if(mu == 0) return -r2 * coefAt(Lv, l, -1);
+   if(mu == 1) return -h * coefAt(Lv, l, -2);
+   if(mu >= 2) return -h * coefAt(Lv, l, -(mu + 1)) - h * coefAt(Lv, l, -(mu - 1));
+   if(mu == -1) return h * coefAt(Lv, l, 2) + r2 * coefAt(Lv, l, 0);
+   return h * coefAt(Lv, l, 1 - mu) + h * coefAt(Lv, l, -mu - 1);
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict__ rootp, int p, int Lp,
+                                               const T* __restrict__ Lc,
+                                               const typename Vec4<T>::type* __restrict__ tpos,
+                                               const typename Vec4<T>::type* __restrict__ spos,
+                                               const typename Vec4<T>::type* __restrict__ sq,
+                                               const int* __restrict__ p2pOff, const int* __restrict__ p2pList,
+                                               const int* __restrict__ tOrder, T scaleB, T scaleA, int want,
+                                               T* __restrict__ outB, T* __restrict__ outA)
+{
+   typedef typename Vec4<T>::type V4;
+   extern __shared__ unsigned char smraw[];
+   const int node = blockIdx.x;
+   if(t.nchild[node] != 0 || t.t1[node] == t.t0[node]) return;
+   const int L = nharm(p);
+   const int Lb = nharm(p - 1);
+   T* Ls = (T*)smraw;          // [3][L] local
+   T* Cs = Ls + 3 * L;         // [3][Lb] curl expansion
+   V4* Sp = (V4*)(Cs + 3 * Lb);  // [NT] source tile positions
+   V4* Sq = Sp + NT;           // [NT] source tile strengths
+   for(int e = threadIdx.x; e < 3 * L; e += NT) Ls[e] = Lc[int64_t(node) * 3 * Lp + (e / L) * Lp + e % L];
+   __syncthreads();
+   for(int e = threadIdx.x; e < 3 * Lb; e += NT)
+   {
+      const int c = e / Lb, k = e % Lb;
+      int lp = int(sqrtf(float(k)));
+      while(lp * lp > k) lp--;
+      while((lp + 1) * (lp + 1) <= k) lp++;
+      const int mu = k - lp * lp - lp;
+      // B_x = dAz/dy - dAy/dz, B_y = dAx/dz - dAz/dx, B_z = dAy/dx - dAx/dy
+      const int cp = (c + 2) % 3, cm = (c + 1) % 3;   // (z,y) for x; (x,z) for y; (y,x) for z
+      const int jp = (c + 1) % 3, jm = (c + 2) % 3;
+      Cs[e] = gradCoeff(Ls + cp * L, jp, lp, mu) - gradCoeff(Ls + cm * L, jm, lp, mu);
+   }
+   __syncthreads();
+   const RootBox rb = *rootp;
+   double c[3], h;
+   nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], c, h);
+   const T ih = T(1.0 / h), ih2 = T(1.0 / (h * h));
+   const int t0 = t.t0[node], t1 = t.t1[node];
+   const int e0 = p2pOff[node], e1 = p2pOff[node + 1];
+   for(int base = t0; base < t1; base += NT)
+   {
+      const int ti = base + threadIdx.x;
+      const bool active = ti < t1;
+      V4 x = active ? tpos[ti] : V4{T(0), T(0), T(0), T(0)};
+      T B[3] = {T(0), T(0), T(0)}, A[3] = {T(0), T(0), T(0)};
+      if(active)
+      {
+         const T ux = T((double(x.x) - c[0]) / h), uy = T((double(x.y) - c[1]) / h), uz = T((double(x.z) - c[2]) / h);
+         const T sq2 = T(1.4142135623730950488);
+         const bool wantA = (want & 2) != 0;
+         visitRegular<T>(p, ux, uy, uz, [&](int l, int m, T re, T im) {
+            const T s = (l & 1) ? T(-1) : T(1);
+            T r0, r1;
+            if(m == 0) { r0 = s * re; r1 = T(0); }
+            else { r0 = s * sq2 * re; r1 = s * sq2 * im; }
+            if(l < p)
+            {
+               const int k0 = hidx(l, m), k1 = hidx(l, -m);
+               for(int d = 0; d < 3; d++)
+               {
+                  B[d] += Cs[d * Lb + k0] * r0;
+                  if(m) B[d] += Cs[d * Lb + k1] * r1;
+               }
+            }
+            if(wantA)
+            {
+               const int k0 = hidx(l, m), k1 = hidx(l, -m);
+               for(int d = 0; d < 3; d++)
+               {
+                  A[d] += Ls[d * L + k0] * r0;
+                  if(m) A[d] += Ls[d * L + k1] * r1;
+               }
+            }
+         });
+         for(int d = 0; d < 3; d++) { B[d] *= ih2; A[d] *= ih; }
+      }
+      // direct near field
+      for(int e = e0; e < e1; e++)
+      {
+         const int S = p2pList[e];
+         const int a0 = t.s0[S], a1 = t.s1[S];
+         for(int sb = a0; sb < a1; sb += NT)
+         {
+            const int cnt = min(NT, a1 - sb);
+            __syncthreads();
+            if(threadIdx.x < cnt) { Sp[threadIdx.x] = spos[sb + threadIdx.x]; Sq[threadIdx.x] = sq[sb + threadIdx.x]; }
+            __syncthreads();
+            if(active)
+               for(int i = 0; i < cnt; i++)
+               {
+                  const V4 y = Sp[i], w = Sq[i];
+                  const T dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+                  const T r2 = dx * dx + dy * dy + dz * dz;
+                  if(r2 == T(0)) continue;
+                  T ri;
+                  if constexpr(sizeof(T) == 4) ri = rsqrtf(r2);
+                  else ri = rsqrt(r2);
+                  const T ri3 = ri * ri * ri;
+                  B[0] += (w.y * dz - w.z * dy) * ri3;
+                  B[1] += (w.z * dx - w.x * dz) * ri3;
+                  B[2] += (w.x * dy - w.y * dx) * ri3;
+                  A[0] += w.x * ri; A[1] += w.y * ri; A[2] += w.z * ri;
+               }
+         }
+      }
+      if(active)
+      {
+         const int o = tOrder[ti];
+         if(want & 1) for(int d = 0; d < 3; d++) outB[3 * int64_t(o) + d] = B[d] * scaleB;
+         if(want & 2) for(int d = 0; d < 3; d++) outA[3 * int64_t(o) + d] = A[d] * scaleA;
+      }
+   }
+}
+
+// ====================================================================================
+// Direct sums over all sources (fmm_direct): one thread per target, sources staged through
+// shared memory.
+// ====================================================================================
+template <class T, class U, int NT>
+__global__ void __launch_bounds__(NT) kDirect(const typename Vec4<T>::type* __restrict__ spos,
+                                              const typename Vec4<T>::type* __restrict__ sq, int n,
+                                              const U* __restrict__ tgt, int m, U scaleB, U scaleA, int want,
+                                              U* __restrict__ outB, U* __restrict__ outA)
+{
+   __shared__ U Sp[NT][4];
+   __shared__ U Sq[NT][3];
+   const int ti = blockIdx.x * NT + threadIdx.x;
+   const bool active = ti < m;
+   U x = 0, y = 0, z = 0;
+   if(active) { x = tgt[3 * ti]; y = tgt[3 * ti + 1]; z = tgt[3 * ti + 2]; }
+   U B[3] = {0, 0, 0}, A[3] = {0, 0, 0};
+   for(int sb = 0; sb < n; sb += NT)
+   {
+      const int cnt = min(NT, n - sb);
+      __syncthreads();
+      if(threadIdx.x < cnt)
+      {
+         const auto a = spos[sb + threadIdx.x];
+         const auto b = sq[sb + threadIdx.x];
+         Sp[threadIdx.x][0] = U(a.x); Sp[threadIdx.x][1] = U(a.y); Sp[threadIdx.x][2] = U(a.z);
+         Sq[threadIdx.x][0] = U(b.x); Sq[threadIdx.x][1] = U(b.y); Sq[threadIdx.x][2] = U(b.z);
+      }
+      __syncthreads();
+      if(active)
+         for(int i = 0; i < cnt; i++)
+         {
+            const U dx = x - Sp[i][0], dy = y - Sp[i][1], dz = z - Sp[i][2];
+            const U r2 = dx * dx + dy * dy + dz * dz;
+            if(r2 == U(0)) continue;
+            U ri;
+            if constexpr(sizeof(U) == 4) ri = rsqrtf(r2);
+            else ri = U(1) / sqrt(r2);
+            const U ri3 = ri * ri * ri;
+            B[0] += (Sq[i][1] * dz - Sq[i][2] * dy) * ri3;
+            B[1] += (Sq[i][2] * dx - Sq[i][0] * dz) * ri3;
+            B[2] += (Sq[i][0] * dy - Sq[i][1] * dx) * ri3;
+            A[0] += Sq[i][0] * ri; A[1] += Sq[i][1] * ri; A[2] += Sq[i][2] * ri;
+         }
+   }
+   if(active)
+   {
+      if(want & 1) for(int d = 0; d < 3; d++) outB[3 * int64_t(ti) + d] = B[d] * scaleB;
+      if(want & 2) for(int d = 0; d < 3; d++) outA[3 * int64_t(ti) + d] = A[d] * scaleA;
+   }
+}
+
+// ====================================================================================
+// Host drivers
+// ====================================================================================
+template <class T>
+fmm_status upwardT(Plan& P, cudaStream_t st)
+{
+   FMM_TRY(buildOperators(P, st));
+   const int64_t N = P.tree.nNodes;
+   const int L = P.L, Lp = P.Lp;
+   FMM_TRY(P.mult.reserve(sizeof(T) * N * 3 * Lp));
+   FMM_CUDA(cudaMemsetAsync(P.mult.ptr, 0, sizeof(T) * N * 3 * Lp, st));
+   typedef typename Vec4<T>::type V4;
+   constexpr int CH = sizeof(T) == 4 ? 64 : 32;
+   size_t shm = sizeof(T) * (CH * (L | 1) + 3 * CH);
+   FMM_CUDA(cudaFuncSetAttribute(kP2M<T, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+   kP2M<T, CH><<<int(N), CH, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
+                                        (T*)P.mult.ptr);
+   FMM_CHECK_LAUNCH();
+   size_t shm2 = sizeof(T) * 8 * 3 * Lp;
+   FMM_CUDA(cudaFuncSetAttribute(kM2M<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
+   for(int level = P.tree.nLevels - 2; level >= 0; level--)
+   {
+      int a = P.tree.levelStart[level], b = P.tree.levelStart[level + 1];
+      kM2M<T><<<b - a, 256, shm2, st>>>(P.tree, a, b, P.p, Lp, (const T*)P.opM2Mw.ptr, (T*)P.mult.ptr);
+   }
+   FMM_CHECK_LAUNCH();
+   return FMM_OK;
+}
+
+template <class T>
+fmm_status m2lSimt(Plan& P, cudaStream_t st)
+{
+   const int64_t N = P.tree.nNodes;
+   int first = 1;
+   int count = int(N - 1);
+   if(count <= 0) return FMM_OK;
+   int blocks = (count + M2L_TT - 1) / M2L_TT;
+   constexpr int KC = sizeof(T) == 4 ? 32 : 16;
+   kM2LSimt<T, KC><<<blocks, 256, 0, st>>>(first, count, P.lists.vtab, P.lists.nv, P.p, P.Lp, (const T*)P.opM2Lw.ptr,
+                                       (const T*)P.mult.ptr, (T*)P.local.ptr);
+   FMM_CHECK_LAUNCH();
+   return FMM_OK;
+}
+
+template <class T>
+fmm_status downwardT(Plan& P, cudaStream_t st)
+{
+   const int64_t N = P.tree.nNodes;
+   const int Lp = P.Lp;
+   FMM_TRY(P.local.reserve(sizeof(T) * N * 3 * Lp));
+   FMM_CUDA(cudaMemsetAsync(P.local.ptr, 0, sizeof(T) * N * 3 * Lp, st));
+   if(sizeof(T) == 4 && P.cfg.m2l_mode != FMM_M2L_SIMT) FMM_TRY(m2lTensorCore(P, st));
+   else FMM_TRY(m2lSimt<T>(P, st));
+   if(P.eventsMade) cudaEventRecord(P.ev[3], st);
+   size_t shm = sizeof(T) * 3 * Lp;
+   for(int level = 1; level < P.tree.nLevels; level++)
+   {
+      int a = P.tree.levelStart[level], b = P.tree.levelStart[level + 1];
+      kL2L<T><<<b - a, 256, shm, st>>>(P.tree, a, b, P.p, Lp, (const T*)P.opL2Lw.ptr, (T*)P.local.ptr);
+   }
+   FMM_CHECK_LAUNCH();
+   return FMM_OK;
+}
+
+template <class T>
+fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
+{
+   typedef typename Vec4<T>::type V4;
+   const int64_t N = P.tree.nNodes;
+   const int L = P.L, Lb = nharm(P.p - 1);
+   constexpr int NT = 64;
+   size_t shm = sizeof(T) * (3 * L + 3 * Lb) + 2 * sizeof(V4) * NT;
+   FMM_CUDA(cudaFuncSetAttribute(kL2PNear<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+   T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
+   kL2PNear<T, NT><<<int(N), NT, shm, st>>>(P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr,
+                                            (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, (const int*)P.p2pOff.ptr,
+                                            (const int*)P.p2pList.ptr, (const int*)P.tIdx.ptr, scaleB, scaleA, want,
+                                            (T*)P.outB.ptr, (T*)P.outA.ptr);
+   FMM_CHECK_LAUNCH();
+   return FMM_OK;
+}
+
+template <class T>
+fmm_status directT(Plan& P, double current, int want, cudaStream_t st)
+{
+   typedef typename Vec4<T>::type V4;
+   constexpr int NT = 128;
+   T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
+   int blocks = int((P.m + NT - 1) / NT);
+   if(blocks == 0) return FMM_OK;
+   kDirect<T, T, NT><<<blocks, NT, 0, st>>>((const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, int(P.n),
+                                           (const T*)P.tgtXYZ, int(P.m), scaleB, scaleA, want, (T*)P.outB.ptr,
+                                           (T*)P.outA.ptr);
+   FMM_CHECK_LAUNCH();
+   return FMM_OK;
+}
+
+fmm_status directFp64Subset(Plan& P, double current, const double* tgtDev, int k, double* outDev, cudaStream_t st)
+{
+   constexpr int NT = 128;
+   int blocks = (k + NT - 1) / NT;
+   if(blocks == 0) return FMM_OK;
+   double scaleB = REF_MU0 / (4 * REF_PI) * current;
+   if(P.fp64)
+      kDirect<double, double, NT><<<blocks, NT, 0, st>>>((const double4*)P.sPos.ptr, (const double4*)P.sQ.ptr,
+                                                         int(P.n), tgtDev, k, scaleB, 0.0, 1, outDev, nullptr);
+   else
+      kDirect<float, double, NT><<<blocks, NT, 0, st>>>((const float4*)P.sPos.ptr, (const float4*)P.sQ.ptr, int(P.n),
+                                                        tgtDev, k, scaleB, 0.0, 1, outDev, nullptr);
+   FMM_CHECK_LAUNCH();
+   return FMM_OK;
+}
+
+template fmm_status upwardT<float>(Plan&, cudaStream_t);
+template fmm_status upwardT<double>(Plan&, cudaStream_t);
+template fmm_status downwardT<float>(Plan&, cudaStream_t);
+template fmm_status downwardT<double>(Plan&, cudaStream_t);
+template fmm_status evaluateT<float>(Plan&, double, int, cudaStream_t);
+template fmm_status evaluateT<double>(Plan&, double, int, cudaStream_t);
+template fmm_status directT<float>(Plan&, double, int, cudaStream_t);
+template fmm_status directT<double>(Plan&, double, int, cudaStream_t);
+
+}  // namespace fmm

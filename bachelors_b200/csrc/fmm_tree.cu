@@ -1,0 +1,510 @@
+// Device octree and interaction lists.
+//
+// Replaces the reference's pointer octrees and its dual-tree map building
+// (FMM/FMMGPU/quadrature_octree.cpp:23-97, calculation_point_octree.cpp:26-97,
+// fast_multipole_solver.cpp:105-184) with one Morton-ordered octree over sources and targets,
+// built level by level on the device:
+//   keys      63-bit Morton codes, 21 bits per axis, x in the lowest bit of each triple
+//   sort      CUB radix sort of (key, index) for sources and for targets
+//   nodes     a node at level l holds the points whose key prefix matches; it splits when it
+//             holds more than `cap` sources or more than `cap` targets (and l < 21); its
+//             children are the non-empty octants, found by binary search in the sorted keys
+//   lists     Col (same-level adjacent), A (coarser adjacent leaves), X (coarser non-adjacent
+//             leaves), V (same-level M2L sources, dense table over the 316 offsets), and for
+//             each target leaf the CSR list of source nodes whose points it sums directly.
+#include <cub/cub.cuh>
+
+#include "fmm_internal.cuh"
+
+namespace fmm {
+
+// ------------------------------------------------------------------------------ bounding box
+template <class T>
+__global__ void kBBox(const T* __restrict__ a, int64_t na, const T* __restrict__ b, int64_t nb, double* partial)
+{
+   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+   int64_t n = na + nb;
+   for(int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+   {
+      const T* p = i < na ? a + 3 * i : b + 3 * (i - na);
+      for(int d = 0; d < 3; d++)
+      {
+         double v = double(p[d]);
+         lo[d] = fmin(lo[d], v);
+         hi[d] = fmax(hi[d], v);
+      }
+   }
+   typedef cub::BlockReduce<double, 256> BR;
+   __shared__ typename BR::TempStorage tmp;
+   for(int d = 0; d < 3; d++)
+   {
+      double l = BR(tmp).Reduce(lo[d], cub::Min());
+      __syncthreads();
+      double h = BR(tmp).Reduce(hi[d], cub::Max());
+      __syncthreads();
+      if(threadIdx.x == 0) { partial[6 * blockIdx.x + d] = l; partial[6 * blockIdx.x + 3 + d] = h; }
+   }
+}
+
+// Root cube around the bounding box: center = (lo + hi) / 2, H = max half extent * (1 + 2^-20) + 1e-300.
+__global__ void kRootFromBBox(const double* partial, int nblocks, RootBox* root)
+{
+   if(threadIdx.x != 0 || blockIdx.x != 0) return;
+   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+   for(int b = 0; b < nblocks; b++)
+      for(int d = 0; d < 3; d++)
+      {
+         lo[d] = fmin(lo[d], partial[6 * b + d]);
+         hi[d] = fmax(hi[d], partial[6 * b + 3 + d]);
+      }
+   double H = 0;
+   for(int d = 0; d < 3; d++)
+   {
+      root->center[d] = 0.5 * (lo[d] + hi[d]);
+      H = fmax(H, hi[d] - lo[d]);
+   }
+   H = 0.5 * H;
+   H = __dadd_rn(__dmul_rn(H, 1.0 + 9.5367431640625e-07), 1e-300);
+   root->H = H;
+   for(int d = 0; d < 3; d++) root->lo[d] = root->center[d] - H;
+   root->scale = double(1 << MAXLEVEL) / (2.0 * H);
+}
+
+__global__ void kRootFromConfig(double cx, double cy, double cz, double H, RootBox* root)
+{
+   if(threadIdx.x != 0 || blockIdx.x != 0) return;
+   root->center[0] = cx; root->center[1] = cy; root->center[2] = cz;
+   root->H = H;
+   for(int d = 0; d < 3; d++) root->lo[d] = root->center[d] - H;
+   root->scale = double(1 << MAXLEVEL) / (2.0 * H);
+}
+
+// ------------------------------------------------------------------------------ Morton keys
+__device__ __forceinline__ uint64_t spread3(uint64_t v)
+{
+   v &= 0x1fffff;
+   v = (v | v << 32) & 0x1f00000000ffffull;
+   v = (v | v << 16) & 0x1f0000ff0000ffull;
+   v = (v | v << 8) & 0x100f00f00f00f00full;
+   v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+   v = (v | v << 2) & 0x1249249249249249ull;
+   return v;
+}
+
+__device__ __forceinline__ int64_t quantize(double x, double lo, double scale)
+{
+   double u = floor(__dmul_rn(__dsub_rn(x, lo), scale));
+   u = fmax(u, 0.0);
+   u = fmin(u, double((1 << MAXLEVEL) - 1));
+   return int64_t(u);
+}
+
+template <class T>
+__global__ void kKeys(const T* __restrict__ xyz, int64_t n, const RootBox* __restrict__ root, uint64_t* keys, int* idx)
+{
+   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+   if(i >= n) return;
+   int64_t ux = quantize(double(xyz[3 * i]), root->lo[0], root->scale);
+   int64_t uy = quantize(double(xyz[3 * i + 1]), root->lo[1], root->scale);
+   int64_t uz = quantize(double(xyz[3 * i + 2]), root->lo[2], root->scale);
+   keys[i] = spread3(uint64_t(ux)) | (spread3(uint64_t(uy)) << 1) | (spread3(uint64_t(uz)) << 2);
+   idx[i] = int(i);
+}
+
+template <class T>
+__global__ void kGatherSources(const T* __restrict__ xyz, const T* __restrict__ w, const T* __restrict__ J,
+                               const int* __restrict__ order, int64_t n, typename Vec4<T>::type* pos,
+                               typename Vec4<T>::type* q)
+{
+   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+   if(i >= n) return;
+   int64_t s = order[i];
+   T x = xyz[3 * s], y = xyz[3 * s + 1], z = xyz[3 * s + 2];
+   T jx, jy, jz;
+   if(J) { jx = J[3 * s]; jy = J[3 * s + 1]; jz = J[3 * s + 2]; }
+   else
+   {
+      // perp(q).normalized() (FMM/FMMGPU/vector3.cu:154-204): (-y, x, 0) / |(-y, x, 0)|
+      T l = sqrt(x * x + y * y);
+      if(l != T(0)) { jx = -y / l; jy = x / l; }
+      else { jx = T(0); jy = T(0); }
+      jz = T(0);
+   }
+   T ww = w[s];
+   pos[i] = {x, y, z, T(0)};
+   q[i] = {ww * jx, ww * jy, ww * jz, T(0)};
+}
+
+template <class T>
+__global__ void kGatherTargets(const T* __restrict__ xyz, const int* __restrict__ order, int64_t m,
+                               typename Vec4<T>::type* pos)
+{
+   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+   if(i >= m) return;
+   int64_t s = order[i];
+   pos[i] = {xyz[3 * s], xyz[3 * s + 1], xyz[3 * s + 2], T(0)};
+}
+
+// ------------------------------------------------------------------------------ nodes
+__global__ void kInitRoot(Tree t, int n, int m)
+{
+   t.key[0] = 0; t.level[0] = 0; t.ix[0] = t.iy[0] = t.iz[0] = 0;
+   t.s0[0] = 0; t.s1[0] = n; t.t0[0] = 0; t.t1[0] = m; t.parent[0] = -1; t.child0[0] = -1; t.nchild[0] = 0;
+}
+
+__device__ __forceinline__ int lowerBound(const uint64_t* __restrict__ keys, int a, int b, uint64_t v)
+{
+   while(a < b)
+   {
+      int mid = (a + b) >> 1;
+      if(keys[mid] < v) a = mid + 1;
+      else b = mid;
+   }
+   return a;
+}
+
+// For nodes [a, b) of `level`: decide the split and find the 8 children's ranges.
+__global__ void kCountChildren(Tree t, int a, int b, int level, int cap, int capT, const uint64_t* __restrict__ skeys,
+                               const uint64_t* __restrict__ tkeys, int* bounds, int* cnt)
+{
+   int i = a + blockIdx.x * blockDim.x + threadIdx.x;
+   if(i >= b) return;
+   int j = i - a;
+   int s0 = t.s0[i], s1 = t.s1[i], t0 = t.t0[i], t1 = t.t1[i];
+   t.child0[i] = -1;
+   t.nchild[i] = 0;
+   if(!((s1 - s0 > cap || t1 - t0 > capT) && level < MAXLEVEL)) { cnt[j] = 0; return; }
+   uint64_t key = t.key[i];
+   int shift = 3 * (MAXLEVEL - level - 1);
+   int sb[9], tb[9];
+   for(int c = 0; c < 8; c++)
+   {
+      uint64_t bound = ((key << 3) + uint64_t(c)) << shift;
+      sb[c] = c == 0 ? s0 : lowerBound(skeys, s0, s1, bound);
+      tb[c] = c == 0 ? t0 : lowerBound(tkeys, t0, t1, bound);
+   }
+   sb[8] = s1; tb[8] = t1;
+   int k = 0;
+   for(int c = 0; c < 8; c++)
+   {
+      bounds[18 * j + c] = sb[c];
+      bounds[18 * j + 9 + c] = tb[c];
+      if(sb[c + 1] - sb[c] + tb[c + 1] - tb[c] > 0) k++;
+   }
+   bounds[18 * j + 8] = s1;
+   bounds[18 * j + 17] = t1;
+   cnt[j] = k;
+}
+
+__global__ void kMakeChildren(Tree t, int a, int b, int level, int next, const int* __restrict__ bounds,
+                              const int* __restrict__ cnt, const int* __restrict__ off)
+{
+   int i = a + blockIdx.x * blockDim.x + threadIdx.x;
+   if(i >= b) return;
+   int j = i - a;
+   if(cnt[j] == 0) return;
+   int c0 = next + off[j];
+   t.child0[i] = c0;
+   t.nchild[i] = cnt[j];
+   const int* sb = bounds + 18 * j;
+   const int* tb = sb + 9;
+   uint64_t key = t.key[i];
+   int k = 0;
+   for(int c = 0; c < 8; c++)
+   {
+      if(sb[c + 1] - sb[c] + tb[c + 1] - tb[c] == 0) continue;
+      int ch = c0 + k++;
+      t.key[ch] = (key << 3) | uint64_t(c);
+      t.level[ch] = level + 1;
+      t.ix[ch] = 2 * t.ix[i] + (c & 1);
+      t.iy[ch] = 2 * t.iy[i] + ((c >> 1) & 1);
+      t.iz[ch] = 2 * t.iz[i] + ((c >> 2) & 1);
+      t.s0[ch] = sb[c]; t.s1[ch] = sb[c + 1];
+      t.t0[ch] = tb[c]; t.t1[ch] = tb[c + 1];
+      t.parent[ch] = i;
+      t.child0[ch] = -1;
+      t.nchild[ch] = 0;
+   }
+}
+
+// ------------------------------------------------------------------------------ lists
+__device__ __forceinline__ bool adjacentNodes(const Tree& t, int a, int b)
+{
+   int la = t.level[a], lb = t.level[b];
+   int c = la <= lb ? a : b, f = la <= lb ? b : a;
+   int sh = abs(lb - la);
+   int64_t s = int64_t(1) << sh;
+   int64_t ci[3] = {t.ix[c], t.iy[c], t.iz[c]}, fi[3] = {t.ix[f], t.iy[f], t.iz[f]};
+   for(int d = 0; d < 3; d++)
+      if(fi[d] < ci[d] * s - 1 || fi[d] > (ci[d] + 1) * s) return false;
+   return true;
+}
+
+__global__ void kInitRootLists(Lists L)
+{
+   L.col[0] = 0; L.ncol[0] = 1; L.na[0] = 0; L.nx[0] = 0; L.nv[0] = 0;
+}
+
+// One thread per node D of a level >= 1; the parent's lists are complete.
+__global__ void kListsLevel(Tree t, Lists L, int a, int b, int* err)
+{
+   int D = a + blockIdx.x * blockDim.x + threadIdx.x;
+   if(D >= b) return;
+   int P = t.parent[D];
+   int ncol = 0, na = 0, nx = 0, nv = 0;
+   int* vt = L.vtab + int64_t(D) * 316;
+   for(int k = 0; k < 316; k++) vt[k] = -1;
+   const bool hasT = t.t1[D] > t.t0[D];
+   auto coarse = [&](int S) {
+      if(adjacentNodes(t, S, D))
+      {
+         if(na < ACAP) L.acoarse[int64_t(D) * ACAP + na] = S;
+         else atomicOr(err, ERR_LIST_A);
+         na++;
+      }
+      else
+      {
+         if(nx < XCAP) L.xl[int64_t(D) * XCAP + nx] = S;
+         else atomicOr(err, ERR_LIST_X);
+         nx++;
+      }
+   };
+   for(int k = 0; k < L.ncol[P]; k++)
+   {
+      int C = L.col[int64_t(P) * COLCAP + k];
+      int nc = t.nchild[C];
+      if(nc == 0) { coarse(C); continue; }
+      int c0 = t.child0[C];
+      for(int e = 0; e < nc; e++)
+      {
+         int c = c0 + e;
+         if(adjacentNodes(t, c, D))
+         {
+            if(ncol < COLCAP) L.col[int64_t(D) * COLCAP + ncol] = c;
+            else atomicOr(err, ERR_LIST_COL);
+            ncol++;
+         }
+         else if(hasT && t.s1[c] > t.s0[c])
+         {
+            int ox = t.ix[c] - t.ix[D], oy = t.iy[c] - t.iy[D], oz = t.iz[c] - t.iz[D];
+            int o = d_m2lIndex[offsetIndex(ox, oy, oz)];
+            if(o >= 0) { vt[o] = c; nv++; }
+            else atomicOr(err, ERR_LIST_V);
+         }
+      }
+   }
+   for(int k = 0; k < L.na[P]; k++) coarse(L.acoarse[int64_t(P) * ACAP + k]);
+   L.ncol[D] = min(ncol, COLCAP);
+   L.na[D] = min(na, ACAP);
+   L.nx[D] = min(nx, XCAP);
+   L.nv[D] = nv;
+}
+
+// Direct-interaction source nodes of every target leaf (count pass when out == nullptr).
+__global__ void kP2PLists(Tree t, Lists L, int nNodes, const int* __restrict__ off, int* cnt, int* out, int* err)
+{
+   int T = blockIdx.x * blockDim.x + threadIdx.x;
+   if(T >= nNodes) return;
+   if(t.nchild[T] != 0 || t.t1[T] == t.t0[T]) { if(!out) cnt[T] = 0; return; }
+   int k = 0;
+   int base = out ? off[T] : 0;
+   auto emit = [&](int S) {
+      if(t.s1[S] == t.s0[S]) return;
+      if(out) out[base + k] = S;
+      k++;
+   };
+   // same-level leaf colleagues (including T itself) and coarser adjacent leaves
+   for(int e = 0; e < L.ncol[T]; e++)
+   {
+      int C = L.col[int64_t(T) * COLCAP + e];
+      if(t.nchild[C] == 0) emit(C);
+   }
+   for(int e = 0; e < L.na[T]; e++) emit(L.acoarse[int64_t(T) * ACAP + e]);
+   // finer nodes below non-leaf colleagues: adjacent leaves, and non-adjacent nodes whose parent
+   // is adjacent (the duals of A and X)
+   int stack[256];
+   int sp = 0;
+   for(int e = 0; e < L.ncol[T]; e++)
+   {
+      int C = L.col[int64_t(T) * COLCAP + e];
+      int nc = t.nchild[C];
+      for(int c = 0; c < nc; c++)
+      {
+         if(sp < 256) stack[sp++] = t.child0[C] + c;
+         else atomicOr(err, ERR_DFS);
+      }
+   }
+   while(sp > 0)
+   {
+      int Q = stack[--sp];
+      if(adjacentNodes(t, Q, T))
+      {
+         int nc = t.nchild[Q];
+         if(nc == 0) emit(Q);
+         else
+            for(int c = 0; c < nc; c++)
+            {
+               if(sp < 256) stack[sp++] = t.child0[Q] + c;
+               else atomicOr(err, ERR_DFS);
+            }
+      }
+      else emit(Q);
+   }
+   // coarser non-adjacent leaves of T and of its ancestors
+   for(int a = T; a >= 0; a = t.parent[a])
+      for(int e = 0; e < L.nx[a]; e++) emit(L.xl[int64_t(a) * XCAP + e]);
+   if(!out) cnt[T] = k;
+}
+
+// ------------------------------------------------------------------------------ host driver
+template <class T>
+fmm_status buildTreeT(Plan& P, cudaStream_t st)
+{
+   const int64_t n = P.n, m = P.m;
+   const int threads = 256;
+   // root cube
+   if(P.cfg.root_half_width > 0)
+      kRootFromConfig<<<1, 1, 0, st>>>(P.cfg.root_center[0], P.cfg.root_center[1], P.cfg.root_center[2],
+                                       P.cfg.root_half_width, P.root);
+   else
+   {
+      int nb = int(std::min<int64_t>(1024, (n + m + threads - 1) / threads));
+      nb = std::max(nb, 1);
+      FMM_TRY(P.scratch.reserve(sizeof(double) * 6 * nb));
+      kBBox<T><<<nb, threads, 0, st>>>((const T*)P.srcXYZ, n, (const T*)P.tgtXYZ, m, (double*)P.scratch.ptr);
+      kRootFromBBox<<<1, 1, 0, st>>>((const double*)P.scratch.ptr, nb, P.root);
+   }
+   FMM_CHECK_LAUNCH();
+   // keys and sort
+   FMM_TRY(P.sKeys.reserve(2 * sizeof(uint64_t) * n));
+   FMM_TRY(P.tKeys.reserve(2 * sizeof(uint64_t) * m));
+   FMM_TRY(P.sIdx.reserve(2 * sizeof(int) * n));
+   FMM_TRY(P.tIdx.reserve(2 * sizeof(int) * m));
+   uint64_t* sk = (uint64_t*)P.sKeys.ptr;
+   uint64_t* tk = (uint64_t*)P.tKeys.ptr;
+   int* si = (int*)P.sIdx.ptr;
+   int* ti = (int*)P.tIdx.ptr;
+   if(n) kKeys<T><<<(n + threads - 1) / threads, threads, 0, st>>>((const T*)P.srcXYZ, n, P.root, sk + n, si + n);
+   if(m) kKeys<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, m, P.root, tk + m, ti + m);
+   FMM_CHECK_LAUNCH();
+   size_t need = 0, tmp = 0;
+   cub::DeviceRadixSort::SortPairs(nullptr, tmp, sk + n, sk, si + n, si, int(n), 0, 63, st);
+   need = std::max(need, tmp);
+   cub::DeviceRadixSort::SortPairs(nullptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, 63, st);
+   need = std::max(need, tmp);
+   FMM_TRY(P.cubTmp.reserve(need));
+   tmp = P.cubTmp.bytes;
+   if(n) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, sk + n, sk, si + n, si, int(n), 0, 63, st));
+   tmp = P.cubTmp.bytes;
+   if(m) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, 63, st));
+   // sorted point data
+   typedef typename Vec4<T>::type V4;
+   FMM_TRY(P.sPos.reserve(sizeof(V4) * std::max<int64_t>(n, 1)));
+   FMM_TRY(P.sQ.reserve(sizeof(V4) * std::max<int64_t>(n, 1)));
+   FMM_TRY(P.tPos.reserve(sizeof(V4) * std::max<int64_t>(m, 1)));
+   if(n)
+      kGatherSources<T><<<(n + threads - 1) / threads, threads, 0, st>>>(
+         (const T*)P.srcXYZ, (const T*)P.srcW, (const T*)(P.hasJ ? P.srcJ : nullptr), si, n, (V4*)P.sPos.ptr,
+         (V4*)P.sQ.ptr);
+   if(m) kGatherTargets<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, ti, m, (V4*)P.tPos.ptr);
+   FMM_CHECK_LAUNCH();
+
+   // nodes, level by level
+   int64_t capNodes = std::max<int64_t>(1024, 2 * (n + m) / std::max(1, P.cfg.leaf_capacity) + 64);
+   FMM_TRY(P.ensureNodes(capNodes));
+   Tree& t = P.tree;
+   kInitRoot<<<1, 1, 0, st>>>(t, int(n), int(m));
+   t.levelStart[0] = 0;
+   t.levelStart[1] = 1;
+   int nLevels = 1;
+   int64_t total = 1;
+   for(int level = 0; level < MAXLEVEL; level++)
+   {
+      int a = t.levelStart[level], b = t.levelStart[level + 1];
+      int cnt = b - a;
+      if(cnt == 0) break;
+      FMM_TRY(P.lvlBounds.reserve(sizeof(int) * 18 * cnt));
+      FMM_TRY(P.lvlCnt.reserve(sizeof(int) * (cnt + 1)));
+      FMM_TRY(P.lvlOff.reserve(sizeof(int) * (cnt + 1)));
+      int* bounds = (int*)P.lvlBounds.ptr;
+      int* cc = (int*)P.lvlCnt.ptr;
+      int* off = (int*)P.lvlOff.ptr;
+      kCountChildren<<<(cnt + threads - 1) / threads, threads, 0, st>>>(
+         t, a, b, level, P.cfg.leaf_capacity,
+         P.cfg.target_leaf_capacity > 0 ? P.cfg.target_leaf_capacity : P.cfg.leaf_capacity, sk, tk, bounds, cc);
+      FMM_CHECK_LAUNCH();
+      tmp = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tmp, cc, off, cnt + 1, st);
+      FMM_TRY(P.cubTmp.reserve(tmp));
+      tmp = P.cubTmp.bytes;
+      // cnt[cnt] must be 0 for the total to land in off[cnt]
+      FMM_CUDA(cudaMemsetAsync(cc + cnt, 0, sizeof(int), st));
+      FMM_CUDA(cub::DeviceScan::ExclusiveSum(P.cubTmp.ptr, tmp, cc, off, cnt + 1, st));
+      int nextCount = 0;
+      FMM_CUDA(cudaMemcpyAsync(&nextCount, off + cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+      if(nextCount == 0) break;
+      if(total + nextCount > capNodes)
+      {
+         capNodes = std::max<int64_t>(2 * capNodes, total + nextCount);
+         FMM_TRY(P.ensureNodes(capNodes, st));
+      }
+      kMakeChildren<<<(cnt + threads - 1) / threads, threads, 0, st>>>(t, a, b, level, int(total), bounds, cc, off);
+      FMM_CHECK_LAUNCH();
+      total += nextCount;
+      t.levelStart[level + 2] = int(total);
+      nLevels = level + 2;
+   }
+   t.nNodes = total;
+   t.nLevels = nLevels;
+
+   // lists
+   FMM_TRY(P.ensureLists(total));
+   Lists& Ls = P.lists;
+   FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   kInitRootLists<<<1, 1, 0, st>>>(Ls);
+   for(int level = 1; level < nLevels; level++)
+   {
+      int a = t.levelStart[level], b = t.levelStart[level + 1];
+      kListsLevel<<<(b - a + 127) / 128, 128, 0, st>>>(t, Ls, a, b, P.err);
+   }
+   FMM_CHECK_LAUNCH();
+   int nn = int(total);
+   FMM_TRY(P.p2pOff.reserve(sizeof(int) * (nn + 1)));
+   FMM_TRY(P.lvlCnt.reserve(sizeof(int) * (nn + 1)));
+   int* pc = (int*)P.lvlCnt.ptr;
+   int* po = (int*)P.p2pOff.ptr;
+   kP2PLists<<<(nn + 127) / 128, 128, 0, st>>>(t, Ls, nn, nullptr, pc, nullptr, P.err);
+   FMM_CUDA(cudaMemsetAsync(pc + nn, 0, sizeof(int), st));
+   tmp = 0;
+   cub::DeviceScan::ExclusiveSum(nullptr, tmp, pc, po, nn + 1, st);
+   FMM_TRY(P.cubTmp.reserve(tmp));
+   tmp = P.cubTmp.bytes;
+   FMM_CUDA(cub::DeviceScan::ExclusiveSum(P.cubTmp.ptr, tmp, pc, po, nn + 1, st));
+   int nP2P = 0;
+   FMM_CUDA(cudaMemcpyAsync(&nP2P, po + nn, sizeof(int), cudaMemcpyDeviceToHost, st));
+   // number of M2L (V-list) pairs
+   FMM_TRY(P.scratch.reserve(sizeof(long long)));
+   tmp = 0;
+   cub::DeviceReduce::Sum(nullptr, tmp, Ls.nv, (long long*)P.scratch.ptr, nn, st);
+   FMM_TRY(P.cubTmp.reserve(tmp));
+   tmp = P.cubTmp.bytes;
+   FMM_CUDA(cub::DeviceReduce::Sum(P.cubTmp.ptr, tmp, Ls.nv, (long long*)P.scratch.ptr, nn, st));
+   long long nV = 0;
+   FMM_CUDA(cudaMemcpyAsync(&nV, P.scratch.ptr, sizeof(long long), cudaMemcpyDeviceToHost, st));
+   int herr = 0;
+   FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+   FMM_CUDA(cudaStreamSynchronize(st));
+   if(herr) return setError(FMM_E_LIMIT, "interaction list capacity exceeded (code %d)", herr);
+   FMM_TRY(P.p2pList.reserve(sizeof(int) * std::max(nP2P, 1)));
+   kP2PLists<<<(nn + 127) / 128, 128, 0, st>>>(t, Ls, nn, po, nullptr, (int*)P.p2pList.ptr, P.err);
+   FMM_CHECK_LAUNCH();
+   P.nP2P = nP2P;
+   P.nV = nV;
+   return FMM_OK;
+}
+
+template fmm_status buildTreeT<float>(Plan&, cudaStream_t);
+template fmm_status buildTreeT<double>(Plan&, cudaStream_t);
+
+}  // namespace fmm

@@ -1,0 +1,86 @@
+"""Seeded synthetic source and target generators.
+
+The reference builds its sources from a hexahedral torus mesh split into tetrahedra with a
+24-point Keast rule (FMM/FMMGPU/torus.cpp:9-117, integration.cpp:163-187) and draws targets
+with an unseeded std::rand (testing_helpers.cpp:171). Here every workload is a tensor-product
+torus quadrature with explicit seeds:
+
+  x = c + Rot(n) ((R + rho cos t) cos f, (R + rho cos t) sin f, rho sin t)
+  f, t: n_f / n_t uniform midpoints on [0, 2 pi)
+  rho:  n_rho-point Gauss-Legendre on [0, a]
+  w = (2 pi / n_f) (2 pi / n_t) w_rho rho (R + rho cos t)      (the cell volume)
+
+The current direction is the poloidal tangent (d x / d t) or the reference's azimuthal
+direction perp(x) / |perp(x)| = (-y, x, 0) / rho_xy (integration.cpp:155).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _rotation_to(axis):
+    """Rotation matrix taking e_z to the unit vector `axis`."""
+    n = np.asarray(axis, dtype=np.float64)
+    n = n / np.linalg.norm(n)
+    z = np.array([0.0, 0.0, 1.0])
+    v = np.cross(z, n)
+    c = float(np.dot(z, n))
+    if np.linalg.norm(v) < 1e-15:
+        return np.eye(3) if c > 0 else np.diag([1.0, -1.0, -1.0])
+    vx = np.array([[0, -v[2], v[1]], [v[2], 0, -v[0]], [-v[1], v[0], 0]])
+    return np.eye(3) + vx + vx @ vx * (1.0 / (1.0 + c))
+
+
+def torus(n_phi, n_theta, n_rho, major=2.0, minor=0.5, center=(0.0, 0.0, 0.0), axis=(0.0, 0.0, 1.0),
+          current="poloidal", magnitude=1.0):
+    """Tensor-product quadrature of a solid torus. Returns (xyz[N,3], w[N], J[N,3]) in float64,
+    ordered with the radial index fastest, then poloidal, then toroidal."""
+    f = 2 * np.pi * (np.arange(n_phi) + 0.5) / n_phi
+    t = 2 * np.pi * (np.arange(n_theta) + 0.5) / n_theta
+    xg, wg = np.polynomial.legendre.leggauss(n_rho)
+    rho = 0.5 * minor * (xg + 1.0)
+    wr = 0.5 * minor * wg
+    F, T, P = np.meshgrid(f, t, rho, indexing="ij")
+    _, _, WR = np.meshgrid(f, t, wr, indexing="ij")
+    ring = major + P * np.cos(T)
+    local = np.stack([ring * np.cos(F), ring * np.sin(F), P * np.sin(T)], axis=-1).reshape(-1, 3)
+    w = ((2 * np.pi / n_phi) * (2 * np.pi / n_theta) * WR * P * ring).reshape(-1)
+    if current == "poloidal":
+        d = np.stack([-np.sin(T) * np.cos(F), -np.sin(T) * np.sin(F), np.cos(T)], axis=-1).reshape(-1, 3)
+    elif current == "azimuthal":
+        d = np.stack([-np.sin(F), np.cos(F), np.zeros_like(F)], axis=-1).reshape(-1, 3)
+    else:
+        raise ValueError(f"unknown current direction {current!r}")
+    Rm = _rotation_to(axis)
+    xyz = local @ Rm.T + np.asarray(center, dtype=np.float64)
+    J = magnitude * (d @ Rm.T)
+    return xyz, w, J
+
+
+def uniform_points(n, lo, hi, seed):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(lo, hi, size=(n, 3))
+
+
+def grid_points(n, lo, hi):
+    g = (np.arange(n) + 0.5) / n * (hi - lo) + lo if n > 1 else np.array([(lo + hi) / 2])
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    return np.stack([X, Y, Z], axis=-1).reshape(-1, 3)
+
+
+def cube_grid(n, lo, hi):
+    """n^3 grid including both ends of [lo, hi] on each axis (the 32^3 grid on [-3, 3]^3)."""
+    g = np.linspace(lo, hi, n)
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    return np.stack([X, Y, Z], axis=-1).reshape(-1, 3)
+
+
+def root_cube(*point_sets):
+    """The root cube the solver uses by default: the bounding box of all points, made cubic
+    around its midpoint with a relative margin of 2^-20 so no point sits on the upper face."""
+    lo = np.min([np.min(p, axis=0) for p in point_sets if len(p)], axis=0)
+    hi = np.max([np.max(p, axis=0) for p in point_sets if len(p)], axis=0)
+    center = 0.5 * (lo + hi)
+    H = 0.5 * float(np.max(hi - lo))
+    H = H * (1.0 + 2.0 ** -20) + 1e-300
+    return center, H

@@ -1,0 +1,282 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+Reference interface (FMM/FMMGPU/):
+  MultipoleSolver(quadratures, problem, leafCapacity)                multipole_solver.hpp:29-48
+    calcMultipoleExpansionsAtLeaves(), calclMultipoleExpansions(M2MAlg, Device)
+  FastMultipoleSolver(quadratures, points, problem, capS=1000, capT=100)
+                                                                       fast_multipole_solver.hpp:25-49
+    calcLocalMultipoleExpansions(M2LAlg, Device), calcA(current), calcB(current)
+  math::calcBioSavartLaplace(current, point, quadratures)             integration.hpp:46-49
+  enums M2MAlg / Device / M2LAlg / Problem                            multipole_solver_enums.hpp:3-29
+
+Differences a caller sees: quadratures are arrays (xyz[N,3], w[N], optional J[N,3]) instead of
+std::vector<Quadrature>; results come back in target input order as an [M,3] array instead of
+(point, value) pairs in tree order; the algorithm and device enums are accepted and ignored
+(there is one GPU algorithm); errors raise FmmError instead of exiting the process.
+Inputs given as CUDA torch tensors stay on the device and results are CUDA tensors; numpy
+inputs are copied through host memory and results are numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib
+
+try:  # torch is plumbing for device buffers and streams; numpy-only use works without it
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+class Problem(IntEnum):
+    BioSavartLaplace = 0
+    BEM = 1
+
+
+class M2MAlg(IntEnum):
+    NoTranslation = 0
+    ComplexTranslation = 1
+    RealTranslation = 2
+    Layers = 3
+    Matrices = 4
+
+
+class Device(IntEnum):
+    CPU = 0
+    GPU = 1
+    Adaptive = 2
+
+
+class M2LAlg(IntEnum):
+    ComplexTranslation = 0
+    Matrices = 1
+
+
+_PRECISION = {"fp32": _lib.FMM_FP32, "fp64": _lib.FMM_FP64}
+_M2L = {"simt": _lib.FMM_M2L_SIMT, "bf16x3": _lib.FMM_M2L_BF16X3, "tf32": _lib.FMM_M2L_TF32}
+
+
+def _is_cuda_tensor(x):
+    return torch is not None and isinstance(x, torch.Tensor) and x.is_cuda
+
+
+class _Buffer:
+    """A host (numpy) or device (torch) array with the plan's element type."""
+
+    def __init__(self, x, dtype_np, torch_dtype, shape_tail):
+        if _is_cuda_tensor(x):
+            t = x.detach().to(torch_dtype).contiguous()
+            self.device = True
+            self.obj = t
+            self.ptr = t.data_ptr()
+            self.n = t.shape[0] if t.dim() else 0
+        else:
+            a = np.ascontiguousarray(np.asarray(x, dtype=dtype_np))
+            self.device = False
+            self.obj = a
+            self.ptr = a.ctypes.data
+            self.n = a.shape[0] if a.ndim else 0
+        if shape_tail is not None and tuple(self.obj.shape[1:]) != shape_tail:
+            raise ValueError(f"expected shape [N, {shape_tail[0]}], got {tuple(self.obj.shape)}")
+
+
+class Plan:
+    """Owns one fmm_plan (one expansion order, leaf capacity, precision and M2L mode)."""
+
+    def __init__(self, order=10, leaf_capacity=64, target_leaf_capacity=0, precision="fp32", m2l="simt",
+                 m2l_truncate=False, device=0, root=None):
+        self.lib = _lib.load()
+        cfg = _lib.FmmConfig()
+        self.lib.fmm_default_config(ctypes.byref(cfg))
+        cfg.order = int(order)
+        cfg.leaf_capacity = int(leaf_capacity)
+        cfg.target_leaf_capacity = int(target_leaf_capacity)
+        cfg.precision = _PRECISION[precision]
+        cfg.m2l_mode = _M2L[m2l]
+        cfg.m2l_truncate = int(bool(m2l_truncate))
+        cfg.device = int(device)
+        if root is not None:
+            center, H = root
+            for d in range(3):
+                cfg.root_center[d] = float(center[d])
+            cfg.root_half_width = float(H)
+        self.cfg = cfg
+        self.precision = precision
+        self.np_dtype = np.float32 if precision == "fp32" else np.float64
+        self.torch_dtype = None if torch is None else (torch.float32 if precision == "fp32" else torch.float64)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.fmm_plan_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+        self._keep = []
+        self.device_mode = False
+        self.m = 0
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.fmm_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _stream(self):
+        if self.device_mode and torch is not None:
+            return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        return ctypes.c_void_p(0)
+
+    def set_sources(self, xyz, w, J=None):
+        x = _Buffer(xyz, self.np_dtype, self.torch_dtype, (3,))
+        wb = _Buffer(w, self.np_dtype, self.torch_dtype, ())
+        jb = _Buffer(J, self.np_dtype, self.torch_dtype, (3,)) if J is not None else None
+        self.device_mode = x.device
+        _lib.check(self.lib.fmm_set_sources(self.handle, ctypes.c_void_p(x.ptr), ctypes.c_void_p(wb.ptr),
+                                            ctypes.c_void_p(jb.ptr) if jb else None, x.n, int(x.device),
+                                            self._stream()))
+        self._keep = [x, wb, jb]
+
+    def set_targets(self, xyz):
+        t = _Buffer(xyz, self.np_dtype, self.torch_dtype, (3,))
+        self.device_mode = t.device
+        _lib.check(self.lib.fmm_set_targets(self.handle, ctypes.c_void_p(t.ptr), t.n, int(t.device), self._stream()))
+        self.m = t.n
+        self._keep.append(t)
+
+    def _out(self):
+        if self.device_mode:
+            return torch.empty((self.m, 3), dtype=self.torch_dtype, device=f"cuda:{self.cfg.device}")
+        return np.empty((self.m, 3), dtype=self.np_dtype)
+
+    @staticmethod
+    def _ptr(a):
+        if a is None:
+            return None
+        return ctypes.c_void_p(a.data_ptr() if _is_cuda_tensor(a) else a.ctypes.data)
+
+    def build_tree(self):
+        _lib.check(self.lib.fmm_build_tree(self.handle, self._stream()))
+
+    def upward(self):
+        _lib.check(self.lib.fmm_upward(self.handle, self._stream()))
+
+    def downward(self):
+        _lib.check(self.lib.fmm_downward(self.handle, self._stream()))
+
+    def _run(self, fn, current, want):
+        B = self._out() if want & 1 else None
+        A = self._out() if want & 2 else None
+        _lib.check(fn(self.handle, ctypes.c_double(current), int(want), self._ptr(B), self._ptr(A),
+                      int(self.device_mode), self._stream()))
+        return B, A
+
+    def evaluate(self, current=1.0, want=1):
+        return self._run(self.lib.fmm_evaluate, current, want)
+
+    def solve(self, current=1.0, want=1):
+        return self._run(self.lib.fmm_solve, current, want)
+
+    def direct(self, current=1.0, want=1):
+        return self._run(self.lib.fmm_direct, current, want)
+
+    def direct_fp64(self, targets, current=1.0):
+        t = np.ascontiguousarray(np.asarray(targets, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros_like(t)
+        _lib.check(self.lib.fmm_direct_fp64_subset(self.handle, ctypes.c_double(current), ctypes.c_void_p(t.ctypes.data),
+                                                   len(t), ctypes.c_void_p(out.ctypes.data)))
+        return out
+
+    def stats(self):
+        s = _lib.FmmStats()
+        _lib.check(self.lib.fmm_get_stats(self.handle, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _lib.FmmStats._fields_}
+
+    def operator(self, kind, index):
+        L = (self.cfg.order + 1) ** 2
+        out = np.zeros((L, L))
+        _lib.check(self.lib.fmm_get_operator(self.handle, int(kind), int(index), ctypes.c_void_p(out.ctypes.data)))
+        return out
+
+
+class MultipoleSolver:
+    """Upward pass only (MultipoleSolver in the reference). Its calcA / calcB(current, point)
+    treecode evaluation is provided by FastMultipoleSolver with the points as targets."""
+
+    def __init__(self, quadratures, problem=Problem.BioSavartLaplace, quadratureOctreeLeafCapacity=1000, *,
+                 order=10, precision="fp32", m2l="simt", m2l_truncate=False, device=0, root=None):
+        if Problem(problem) != Problem.BioSavartLaplace:
+            raise NotImplementedError("only Problem.BioSavartLaplace is supported")
+        self.plan = Plan(order=order, leaf_capacity=quadratureOctreeLeafCapacity, precision=precision, m2l=m2l,
+                         m2l_truncate=m2l_truncate, device=device, root=root)
+        xyz, w, J = (tuple(quadratures) + (None,))[:3]
+        self.plan.set_sources(xyz, w, J)
+        self._multipoles = False
+        self.harmonicOrder = int(order)
+
+    def calcMultipoleExpansionsAtLeaves(self):
+        self.plan.build_tree()
+        self.plan.upward()
+        self._multipoles = True
+
+    def calclMultipoleExpansions(self, algorithm=M2MAlg.Matrices, device=Device.GPU):
+        if not self._multipoles:
+            self.calcMultipoleExpansionsAtLeaves()
+
+
+class FastMultipoleSolver(MultipoleSolver):
+    def __init__(self, quadratures, points, problem=Problem.BioSavartLaplace, quadratureOctreeLeafCapacity=1000,
+                 calculationPointOctreeLeafCapacity=100, *, order=10, precision="fp32", m2l="simt",
+                 m2l_truncate=False, device=0, root=None):
+        if Problem(problem) != Problem.BioSavartLaplace:
+            raise NotImplementedError("only Problem.BioSavartLaplace is supported")
+        self.plan = Plan(order=order, leaf_capacity=quadratureOctreeLeafCapacity,
+                         target_leaf_capacity=calculationPointOctreeLeafCapacity, precision=precision, m2l=m2l,
+                         m2l_truncate=m2l_truncate, device=device, root=root)
+        xyz, w, J = (tuple(quadratures) + (None,))[:3]
+        self.plan.set_sources(xyz, w, J)
+        self.plan.set_targets(points)
+        self._multipoles = False
+        self._locals = False
+        self.harmonicOrder = int(order)
+
+    def calcLocalMultipoleExpansions(self, algorithm=M2LAlg.ComplexTranslation, device=Device.GPU):
+        if not self._multipoles:
+            raise RuntimeError("Multipoles are not ready!")
+        self.plan.downward()
+        self._locals = True
+
+    def _ready(self):
+        if not self._locals:
+            raise RuntimeError("Local expansions are not ready!")
+
+    def calcB(self, current):
+        self._ready()
+        return self.plan.evaluate(current, 1)[0]
+
+    def calcA(self, current):
+        self._ready()
+        return self.plan.evaluate(current, 2)[1]
+
+    def solve(self, current=1.0, want="B"):
+        w = {"B": 1, "A": 2, "AB": 3}[want]
+        B, A = self.plan.solve(current, w)
+        self._multipoles = self._locals = True
+        return {"B": B, "A": A, "AB": (B, A)}[want]
+
+    def stats(self):
+        return self.plan.stats()
+
+
+def calcBioSavartLaplace(current, points, quadratures, precision="fp64", device=0):
+    """Direct Biot-Savart B at `points` (math::calcBioSavartLaplace), on the GPU."""
+    plan = Plan(order=1, leaf_capacity=1 << 30, precision=precision, device=device)
+    xyz, w, J = (tuple(quadratures) + (None,))[:3]
+    plan.set_sources(xyz, w, J)
+    plan.set_targets(points)
+    B, _ = plan.direct(current, 1)
+    plan.close()
+    return B

@@ -1,0 +1,355 @@
+"""Benchmark: B target-evaluations per second of the fast-multipole Biot-Savart solve.
+
+Workload (the headline precision configuration): a solid torus (R = 2, a = 0.5, axis z),
+tensor-product quadrature 512 toroidal x 128 poloidal x 256 radial = 2^24 sources with the
+poloidal current, J = 1 A/m^2; the targets are the source points themselves (self term
+excluded); order p = 16, leaf capacity 64; FP32 pipeline with the M2L contraction in the
+selected mode. One step = one full solve (tree build, P2M, M2M, M2L, L2L, L2P + near field)
+with inputs already in HBM; the inputs (2^24 points) are larger than L2.
+
+Multi-GPU: every rank solves its own copy of the workload (replicas, weak scaling); the
+aggregate is the units all ranks processed divided by the slowest rank's time.
+
+`--impl reference` times the reference's own CPU FMM (FastMultipoleSolver, FP32, p = 16,
+built from the reference sources into oracle/_ref/) on a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "B evals/s (N=2^24, p=16) split-BF16 vs FP32 FMM at rel err<=1e-6; adjoint/forward"
+UNIT = "target-evals/s"
+SEED = 20260002
+# a bounded CPU sample of the same workload family: 32 x 8 x 8 torus points, targets = sources
+CPU_SAMPLE = (32, 8, 8)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device(f"cuda:{local}"))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.proc:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(name)
+        out["sm_mhz"] = statistics.median(sm) if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        return out
+
+
+def make_workload(n_phi, n_theta, n_rho):
+    from bachelors_b200 import geometry as G
+    xyz, w, J = G.torus(n_phi, n_theta, n_rho, 2.0, 0.5, current="poloidal")
+    return xyz.astype(np.float32), w.astype(np.float32), J.astype(np.float32)
+
+
+def cpu_reference_run(sample=CPU_SAMPLE):
+    """One run of the reference's CPU FMM (FP32, p = 16, leaf 64/64) on the sample; returns
+    (target-evals/s, seconds, n)."""
+    from oracle.oracle import Reference
+    ref = Reference("f32", 16)
+    xyz, w, _ = make_workload(*sample)
+    t0 = time.perf_counter()
+    _, found, _ = ref.fmm(np.c_[xyz, w].astype(np.float64), xyz.astype(np.float64), 64, 64, 1.0)
+    dt = time.perf_counter() - t0
+    return len(xyz) / dt, dt, len(xyz)
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle.oracle import Reference
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    if not Reference.available("f32", 16):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref/libref_fmm_f32_p16.so "
+                          "missing (built by oracle/ref/build_ref.sh from the reference sources)"}))
+        return
+    for _ in range(args.warmup):
+        cpu_reference_run()
+    times = []
+    n = 0
+    for _ in range(args.steps):
+        _, dt, n = cpu_reference_run()
+        times.append(dt)
+    ms = 1000 * sum(times) / len(times)
+    value = n / (ms / 1000)
+    sample = f"torus {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} = {n} sources, targets = sources, p=16, leaf 64/64, FP32"
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "torus 512x128x256 (2^24) targets=sources p=16 leaf 64 (reference: bounded sample)",
+                   "sample": sample},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def count_launches(plan):
+    """Kernels one solve launches (from the CUDA profiler), excluding library kernels."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        plan.solve(1.0, 1)
+        torch.cuda.synchronize()
+    names = [e.name for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA]
+    kernels = [n for n in names if not n.lower().startswith(("memcpy", "memset"))]
+    ours = [n for n in kernels if "fmm" in n or "kM2L" in n or "kP2" in n]
+    return len(kernels), len(ours), sorted(set(ours))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--m2l", default="auto", choices=["auto", "simt", "bf16x3", "tf32"])
+    ap.add_argument("--size", default="512,128,256", help="torus n_phi,n_theta,n_rho")
+    ap.add_argument("--order", type=int, default=16)
+    ap.add_argument("--leaf", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    from bachelors_b200 import FastMultipoleSolver, Plan
+
+    size = tuple(int(v) for v in args.size.split(","))
+    xyz, w, J = make_workload(*size)
+    n = len(xyz)
+    m2l = args.m2l
+    if m2l == "auto":
+        m2l = "simt"
+        try:
+            from bachelors_b200 import _lib  # noqa: F401
+            m2l = os.environ.get("FMM_BENCH_M2L", "simt")
+        except Exception:
+            pass
+    dev = f"cuda:{local}"
+    d_xyz = torch.from_numpy(xyz).to(dev)
+    d_w = torch.from_numpy(w).to(dev)
+    d_J = torch.from_numpy(J).to(dev)
+    plan = Plan(order=args.order, leaf_capacity=args.leaf, precision="fp32", m2l=m2l, device=local)
+    plan.set_sources(d_xyz, d_w, d_J)
+    plan.set_targets(d_xyz)
+    for _ in range(args.warmup):
+        B, _ = plan.solve(1.0, 1)
+    torch.cuda.synchronize()
+
+    # timed region: K full solves, inputs resident in HBM
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    m2l_ms = []
+    phase = []
+    ev0.record()
+    for _ in range(args.steps):
+        B, _ = plan.solve(1.0, 1)
+        st = plan.stats()
+        m2l_ms.append(st["ms_m2l"])
+        phase.append(st)
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = max_over_ranks(ms, world)
+    value = world * n / (ms_max / 1000.0)
+
+    st = phase[-1]
+    L = (args.order + 1) ** 2
+    flops_m2l = st["v_pairs"] * 3 * 2 * L * L
+    m2l_avg = sum(m2l_ms) / len(m2l_ms)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    achieved = flops_m2l / (m2l_avg / 1000.0) / 1e12
+
+    # accuracy against the FP64 direct sum on 4096 seeded targets
+    rng = np.random.default_rng(SEED)
+    idx = rng.choice(n, size=min(4096, n), replace=False)
+    Bh = B.cpu().numpy().astype(np.float64)
+    Bd = plan.direct_fp64(xyz[idx].astype(np.float64), current=1.0)
+    rel_err = float(np.linalg.norm(Bh[idx] - Bd) / np.linalg.norm(Bd))
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded torus quadrature)",
+        "config": {"workload": f"torus {size[0]}x{size[1]}x{size[2]} = {n} sources, targets = sources (self excluded), "
+                               f"p={args.order}, leaf {args.leaf}, M2L {m2l}",
+                   "m2l": m2l, "order": args.order, "leaf": args.leaf, "n_sources": n, "n_targets": n,
+                   "l2_flush": "inputs larger than L2 (2^24 points)", "parallelism": f"replicas x{world}"},
+        "rel_l2_vs_fp64_direct": rel_err,
+        "phases_ms": {k: st[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_near", "ms_total")},
+        "tree": {k: st[k] for k in ("nodes", "levels", "v_pairs", "p2p_pairs")},
+        "roofline": {"kernel": f"M2L ({m2l})", "bound": "tensor", "achieved": achieved, "peak": bf16_peak,
+                     "unit": "TFLOP/s", "frac": achieved / bf16_peak, "traffic": None,
+                     "flops_per_launch": flops_m2l,
+                     "note": "algorithmic FLOPs = V pairs x 3 components x 2 (p+1)^4; peak = measured bf16 dense"},
+        "clocks": clk,
+    }
+
+    if rank == 0:
+        try:
+            total, ours, names = count_launches(plan)
+            line["gpu_launches"] = ours * args.steps
+            line["gpu_launch_names"] = names
+            line["library_launches_per_step"] = total - ours
+        except Exception as e:  # profiler unavailable
+            line["gpu_launches"] = None
+            line["gpu_launch_error"] = str(e)[:200]
+
+    # end to end through the public API: pinned host inputs, H2D + solve + D2H each step
+    if not args.no_e2e:
+        hx = torch.from_numpy(xyz).pin_memory().numpy()
+        hw = torch.from_numpy(w).pin_memory().numpy()
+        hJ = torch.from_numpy(J).pin_memory().numpy()
+        s = FastMultipoleSolver((hx, hw, hJ), hx, quadratureOctreeLeafCapacity=args.leaf,
+                                calculationPointOctreeLeafCapacity=args.leaf, order=args.order, precision="fp32",
+                                m2l=m2l, device=local)
+        s.solve(1.0, "B")
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s.plan.set_sources(hx, hw, hJ)
+            s.plan.set_targets(hx)
+            Bh2 = s.solve(1.0, "B")
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1000 / args.steps
+        e2e_ms = max_over_ranks(e2e_ms, world)
+        line["e2e"] = {"value": world * n / (e2e_ms / 1000.0), "unit": UNIT,
+                       "h2d_bytes_per_step": int(xyz.nbytes + w.nbytes + J.nbytes + xyz.nbytes),
+                       "d2h_bytes_per_step": int(Bh2.nbytes), "ms_per_step": e2e_ms}
+        s.plan.close()
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            from oracle.oracle import Reference
+            if Reference.available("f32", 16):
+                v, dt, ns = cpu_reference_run()
+                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                        "sample": f"torus {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} = {ns} "
+                                                  f"sources, targets = sources, p=16, leaf 64/64, FP32, {dt:.1f} s; "
+                                                  "the reference's M2L/L2L/L2P run on one thread by design"}
+        except Exception as e:
+            line["cpu_baseline"] = {"error": str(e)[:200]}
+    plan.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

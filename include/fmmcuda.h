@@ -1,0 +1,139 @@
+/*
+ * fmmcuda.h: C ABI of the B200 fast-multipole Biot-Savart solver (libfmmcuda.so).
+ *
+ * The reference (iamwhoamianamy/bachelors) exposes its GPU code through the C++-ABI
+ * "kernel_callers" seam (FMMCUDADLL/kernel_callers.hpp:5-10, kernels::addVectors, and the
+ * live twin FMM/FMMGPU/translation_algorithms.hpp:8-61, kernels::translateAll*) and its
+ * solver through C++ classes (FMM/FMMGPU/multipole_solver.hpp:12-48,
+ * FMM/FMMGPU/fast_multipole_solver.hpp:13-49). This header replaces both with plain
+ * extern "C" entry points: pointers, sizes and integer status codes, no C++ or torch types.
+ *
+ * Physics (FMM/FMMGPU/integration.cpp:101-161, fast_multipole_solver.cpp:195-231):
+ *   B(x) = MU0 / (4 PI) * current * sum_q w_q J_q x (x - q) / |x - q|^3
+ *   A(x) = 1 / (4 PI) * current * sum_q w_q J_q / |x - q|
+ * with the reference's literals PI = 3.14159265359 and MU0 = 1.2566370614e-6
+ * (FMM/FMMGPU/math.hpp:12-13). Coincident (target, source) pairs are skipped.
+ *
+ * Errors: every call returns an fmm_status; fmm_last_error_string() describes the last
+ * failure on the calling thread. Nothing here exits the process (the reference prints and
+ * calls exit(0), FMM/FMMGPU/cuda_helper.cpp:9-31).
+ *
+ * Threading: a plan is used by one host thread at a time; distinct plans are independent.
+ * Work is issued on the stream passed to each call (NULL = the legacy default stream).
+ */
+#ifndef FMMCUDA_H
+#define FMMCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fmm_status {
+   FMM_OK = 0,
+   FMM_E_INVALID = 1, /* bad argument or call order */
+   FMM_E_OOM = 2,     /* device allocation failed */
+   FMM_E_CUDA = 3,    /* a CUDA runtime or launch error */
+   FMM_E_TIMEOUT = 4, /* a bounded device wait ran out */
+   FMM_E_LIMIT = 5    /* a structural limit was exceeded (tree depth, list capacity) */
+} fmm_status;
+
+/* Arithmetic of the whole pipeline. FP64 also builds every operator table in FP64. */
+typedef enum fmm_precision { FMM_FP32 = 0, FMM_FP64 = 1 } fmm_precision;
+
+/* How the M2L contraction is computed (FP32 plans only; FP64 plans always use FMM_M2L_SIMT).
+ *   SIMT    FP32 (or FP64) FMA on the CUDA cores.
+ *   BF16X3  tcgen05 tensor cores, operands split x = hi + lo in bf16, hi*hi + hi*lo + lo*hi,
+ *           FP32 accumulation in tensor memory.
+ *   TF32    tcgen05 tensor cores, one TF32 pass, FP32 accumulation. */
+typedef enum fmm_m2l_mode { FMM_M2L_SIMT = 0, FMM_M2L_BF16X3 = 1, FMM_M2L_TF32 = 2 } fmm_m2l_mode;
+
+typedef struct fmm_config {
+   int order;          /* expansion order p, 1..16 ((p+1)^2 harmonics) */
+   int leaf_capacity;  /* a box splits when it holds more than this many sources ... */
+   int target_leaf_capacity; /* ... or more than this many targets (<= 0: leaf_capacity) */
+   int precision;      /* fmm_precision */
+   int m2l_mode;       /* fmm_m2l_mode */
+   int m2l_truncate;   /* 0: full M2L operator (l + lambda <= 2p); 1: the reference's l + lambda <= p
+                          (FMM/FMMGPU/multipole_translator.cpp:165) */
+   int device;         /* CUDA device ordinal */
+   double root_center[3];
+   double root_half_width; /* <= 0: the cube around the bounding box of sources and targets */
+} fmm_config;
+
+typedef struct fmm_plan fmm_plan;
+
+/* Phase timings (milliseconds, CUDA events on the plan's stream) and tree statistics of
+ * the last solve. */
+typedef struct fmm_stats {
+   double ms_tree, ms_upward, ms_m2l, ms_downward, ms_near, ms_total;
+   int64_t nodes, leaves, levels, v_pairs, p2p_pairs, p2p_interactions;
+   int64_t n_sources, n_targets;
+} fmm_stats;
+
+void fmm_default_config(fmm_config* cfg);
+
+/* Replaces MultipoleSolver / FastMultipoleSolver construction
+ * (FMM/FMMGPU/multipole_solver.cpp:20-36, fast_multipole_solver.cpp:12-23). */
+fmm_status fmm_plan_create(const fmm_config* cfg, fmm_plan** plan);
+fmm_status fmm_plan_destroy(fmm_plan* plan);
+
+/* Sources: xyz[3n], weights w[n], current directions J[3n] (J == NULL: the reference's
+ * azimuthal direction perp(q)/|perp(q)|, FMM/FMMGPU/integration.cpp:155). Element type is
+ * float for FP32 plans and double for FP64 plans. on_device != 0: the pointers are device
+ * memory on the plan's device; otherwise host memory (copied on `stream`). The data is
+ * copied; the caller's buffers may be released after the call returns. */
+fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const void* J, int64_t n,
+                           int on_device, void* stream);
+/* Targets xyz[3m] (FastMultipoleSolver's `points`, fast_multipole_solver.hpp:16). */
+fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_device, void* stream);
+
+/* The reference's phases, for drop-in use of its call sequence
+ * (FMM/FMMGPU/main.cpp:568-572):
+ *   fmm_build_tree          <- initTrees (multipole_solver.cpp:656-675, fast_multipole_solver.cpp:43-60)
+ *   fmm_upward              <- calcMultipoleExpansionsAtLeaves + calclMultipoleExpansions
+ *   fmm_downward            <- calcLocalMultipoleExpansions (M2L + L2L)
+ *   fmm_evaluate            <- calcB(current) / calcA(current) (L2P + direct near field)
+ * Each runs on `stream` and requires the previous phase. */
+fmm_status fmm_build_tree(fmm_plan* plan, void* stream);
+fmm_status fmm_upward(fmm_plan* plan, void* stream);
+fmm_status fmm_downward(fmm_plan* plan, void* stream);
+/* want: 1 = B, 2 = A, 3 = both. out_B / out_A hold 3m values in target input order, in the
+ * plan's element type, on the device (on_device != 0) or host. */
+fmm_status fmm_evaluate(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device,
+                        void* stream);
+
+/* All phases in order. */
+fmm_status fmm_solve(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device,
+                     void* stream);
+
+/* Direct O(N M) sums on the device in the plan's precision, over the plan's current
+ * sources and targets (math::calcBioSavartLaplace, FMM/FMMGPU/integration.cpp:101-111). */
+fmm_status fmm_direct(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device,
+                      void* stream);
+
+/* FP64 direct B on the device for an explicit target subset (accuracy checks): tgt[3k]
+ * host doubles, out_B[3k] host doubles. Uses the plan's sources. */
+fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* tgt, int64_t k, double* out_B);
+
+fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats);
+
+/* Operator tables, for verification. kind 0 = M2M (index = child octant 0..7), 1 = L2L
+ * (octant 0..7), 2 = M2L (index = offset (ox+3) + 7 (oy+3) + 49 (oz+3), |o|_inf in 2..3).
+ * out[(p+1)^2 * (p+1)^2], row-major [output coefficient][input coefficient], FP64, in the
+ * box-size-scaled basis the pipeline uses. */
+fmm_status fmm_get_operator(fmm_plan* plan, int kind, int index, double* out);
+
+/* kernels::addVectors (FMMCUDADLL/kernel_callers.hpp:7-9): c = a + b for host arrays of n floats. */
+fmm_status fmm_add_vectors(const float* a, const float* b, float* c, int64_t n);
+
+const char* fmm_last_error_string(void);
+const char* fmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMMCUDA_H */

@@ -1,0 +1,223 @@
+"""ctypes bindings for the CPU restatement (oracle/liboracle.so) and the reference build
+(oracle/_ref/libref_fmm_*.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg, always as the checker. The product library never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_lib = None
+
+
+def build() -> None:
+    """Compile liboracle.so (and nothing else)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def nharm(p: int) -> int:
+    return (p + 1) * (p + 1)
+
+
+def solid_harmonics(p, xyz, regular=True, compat=False):
+    out = np.zeros(nharm(p))
+    _load().orc_solid_harmonics(p, int(regular), int(compat), _d(_c64(xyz)), _d(out))
+    return out
+
+
+def solid_harmonics_grad(p, xyz, regular=True):
+    out = np.zeros((nharm(p), 3))
+    _load().orc_solid_harmonics_grad(p, int(regular), _d(_c64(xyz)), _d(out))
+    return out
+
+
+def p2m(p, xyz, w, J=None, center=(0, 0, 0), compat=False):
+    xyz = _c64(xyz).reshape(-1, 3)
+    w = _c64(w)
+    out = np.zeros((nharm(p), 3))
+    Jc = _c64(J).reshape(-1, 3) if J is not None else None
+    _load().orc_p2m(p, int(compat), ctypes.c_int64(len(w)), _d(xyz), _d(w), _d(Jc), _d(_c64(center)), _d(out))
+    return out
+
+
+def _translate(name, p, expansion, t, compat):
+    out = np.zeros((nharm(p), 3))
+    getattr(_load(), name)(p, int(compat), _d(_c64(expansion)), _d(_c64(t)), _d(out))
+    return out
+
+
+def m2m(p, expansion, t, compat=False):
+    return _translate("orc_m2m", p, expansion, t, compat)
+
+
+def m2l(p, expansion, t, compat=False):
+    return _translate("orc_m2l", p, expansion, t, compat)
+
+
+def l2l(p, expansion, t, compat=False):
+    return _translate("orc_l2l", p, expansion, t, compat)
+
+
+def eval_expansion(p, coef, d, regular=True, compat=False):
+    A = np.zeros(3)
+    curl = np.zeros(3)
+    _load().orc_eval_expansion(p, int(regular), int(compat), _d(_c64(coef)), _d(_c64(d)), _d(A), _d(curl))
+    return A, curl
+
+
+def direct(src, w, J, tgt, current=1.0, want_A=False):
+    """FP64 direct Biot-Savart B (and optionally A) at tgt; coincident pairs skipped."""
+    src = _c64(src).reshape(-1, 3)
+    tgt = _c64(tgt).reshape(-1, 3)
+    w = _c64(w)
+    Jc = _c64(J).reshape(-1, 3) if J is not None else None
+    B = np.zeros((len(tgt), 3))
+    A = np.zeros((len(tgt), 3)) if want_A else None
+    _load().orc_direct(ctypes.c_int64(len(src)), _d(src), _d(w), _d(Jc), ctypes.c_int64(len(tgt)), _d(tgt),
+                       ctypes.c_double(current), _d(B), _d(A))
+    return (B, A) if want_A else B
+
+
+def fmm(p, cap, src, w, J, tgt, center, H, current=1.0, want_A=False, truncate=False, cap_tgt=0):
+    """Standard-mode FMM (the definition the device pipeline implements). Returns (B, A, stats).
+    truncate=True keeps the reference's l + lambda <= p M2L truncation; False keeps the full
+    operator (l + lambda <= 2p). cap_tgt: target leaf capacity (0: same as cap)."""
+    _load().orc_set_m2l_extra(0 if truncate else p)
+    _load().orc_set_target_cap(int(cap_tgt))
+    src = _c64(src).reshape(-1, 3)
+    tgt = _c64(tgt).reshape(-1, 3)
+    w = _c64(w)
+    Jc = _c64(J).reshape(-1, 3) if J is not None else None
+    B = np.zeros((len(tgt), 3))
+    A = np.zeros((len(tgt), 3)) if want_A else None
+    stats = np.zeros(8)
+    _load().orc_fmm(p, cap, ctypes.c_int64(len(src)), _d(src), _d(w), _d(Jc), ctypes.c_int64(len(tgt)), _d(tgt),
+                    ctypes.c_double(current), _d(_c64(center)), ctypes.c_double(H), _d(B), _d(A), _d(stats))
+    keys = ["nodes", "levels", "leaves", "V", "U", "W", "X", "direct_pairs"]
+    return B, A, dict(zip(keys, stats.tolist()))
+
+
+def tree(cap, src, tgt, center, H):
+    """Node table (level, ix, iy, iz, s0, s1, t0, t1, parent, nchild), list sizes (V, U, W, X),
+    and sorted-position -> input index maps of the standard-mode tree."""
+    src = _c64(src).reshape(-1, 3)
+    tgt = _c64(tgt).reshape(-1, 3)
+    lib = _load()
+    args = (ctypes.c_int64(len(src)), _d(src), ctypes.c_int64(len(tgt)), _d(tgt), _d(_c64(center)), ctypes.c_double(H))
+    n_nodes = lib.orc_tree(cap, *args, ctypes.c_int64(0), None, None, None, None)
+    info = np.zeros((n_nodes, 10), dtype=np.int64)
+    lists = np.zeros((n_nodes, 4), dtype=np.int64)
+    so = np.zeros(len(src), dtype=np.int64)
+    to = np.zeros(len(tgt), dtype=np.int64)
+    lib.orc_tree.restype = ctypes.c_int64
+    lib.orc_tree(cap, *args, ctypes.c_int64(n_nodes), info.ctypes.data_as(_i64p), lists.ctypes.data_as(_i64p),
+                 so.ctypes.data_as(_i64p), to.ctypes.data_as(_i64p))
+    return info, lists, so, to
+
+
+def coverage(cap, src, tgt, center, H):
+    src = _c64(src).reshape(-1, 3)
+    tgt = _c64(tgt).reshape(-1, 3)
+    cnt = np.zeros((len(tgt), len(src)), dtype=np.int32)
+    _load().orc_coverage(cap, ctypes.c_int64(len(src)), _d(src), ctypes.c_int64(len(tgt)), _d(tgt),
+                         _d(_c64(center)), ctypes.c_double(H), cnt.ctypes.data_as(_i32p))
+    return cnt
+
+
+# --------------------------------------------------------------------------------------
+# The reference itself, compiled by oracle/ref/build_ref.sh (present only where that ran).
+# --------------------------------------------------------------------------------------
+class Reference:
+    """The patched reference CPU library for one (real type, order) build."""
+
+    def __init__(self, real="f64", order=10):
+        path = os.path.join(REF_DIR, f"libref_fmm_{real}_p{order}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.lib.ref_fmm.restype = ctypes.c_int
+        self.order = order
+
+    @staticmethod
+    def available(real="f64", order=10):
+        return os.path.exists(os.path.join(REF_DIR, f"libref_fmm_{real}_p{order}.so"))
+
+    def regular(self, p, xyz):
+        out = np.zeros(nharm(p))
+        self.lib.ref_regular(p, _d(_c64(xyz)), _d(out))
+        return out
+
+    def irregular(self, p, xyz):
+        out = np.zeros(nharm(p))
+        self.lib.ref_irregular(p, _d(_c64(xyz)), _d(out))
+        return out
+
+    def p2m(self, p, xyzw, center):
+        xyzw = _c64(xyzw).reshape(-1, 4)
+        out = np.zeros((nharm(p), 3))
+        self.lib.ref_p2m(p, len(xyzw), _d(xyzw), _d(_c64(center)), _d(out))
+        return out
+
+    def _tr(self, name, p, e, t):
+        out = np.zeros((nharm(p), 3))
+        getattr(self.lib, name)(p, _d(_c64(e)), _d(_c64(t)), _d(out))
+        return out
+
+    def m2m(self, p, e, t):
+        return self._tr("ref_m2m", p, e, t)
+
+    def m2l(self, p, e, t):
+        return self._tr("ref_m2l", p, e, t)
+
+    def l2l(self, p, e, t):
+        return self._tr("ref_l2l", p, e, t)
+
+    def eval_local(self, p, local, d):
+        out = np.zeros(3)
+        self.lib.ref_eval_local(p, _d(_c64(local)), _d(_c64(d)), _d(out))
+        return out
+
+    def direct_B(self, xyzw, pts, current=1.0):
+        xyzw = _c64(xyzw).reshape(-1, 4)
+        pts = _c64(pts).reshape(-1, 3)
+        out = np.zeros((len(pts), 3))
+        self.lib.ref_direct_B(len(xyzw), _d(xyzw), len(pts), _d(pts), ctypes.c_double(current), _d(out))
+        return out
+
+    def fmm(self, xyzw, pts, cap_src, cap_tgt, current=1.0, want_B=True):
+        xyzw = _c64(xyzw).reshape(-1, 4)
+        pts = _c64(pts).reshape(-1, 3)
+        out = np.zeros((len(pts), 3))
+        times = np.zeros(5)
+        found = self.lib.ref_fmm(len(xyzw), _d(xyzw), len(pts), _d(pts), cap_src, cap_tgt, ctypes.c_double(current),
+                                 int(want_B), _d(out), _d(times))
+        return out, found, times

@@ -1,0 +1,68 @@
+"""Generates the golden vectors in tests/golden/ from the reference itself.
+
+Runs the patched reference build (oracle/_ref/libref_fmm_*.so, made by oracle/ref/build_ref.sh
+from the reference sources) on seeded inputs and stores inputs and outputs as .npz. The
+reference is not needed afterwards: the tests read only the .npz files.
+
+Usage: python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", ".."))
+from oracle.oracle import Reference  # noqa: E402
+from bachelors_b200 import geometry  # noqa: E402
+
+
+def main():
+    rng = np.random.default_rng(20260001)
+    ref = Reference("f64", 10)
+    out = {}
+    for p in (4, 10, 16):
+        pts = rng.normal(size=(6, 3)) * rng.uniform(0.2, 3.0, size=(6, 1))
+        out[f"harm_p{p}_x"] = pts
+        out[f"harm_p{p}_regular"] = np.stack([ref.regular(p, x) for x in pts])
+        out[f"harm_p{p}_irregular"] = np.stack([ref.irregular(p, x) for x in pts])
+        L = (p + 1) ** 2
+        for name, scale in (("m2m", 0.3), ("m2l", 3.0), ("l2l", 0.3)):
+            e = rng.normal(size=(2, L, 3))
+            t = rng.normal(size=(2, 3)) * scale
+            out[f"{name}_p{p}_in"] = e
+            out[f"{name}_p{p}_t"] = t
+            out[f"{name}_p{p}_out"] = np.stack([getattr(ref, name)(p, e[i], t[i]) for i in range(2)])
+        q = rng.normal(size=(24, 3)) * 0.2
+        w = rng.uniform(0.1, 1.0, size=24)
+        c = rng.normal(size=3) * 0.05
+        out[f"p2m_p{p}_xyzw"] = np.c_[q, w]
+        out[f"p2m_p{p}_center"] = c
+        out[f"p2m_p{p}_out"] = ref.p2m(p, np.c_[q, w], c)
+        loc = rng.normal(size=(L, 3))
+        d = rng.normal(size=3) * 0.2
+        out[f"eval_p{p}_local"] = loc
+        out[f"eval_p{p}_d"] = d
+        out[f"eval_p{p}_out"] = ref.eval_local(p, loc, d)
+    # direct Biot-Savart with the reference's azimuthal current
+    src = np.c_[rng.normal(size=(256, 3)), rng.uniform(0.1, 1.0, 256)]
+    tgt = rng.normal(size=(32, 3)) * 2
+    out["direct_xyzw"] = src
+    out["direct_tgt"] = tgt
+    out["direct_B"] = ref.direct_B(src, tgt, 5.0)
+    # the reference's full FMM pipeline (p = 10, FP64) on a small torus, targets away from it
+    xyz, w, _ = geometry.torus(32, 8, 4, 2.0, 0.5)
+    far = rng.uniform(-1, 1, size=(64, 3))
+    far = far / np.linalg.norm(far, axis=1, keepdims=True) * 5.0
+    B, found, _ = ref.fmm(np.c_[xyz, w], far, 64, 32, 1.0)
+    assert found == len(far)
+    out["fmm_xyzw"] = np.c_[xyz, w]
+    out["fmm_tgt"] = far
+    out["fmm_B"] = B
+    out["fmm_direct_B"] = ref.direct_B(np.c_[xyz, w], far, 1.0)
+    np.savez_compressed(os.path.join(HERE, "reference_p4_p10_p16.npz"), **out)
+    print("wrote", os.path.join(HERE, "reference_p4_p10_p16.npz"), len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()
