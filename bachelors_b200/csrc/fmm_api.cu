@@ -1,5 +1,6 @@
 // C ABI of libfmmcuda.so (declared in include/fmmcuda.h): plan lifetime, input staging,
 // phase sequencing, timing and error reporting.
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -178,6 +179,10 @@ fmm_status fmm_plan_create(const fmm_config* cfg, fmm_plan** plan)
    P.L = nharm(P.p);
    P.Lp = padded(P.L);
    P.fp64 = cfg->precision == FMM_FP64;
+   {
+      const char* dbg = getenv("FMM_DEBUG_SYNC");
+      P.debugSync = dbg && dbg[0] == '1';
+   }
    fmm_status s = P.rootb.reserve(sizeof(RootBox));
    if(s == FMM_OK) s = P.errb.reserve(sizeof(int));
    if(s != FMM_OK) { delete h; return s; }
@@ -381,6 +386,7 @@ fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats)
    const Plan& P = plan->P;
    DeviceGuard g(P.cfg.device);
    fmm_stats s{};
+   if(P.downReady) cudaEventSynchronize(P.ev[5]);
    s.ms_tree = elapsed(P.ev[0], P.ev[1]);
    s.ms_upward = elapsed(P.ev[1], P.ev[2]);
    s.ms_m2l = elapsed(P.ev[2], P.ev[3]);

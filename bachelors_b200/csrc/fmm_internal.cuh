@@ -130,9 +130,25 @@ struct Plan
    cudaEvent_t ev[8];
    bool eventsMade = false;
 
+   int64_t launches = 0;      // kernels this plan launched (all phases, cumulative)
+   bool debugSync = false;    // FMM_DEBUG_SYNC=1: synchronise and check after every launch
+
    fmm_status ensureNodes(int64_t cap, cudaStream_t st = 0);
    fmm_status ensureLists(int64_t cap);
 };
+
+// Bookkeeping after every kernel launch: counts it, surfaces launch errors, and in debug mode
+// synchronises so a fault is attributed to the kernel that raised it.
+inline fmm_status launched(Plan& P, const char* name, cudaStream_t st)
+{
+   P.launches++;
+   cudaError_t e = cudaGetLastError();
+   if(e == cudaSuccess && P.debugSync) e = cudaStreamSynchronize(st);
+   if(e != cudaSuccess)
+      return setError(e == cudaErrorMemoryAllocation ? FMM_E_OOM : FMM_E_CUDA, "kernel %s: %s", name,
+                      cudaGetErrorString(e));
+   return FMM_OK;
+}
 
 template <class T> fmm_status buildTreeT(Plan& P, cudaStream_t st);
 template <class T> fmm_status upwardT(Plan& P, cudaStream_t st);

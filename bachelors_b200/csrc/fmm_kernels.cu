@@ -183,6 +183,7 @@ fmm_status buildOperators(Plan& P, cudaStream_t st)
    size_t shm = sizeof(double) * nharm(std::max(lim, p));
    kBuildOperators<<<16 + 316, 256, shm, st>>>(p, lim, 0, 16 + 316, (double*)P.opM2M64.ptr, (double*)P.opL2L64.ptr,
                                                (double*)P.opM2L64.ptr);
+   FMM_TRY(launched(P, "kBuildOperators", st));
    FMM_CHECK_LAUNCH();
    size_t es = P.fp64 ? sizeof(double) : sizeof(float);
    FMM_TRY(P.opM2Mw.reserve(es * 8 * L * Lp));
@@ -191,14 +192,20 @@ fmm_status buildOperators(Plan& P, cudaStream_t st)
    if(P.fp64)
    {
       kTransposeOps<double><<<1024, 256, 0, st>>>((const double*)P.opM2M64.ptr, 8, L, Lp, (double*)P.opM2Mw.ptr);
+      FMM_TRY(launched(P, "kTransposeOps", st));
       kTransposeOps<double><<<1024, 256, 0, st>>>((const double*)P.opL2L64.ptr, 8, L, Lp, (double*)P.opL2Lw.ptr);
+      FMM_TRY(launched(P, "kTransposeOps", st));
       kTransposeOps<double><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, 316, L, Lp, (double*)P.opM2Lw.ptr);
+      FMM_TRY(launched(P, "kTransposeOps", st));
    }
    else
    {
       kTransposeOps<float><<<1024, 256, 0, st>>>((const double*)P.opM2M64.ptr, 8, L, Lp, (float*)P.opM2Mw.ptr);
+      FMM_TRY(launched(P, "kTransposeOps", st));
       kTransposeOps<float><<<1024, 256, 0, st>>>((const double*)P.opL2L64.ptr, 8, L, Lp, (float*)P.opL2Lw.ptr);
+      FMM_TRY(launched(P, "kTransposeOps", st));
       kTransposeOps<float><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, 316, L, Lp, (float*)P.opM2Lw.ptr);
+      FMM_TRY(launched(P, "kTransposeOps", st));
    }
    FMM_CHECK_LAUNCH();
    P.opOrder = p;
@@ -507,14 +514,16 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
                                                T* __restrict__ outB, T* __restrict__ outA)
 {
    typedef typename Vec4<T>::type V4;
-   extern __shared__ unsigned char smraw[];
+   extern __shared__ __align__(32) unsigned char smraw[];
    const int node = blockIdx.x;
    if(t.nchild[node] != 0 || t.t1[node] == t.t0[node]) return;
    const int L = nharm(p);
    const int Lb = nharm(p - 1);
    T* Ls = (T*)smraw;          // [3][L] local
    T* Cs = Ls + 3 * L;         // [3][Lb] curl expansion
-   V4* Sp = (V4*)(Cs + 3 * Lb);  // [NT] source tile positions
+   // source tiles start on a 32-byte boundary after the two coefficient arrays
+   const size_t coefBytes = (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31);
+   V4* Sp = (V4*)(smraw + coefBytes);  // [NT] source tile positions
    V4* Sq = Sp + NT;           // [NT] source tile strengths
    for(int e = threadIdx.x; e < 3 * L; e += NT) Ls[e] = Lc[int64_t(node) * 3 * Lp + (e / L) * Lp + e % L];
    __syncthreads();
@@ -681,6 +690,7 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
    FMM_CUDA(cudaFuncSetAttribute(kP2M<T, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
    kP2M<T, CH><<<int(N), CH, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
                                         (T*)P.mult.ptr);
+   FMM_TRY(launched(P, "kP2M", st));
    FMM_CHECK_LAUNCH();
    size_t shm2 = sizeof(T) * 8 * 3 * Lp;
    FMM_CUDA(cudaFuncSetAttribute(kM2M<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
@@ -688,6 +698,7 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
    {
       int a = P.tree.levelStart[level], b = P.tree.levelStart[level + 1];
       kM2M<T><<<b - a, 256, shm2, st>>>(P.tree, a, b, P.p, Lp, (const T*)P.opM2Mw.ptr, (T*)P.mult.ptr);
+      FMM_TRY(launched(P, "kM2M", st));
    }
    FMM_CHECK_LAUNCH();
    return FMM_OK;
@@ -704,6 +715,7 @@ fmm_status m2lSimt(Plan& P, cudaStream_t st)
    constexpr int KC = sizeof(T) == 4 ? 32 : 16;
    kM2LSimt<T, KC><<<blocks, 256, 0, st>>>(first, count, P.lists.vtab, P.lists.nv, P.p, P.Lp, (const T*)P.opM2Lw.ptr,
                                        (const T*)P.mult.ptr, (T*)P.local.ptr);
+   FMM_TRY(launched(P, "kM2LSimt", st));
    FMM_CHECK_LAUNCH();
    return FMM_OK;
 }
@@ -723,6 +735,7 @@ fmm_status downwardT(Plan& P, cudaStream_t st)
    {
       int a = P.tree.levelStart[level], b = P.tree.levelStart[level + 1];
       kL2L<T><<<b - a, 256, shm, st>>>(P.tree, a, b, P.p, Lp, (const T*)P.opL2Lw.ptr, (T*)P.local.ptr);
+      FMM_TRY(launched(P, "kL2L", st));
    }
    FMM_CHECK_LAUNCH();
    return FMM_OK;
@@ -735,13 +748,14 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
    const int64_t N = P.tree.nNodes;
    const int L = P.L, Lb = nharm(P.p - 1);
    constexpr int NT = 64;
-   size_t shm = sizeof(T) * (3 * L + 3 * Lb) + 2 * sizeof(V4) * NT;
+   size_t shm = ((sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31)) + 2 * sizeof(V4) * NT;
    FMM_CUDA(cudaFuncSetAttribute(kL2PNear<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
    kL2PNear<T, NT><<<int(N), NT, shm, st>>>(P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr,
                                             (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, (const int*)P.p2pOff.ptr,
                                             (const int*)P.p2pList.ptr, (const int*)P.tIdx.ptr, scaleB, scaleA, want,
                                             (T*)P.outB.ptr, (T*)P.outA.ptr);
+   FMM_TRY(launched(P, "kL2PNear", st));
    FMM_CHECK_LAUNCH();
    return FMM_OK;
 }
@@ -757,6 +771,7 @@ fmm_status directT(Plan& P, double current, int want, cudaStream_t st)
    kDirect<T, T, NT><<<blocks, NT, 0, st>>>((const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, int(P.n),
                                            (const T*)P.tgtXYZ, int(P.m), scaleB, scaleA, want, (T*)P.outB.ptr,
                                            (T*)P.outA.ptr);
+   FMM_TRY(launched(P, "kDirect", st));
    FMM_CHECK_LAUNCH();
    return FMM_OK;
 }
@@ -768,11 +783,17 @@ fmm_status directFp64Subset(Plan& P, double current, const double* tgtDev, int k
    if(blocks == 0) return FMM_OK;
    double scaleB = REF_MU0 / (4 * REF_PI) * current;
    if(P.fp64)
+   {
       kDirect<double, double, NT><<<blocks, NT, 0, st>>>((const double4*)P.sPos.ptr, (const double4*)P.sQ.ptr,
                                                          int(P.n), tgtDev, k, scaleB, 0.0, 1, outDev, nullptr);
+      FMM_TRY(launched(P, "kDirect", st));
+   }
    else
+   {
       kDirect<float, double, NT><<<blocks, NT, 0, st>>>((const float4*)P.sPos.ptr, (const float4*)P.sQ.ptr, int(P.n),
                                                         tgtDev, k, scaleB, 0.0, 1, outDev, nullptr);
+      FMM_TRY(launched(P, "kDirect", st));
+   }
    FMM_CHECK_LAUNCH();
    return FMM_OK;
 }

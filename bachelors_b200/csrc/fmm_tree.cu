@@ -364,15 +364,20 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    const int threads = 256;
    // root cube
    if(P.cfg.root_half_width > 0)
+   {
       kRootFromConfig<<<1, 1, 0, st>>>(P.cfg.root_center[0], P.cfg.root_center[1], P.cfg.root_center[2],
                                        P.cfg.root_half_width, P.root);
+      FMM_TRY(launched(P, "kRootFromConfig", st));
+   }
    else
    {
       int nb = int(std::min<int64_t>(1024, (n + m + threads - 1) / threads));
       nb = std::max(nb, 1);
       FMM_TRY(P.scratch.reserve(sizeof(double) * 6 * nb));
       kBBox<T><<<nb, threads, 0, st>>>((const T*)P.srcXYZ, n, (const T*)P.tgtXYZ, m, (double*)P.scratch.ptr);
+      FMM_TRY(launched(P, "kBBox", st));
       kRootFromBBox<<<1, 1, 0, st>>>((const double*)P.scratch.ptr, nb, P.root);
+      FMM_TRY(launched(P, "kRootFromBBox", st));
    }
    FMM_CHECK_LAUNCH();
    // keys and sort
@@ -384,8 +389,14 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    uint64_t* tk = (uint64_t*)P.tKeys.ptr;
    int* si = (int*)P.sIdx.ptr;
    int* ti = (int*)P.tIdx.ptr;
-   if(n) kKeys<T><<<(n + threads - 1) / threads, threads, 0, st>>>((const T*)P.srcXYZ, n, P.root, sk + n, si + n);
-   if(m) kKeys<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, m, P.root, tk + m, ti + m);
+   if(n) {
+      kKeys<T><<<(n + threads - 1) / threads, threads, 0, st>>>((const T*)P.srcXYZ, n, P.root, sk + n, si + n);
+      FMM_TRY(launched(P, "kKeys", st));
+   }
+   if(m) {
+      kKeys<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, m, P.root, tk + m, ti + m);
+      FMM_TRY(launched(P, "kKeys", st));
+   }
    FMM_CHECK_LAUNCH();
    size_t need = 0, tmp = 0;
    cub::DeviceRadixSort::SortPairs(nullptr, tmp, sk + n, sk, si + n, si, int(n), 0, 63, st);
@@ -397,16 +408,23 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    if(n) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, sk + n, sk, si + n, si, int(n), 0, 63, st));
    tmp = P.cubTmp.bytes;
    if(m) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, 63, st));
+   if(P.debugSync) FMM_CUDA(cudaStreamSynchronize(st));
    // sorted point data
    typedef typename Vec4<T>::type V4;
    FMM_TRY(P.sPos.reserve(sizeof(V4) * std::max<int64_t>(n, 1)));
    FMM_TRY(P.sQ.reserve(sizeof(V4) * std::max<int64_t>(n, 1)));
    FMM_TRY(P.tPos.reserve(sizeof(V4) * std::max<int64_t>(m, 1)));
    if(n)
+   {
       kGatherSources<T><<<(n + threads - 1) / threads, threads, 0, st>>>(
          (const T*)P.srcXYZ, (const T*)P.srcW, (const T*)(P.hasJ ? P.srcJ : nullptr), si, n, (V4*)P.sPos.ptr,
          (V4*)P.sQ.ptr);
-   if(m) kGatherTargets<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, ti, m, (V4*)P.tPos.ptr);
+      FMM_TRY(launched(P, "kGatherSources", st));
+   }
+   if(m) {
+      kGatherTargets<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, ti, m, (V4*)P.tPos.ptr);
+      FMM_TRY(launched(P, "kGatherTargets", st));
+   }
    FMM_CHECK_LAUNCH();
 
    // nodes, level by level
@@ -414,6 +432,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    FMM_TRY(P.ensureNodes(capNodes));
    Tree& t = P.tree;
    kInitRoot<<<1, 1, 0, st>>>(t, int(n), int(m));
+   FMM_TRY(launched(P, "kInitRoot", st));
    t.levelStart[0] = 0;
    t.levelStart[1] = 1;
    int nLevels = 1;
@@ -432,6 +451,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       kCountChildren<<<(cnt + threads - 1) / threads, threads, 0, st>>>(
          t, a, b, level, P.cfg.leaf_capacity,
          P.cfg.target_leaf_capacity > 0 ? P.cfg.target_leaf_capacity : P.cfg.leaf_capacity, sk, tk, bounds, cc);
+      FMM_TRY(launched(P, "kCountChildren", st));
       FMM_CHECK_LAUNCH();
       tmp = 0;
       cub::DeviceScan::ExclusiveSum(nullptr, tmp, cc, off, cnt + 1, st);
@@ -440,6 +460,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       // cnt[cnt] must be 0 for the total to land in off[cnt]
       FMM_CUDA(cudaMemsetAsync(cc + cnt, 0, sizeof(int), st));
       FMM_CUDA(cub::DeviceScan::ExclusiveSum(P.cubTmp.ptr, tmp, cc, off, cnt + 1, st));
+      if(P.debugSync) FMM_CUDA(cudaStreamSynchronize(st));
       int nextCount = 0;
       FMM_CUDA(cudaMemcpyAsync(&nextCount, off + cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
       FMM_CUDA(cudaStreamSynchronize(st));
@@ -450,6 +471,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
          FMM_TRY(P.ensureNodes(capNodes, st));
       }
       kMakeChildren<<<(cnt + threads - 1) / threads, threads, 0, st>>>(t, a, b, level, int(total), bounds, cc, off);
+      FMM_TRY(launched(P, "kMakeChildren", st));
       FMM_CHECK_LAUNCH();
       total += nextCount;
       t.levelStart[level + 2] = int(total);
@@ -463,10 +485,12 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    Lists& Ls = P.lists;
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
    kInitRootLists<<<1, 1, 0, st>>>(Ls);
+   FMM_TRY(launched(P, "kInitRootLists", st));
    for(int level = 1; level < nLevels; level++)
    {
       int a = t.levelStart[level], b = t.levelStart[level + 1];
       kListsLevel<<<(b - a + 127) / 128, 128, 0, st>>>(t, Ls, a, b, P.err);
+      FMM_TRY(launched(P, "kListsLevel", st));
    }
    FMM_CHECK_LAUNCH();
    int nn = int(total);
@@ -475,6 +499,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    int* pc = (int*)P.lvlCnt.ptr;
    int* po = (int*)P.p2pOff.ptr;
    kP2PLists<<<(nn + 127) / 128, 128, 0, st>>>(t, Ls, nn, nullptr, pc, nullptr, P.err);
+   FMM_TRY(launched(P, "kP2PLists", st));
    FMM_CUDA(cudaMemsetAsync(pc + nn, 0, sizeof(int), st));
    tmp = 0;
    cub::DeviceScan::ExclusiveSum(nullptr, tmp, pc, po, nn + 1, st);
@@ -498,6 +523,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    if(herr) return setError(FMM_E_LIMIT, "interaction list capacity exceeded (code %d)", herr);
    FMM_TRY(P.p2pList.reserve(sizeof(int) * std::max(nP2P, 1)));
    kP2PLists<<<(nn + 127) / 128, 128, 0, st>>>(t, Ls, nn, po, nullptr, (int*)P.p2pList.ptr, P.err);
+   FMM_TRY(launched(P, "kP2PLists", st));
    FMM_CHECK_LAUNCH();
    P.nP2P = nP2P;
    P.nV = nV;
