@@ -124,6 +124,7 @@ struct Plan
    DevBuf opM2Mw, opL2Lw, opM2Lw;        // transposed working copies, see fmm_kernels.cu
    DevBuf opM2Lbf;                       // bf16 hi/lo split for the tensor-core M2L
    int opOrder = -1;
+   int opImgOrder = -1;                  // order the tensor-core operator image was built for
    // state
    bool treeReady = false, upReady = false, downReady = false;
    fmm_stats stats{};

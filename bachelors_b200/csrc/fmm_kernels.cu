@@ -209,6 +209,7 @@ fmm_status buildOperators(Plan& P, cudaStream_t st)
    }
    FMM_CHECK_LAUNCH();
    P.opOrder = p;
+   P.opImgOrder = -1;
    return FMM_OK;
 }
 
