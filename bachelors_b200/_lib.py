@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libfmmcuda.so")
 
 FMM_OK, FMM_E_INVALID, FMM_E_OOM, FMM_E_CUDA, FMM_E_TIMEOUT, FMM_E_LIMIT = range(6)
 FMM_FP32, FMM_FP64 = 0, 1
-FMM_M2L_SIMT, FMM_M2L_BF16X3, FMM_M2L_TF32 = 0, 1, 2
+FMM_M2L_SIMT, FMM_M2L_BF16X3, FMM_M2L_TF32, FMM_M2L_BF16X6 = 0, 1, 2, 3
 
 # Every extern "C" symbol include/fmmcuda.h declares.
 EXPORTS = [

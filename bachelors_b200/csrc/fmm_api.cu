@@ -161,7 +161,7 @@ fmm_status fmm_plan_create(const fmm_config* cfg, fmm_plan** plan)
    if(cfg->leaf_capacity < 1) return setError(FMM_E_INVALID, "leaf_capacity must be >= 1");
    if(cfg->precision != FMM_FP32 && cfg->precision != FMM_FP64)
       return setError(FMM_E_INVALID, "unknown precision %d", cfg->precision);
-   if(cfg->m2l_mode < FMM_M2L_SIMT || cfg->m2l_mode > FMM_M2L_TF32)
+   if(cfg->m2l_mode < FMM_M2L_SIMT || cfg->m2l_mode > FMM_M2L_BF16X6)
       return setError(FMM_E_INVALID, "unknown m2l_mode %d", cfg->m2l_mode);
    int ndev = 0;
    cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -203,7 +203,7 @@ fmm_status fmm_plan_destroy(fmm_plan* plan)
    DeviceGuard g(P.cfg.device);
    DevBuf* bufs[] = {&P.srcXYZb, &P.srcWb, &P.srcJb, &P.tgtXYZb, &P.rootb, &P.sKeys, &P.tKeys, &P.sIdx, &P.tIdx,
                      &P.sPos, &P.sQ, &P.tPos, &P.cubTmp, &P.scratch, &P.lvlBounds, &P.lvlCnt, &P.lvlOff,
-                     &P.p2pOff, &P.p2pList, &P.errb, &P.mult, &P.local, &P.outB, &P.outA, &P.opM2M64,
+                     &P.p2pOff, &P.p2pList, &P.m2lTargets, &P.m2lKeys, &P.errb, &P.mult, &P.local, &P.outB, &P.outA, &P.opM2M64,
                      &P.opL2L64, &P.opM2L64, &P.opM2Mw, &P.opL2Lw, &P.opM2Lw, &P.opM2Lbf};
    for(DevBuf* b : bufs) b->release();
    for(auto& b : P.nodeBufs) b.release();

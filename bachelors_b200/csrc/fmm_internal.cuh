@@ -115,6 +115,8 @@ struct Plan
    DevBuf p2pOff, p2pList;
    int nP2P = 0;
    int64_t nV = 0;
+   DevBuf m2lTargets, m2lKeys;          // boxes with an M2L list, grouped by octant
+   int nM2LTargets = 0;
    int* err = nullptr;
    DevBuf errb;
    // expansions [node][3][Lp] and outputs

@@ -10,15 +10,16 @@
 // One CTA owns 42 consecutive target boxes = 126 rows (box, component) of a 128-row tile and
 // all (p+1)^2 output coefficients (TMEM columns). For each offset with at least one source in
 // the tile it accumulates  D[128 x N] += A_o[128 x K] * T_o^T[K x N]  where the rows of A_o are
-// the gathered source multipoles. Operands are split x = hi + lo in bf16 and the three products
-// hi*hi + hi*lo + lo*hi are accumulated in FP32 in tensor memory.
+// the gathered source multipoles. Operands are split into bf16 pieces: x = hi + lo with the three
+// products hi*hi + hi*lo + lo*hi (BF16X3), or x = hi + mid + lo with the six products down to
+// 2^-16 relative (BF16X6); all are accumulated in FP32 in tensor memory.
 //
 // Warp roles (320 threads):
 //   warp 0      TMEM allocation; lane 0 issues the tcgen05.mma instructions
 //   warp 1      lane 0 streams the pre-swizzled operator image with cp.async.bulk (no multicast)
 //   warps 2..9  gather source rows (FP32), split to bf16 hi/lo, store in the SW128 K-major layout
 //   warps 2..5  epilogue: tcgen05.ld of the accumulator, store of the local expansions
-// Stages hold one 64-wide K chunk of A (hi, lo) and of T_o (hi, lo); two stages rotate through
+// Stages hold one K chunk (64 wide with two pieces, 32 with three) of every piece of A and of T_o; two stages rotate through
 // mbarriers (full: producers + bulk-copy bytes, empty: tcgen05.commit). Every wait is bounded by
 // a 2 s global-timer limit; on expiry the CTA records FMM timeout in the error word and stops.
 #include <cuda_bf16.h>
@@ -31,7 +32,7 @@ namespace tc {
 
 constexpr int TT = 42;               // target boxes per tile
 constexpr int ROWS = 128;            // MMA M
-constexpr int KC = 64;               // K chunk (one 128-byte swizzle atom of bf16)
+// (the K chunk width depends on the number of bf16 pieces, see Layout)
 constexpr int NPROD = 256;           // producer threads
 constexpr int NTHREADS = 320;
 constexpr uint64_t TIMEOUT_NS = 2000000000ull;
@@ -98,18 +99,6 @@ __device__ __forceinline__ void bulkLoad(uint32_t dst, const void* src, uint32_t
                 : "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 bytes apart.
-__device__ __forceinline__ uint64_t smemDesc(uint32_t addr)
-{
-   uint64_t d = 0;
-   d |= uint64_t((addr >> 4) & 0x3FFF);          // start address
-   d |= uint64_t(1) << 16;                        // leading byte offset (unused for swizzled K-major)
-   d |= uint64_t(1024 >> 4) << 32;                // stride byte offset
-   d |= uint64_t(1) << 46;                        // descriptor version for sm_100
-   d |= uint64_t(2) << 61;                        // SWIZZLE_128B
-   return d;
-}
-
 // Instruction descriptor: bf16 x bf16 -> f32, A and B K-major, shape M x N.
 __host__ __device__ constexpr uint32_t instrDescBf16(int M, int N)
 {
@@ -151,49 +140,98 @@ __device__ __forceinline__ void tmemLd16(uint32_t addr, float* v)
    for(int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// Byte offset of element (row, k) (k < 64, bf16) inside a SW128 K-major block of 128-byte rows.
-__host__ __device__ constexpr uint32_t swz(uint32_t row, uint32_t k)
+
+// Operand layouts. NP bf16 pieces per value (2: hi + lo, 3: hi + mid + lo). With two pieces a
+// K chunk is 64 elements in 128-byte rows (SW128); with three it is 32 elements in 64-byte rows
+// (SW64) so that two pipeline stages still fit in shared memory.
+template <int NP> struct Layout;
+template <> struct Layout<2>
 {
-   return row * 128u + ((((k >> 3) ^ (row & 7u)) & 7u) << 4) + ((k & 7u) << 1);
+   static constexpr int KC = 64, RB = 128, SBO = 1024, SWZ = 2;
+   __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
+   { return row * 128u + ((((k >> 3) ^ (row & 7u)) & 7u) << 4) + ((k & 7u) << 1); }
+};
+template <> struct Layout<3>
+{
+   static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4;
+   __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
+   { return row * 64u + ((((k >> 3) ^ ((row >> 1) & 3u)) & 3u) << 4) + ((k & 7u) << 1); }
+};
+
+// Shared-memory matrix descriptor: K-major, swizzled rows, 8-row groups SBO bytes apart.
+template <int NP>
+__device__ __forceinline__ uint64_t smemDescT(uint32_t addr)
+{
+   uint64_t d = 0;
+   d |= uint64_t((addr >> 4) & 0x3FFF);               // start address
+   d |= uint64_t(1) << 16;                             // leading byte offset (unused when swizzled)
+   d |= uint64_t(Layout<NP>::SBO >> 4) << 32;         // stride byte offset
+   d |= uint64_t(1) << 46;                             // descriptor version for sm_100
+   d |= uint64_t(Layout<NP>::SWZ) << 61;              // swizzle mode
+   return d;
+}
+
+// Split of x into NP bf16 pieces, each the round-to-nearest of the remaining residual.
+template <int NP>
+__device__ __forceinline__ void splitBf16(double x, __nv_bfloat16* piece)
+{
+   double r = x;
+#pragma unroll
+   for(int i = 0; i < NP; i++)
+   {
+      piece[i] = __float2bfloat16_rn(float(r));
+      r -= double(__bfloat162float(piece[i]));
+   }
 }
 
 }  // namespace tc
 
-// Operator image for the tensor-core M2L: for every offset slot and K chunk, the hi block then
-// the lo block, each N rows (output coefficients, N = Lp) x 64 bf16 (input coefficients) in
-// the SW128 K-major layout, zero outside the (p+1)^2 x (p+1)^2 operator.
-__global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int nChunks, __nv_bfloat16* img)
+// Operator image for the tensor-core M2L: for every offset slot and K chunk, the NP piece blocks
+// (hi first), each N rows (output coefficients, N = Lp) x KC bf16 (input coefficients) in the
+// swizzled K-major layout, zero outside the (p+1)^2 x (p+1)^2 operator.
+template <int NP>
+__global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int nChunks, uint8_t* img)
 {
-   const int64_t blockElems = int64_t(N) * tc::KC;             // one hi or lo block
-   const int64_t total = int64_t(316) * nChunks * 2 * blockElems;
+   using Lay = tc::Layout<NP>;
+   const int64_t blockBytes = int64_t(N) * Lay::RB;
+   const int64_t total = int64_t(316) * nChunks * int64_t(N) * Lay::KC;
    for(int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
    {
       int64_t r = e;
-      const int kk = int(r % tc::KC); r /= tc::KC;
+      const int kk = int(r % Lay::KC); r /= Lay::KC;
       const int n = int(r % N); r /= N;
-      const int half = int(r % 2); r /= 2;
       const int c = int(r % nChunks);
       const int o = int(r / nChunks);
-      const int k = c * tc::KC + kk;
-      double x = (n < L && k < L) ? op64[(int64_t(o) * L + n) * L + k] : 0.0;
-      __nv_bfloat16 hi = __float2bfloat16_rn(float(x));
-      __nv_bfloat16 v = half == 0 ? hi : __float2bfloat16_rn(float(x - double(__bfloat162float(hi))));
-      uint8_t* blk = reinterpret_cast<uint8_t*>(img) + ((int64_t(o) * nChunks + c) * 2 + half) * blockElems * 2;
-      *reinterpret_cast<__nv_bfloat16*>(blk + tc::swz(uint32_t(n), uint32_t(kk))) = v;
+      const int k = c * Lay::KC + kk;
+      const double x = (n < L && k < L) ? op64[(int64_t(o) * L + n) * L + k] : 0.0;
+      __nv_bfloat16 piece[NP];
+      tc::splitBf16<NP>(x, piece);
+      uint8_t* blk = img + (int64_t(o) * nChunks + c) * NP * blockBytes;
+#pragma unroll
+      for(int i = 0; i < NP; i++)
+         *reinterpret_cast<__nv_bfloat16*>(blk + i * blockBytes + Lay::off(uint32_t(n), uint32_t(kk))) = piece[i];
    }
 }
 
+template <int NP>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
-kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChunks,
+kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int Lp, int nChunks,
        const uint8_t* __restrict__ img, const float* __restrict__ M, float* __restrict__ Lc, int* err)
 {
    using namespace tc;
+   using Lay = Layout<NP>;
+   constexpr int KCH = Lay::KC;
+   constexpr int NPASS = NP == 2 ? 3 : 6;
+   // (A piece, B piece) of every product kept: hi*hi, hi*lo, lo*hi  /  down to 2^-16 with three pieces
+   constexpr int PA[6] = {0, 0, 1, 1, 0, 2};
+   constexpr int PB[6] = {0, 1, 0, 1, 2, 0};
+   constexpr int PA2[3] = {0, 0, 1};
+   constexpr int PB2[3] = {0, 1, 0};
    extern __shared__ uint8_t smraw[];
-   const int N = Lp;                                  // output columns (<= 320)
-   const uint32_t aBytes = ROWS * 128;                // one A block (hi or lo), 16 KB
-   const uint32_t bBytes = uint32_t(N) * 128;         // one B block (hi or lo)
-   const uint32_t stageBytes = 2 * aBytes + 2 * bBytes;
-   // 1024-byte aligned stage area, then the control block
+   const int N = Lp;                                   // output columns (<= 320)
+   const uint32_t aBytes = ROWS * Lay::RB;             // one A piece
+   const uint32_t bBytes = uint32_t(N) * Lay::RB;      // one B piece
+   const uint32_t stageBytes = NP * (aBytes + bBytes);
    const uint32_t rawAddr = smemAddr(smraw);
    const uint32_t base = (rawAddr + 1023u) & ~1023u;
    uint8_t* sbase = smraw + (base - rawAddr);
@@ -202,15 +240,17 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
    uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 64);
    volatile int* abortFlag = reinterpret_cast<volatile int*>(ctrl + 68);
    uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 72);  // 10 words: offsets present in the tile
-   int* itemOffset = reinterpret_cast<int*>(ctrl + 128);        // compacted present offsets [316]
+   int* itemOffset = reinterpret_cast<int*>(ctrl + 128);        // compacted present offsets [316] + count
+   int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
-   const int t0 = firstNode + blockIdx.x * TT;
-   const int tEnd = min(t0 + TT, firstNode + nNodes);
+   const int first = blockIdx.x * TT;
+   const int nTile = min(TT, nTargets - first);
    const uint32_t fullBar0 = smemAddr(&bars[0]), emptyBar0 = smemAddr(&bars[2]), doneBar = smemAddr(&bars[4]);
 
    if(tid < 10) present[tid] = 0;
+   if(tid < TT) tileNode[tid] = tid < nTile ? targets[first + tid] : -1;
    if(tid == 0)
    {
       *abortFlag = 0;
@@ -231,13 +271,12 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
    // which offsets have a source for some box of the tile
    for(int e = tid; e < TT * 316; e += NTHREADS)
    {
-      const int t = t0 + e / 316, o = e % 316;
-      if(t < tEnd && vtab[int64_t(t) * 316 + o] >= 0) atomicOr(&present[o >> 5], 1u << (o & 31));
+      const int t = tileNode[e / 316], o = e % 316;
+      if(t >= 0 && vtab[int64_t(t) * 316 + o] >= 0) atomicOr(&present[o >> 5], 1u << (o & 31));
    }
    fenceBeforeSync();
    __syncthreads();
    fenceAfterSync();
-   // compact the present offsets (same list for every role)
    if(tid == 0)
    {
       int k = 0;
@@ -254,31 +293,32 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
    {
       if(lane == 0)
       {
-         const uint32_t idA = instrDescBf16(ROWS, 256);
-         const int nB = N - 256;                      // 48 for p = 16; <= 0 for smaller orders
+         const int nB = N - 256;                       // second MMA's width (48 at p = 16)
+         const uint32_t idA = instrDescBf16(ROWS, N <= 256 ? N : 256);
          const uint32_t idB = nB > 0 ? instrDescBf16(ROWS, nB) : 0u;
-         const uint32_t idFull = instrDescBf16(ROWS, N <= 256 ? N : 256);
-         bool first = true;
+         bool firstMma = true;
          for(int it = 0; it < nItems; it++)
          {
             const int s = it & 1;
             if(!mbarWait(fullBar0 + 8 * s, (it >> 1) & 1, err, abortFlag)) break;
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
-            const uint32_t aHi = st, aLo = st + aBytes, bHi = st + 2 * aBytes, bLo = bHi + bBytes;
+            const uint32_t aSt = st, bSt = st + NP * aBytes;
 #pragma unroll
-            for(int ks = 0; ks < KC / 16; ks++)
+            for(int ks = 0; ks < KCH / 16; ks++)
             {
                const uint32_t koff = ks * 32;
-               const uint32_t a[3] = {aHi + koff, aHi + koff, aLo + koff};
-               const uint32_t b[3] = {bHi + koff, bLo + koff, bHi + koff};
 #pragma unroll
-               for(int pass = 0; pass < 3; pass++)
+               for(int pass = 0; pass < NPASS; pass++)
                {
-                  const uint32_t acc = first ? 0u : 1u;
-                  mmaBf16(tmem, smemDesc(a[pass]), smemDesc(b[pass]), N <= 256 ? idFull : idA, acc);
-                  if(nB > 0) mmaBf16(tmem + 256, smemDesc(a[pass]), smemDesc(b[pass] + 256 * 128), idB, acc);
-                  first = false;
+                  const int pa = NP == 2 ? PA2[pass] : PA[pass];
+                  const int pb = NP == 2 ? PB2[pass] : PB[pass];
+                  const uint32_t a = aSt + pa * aBytes + koff;
+                  const uint32_t b = bSt + pb * bBytes + koff;
+                  const uint32_t acc = firstMma ? 0u : 1u;
+                  mmaBf16(tmem, smemDescT<NP>(a), smemDescT<NP>(b), idA, acc);
+                  if(nB > 0) mmaBf16(tmem + 256, smemDescT<NP>(a), smemDescT<NP>(b + 256 * Lay::RB), idB, acc);
+                  firstMma = false;
                }
             }
             mmaCommit(emptyBar0 + 8 * s);
@@ -296,33 +336,32 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
             const int s = it & 1;
             if(it >= 2 && !mbarWait(emptyBar0 + 8 * s, ((it >> 1) - 1) & 1, err, abortFlag)) break;
             const int o = itemOffset[it / nChunks], c = it % nChunks;
-            const uint8_t* src = img + (int64_t(o) * nChunks + c) * 2 * bBytes;
-            const uint32_t dst = base + s * stageBytes + 2 * aBytes;
-            mbarArriveExpectTx(fullBar0 + 8 * s, 2 * bBytes);
-            bulkLoad(dst, src, 2 * bBytes, fullBar0 + 8 * s);
+            const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
+            const uint32_t dst = base + s * stageBytes + NP * aBytes;
+            mbarArriveExpectTx(fullBar0 + 8 * s, NP * bBytes);
+            bulkLoad(dst, src, NP * bBytes, fullBar0 + 8 * s);
          }
       }
       __syncwarp();
    }
    else
    {
-      // producers: two threads per row, 32 K-elements each
+      // producers: two threads per row, KCH / 2 K-elements each
+      constexpr int PER = KCH / 2;
       const int ptid = tid - 64;
       const int row = ptid >> 1, half = ptid & 1;
-      const int tgt = t0 + row / 3, comp = row % 3;
-      const bool rowValid = row < 3 * TT && tgt < tEnd;
+      const int slot = row / 3, comp = row % 3;
+      const int tgt = row < 3 * TT ? tileNode[slot] : -1;
       for(int it = 0; it < nItems; it++)
       {
          const int s = it & 1;
          if(it >= 2 && !mbarWait(emptyBar0 + 8 * s, ((it >> 1) - 1) & 1, err, abortFlag)) break;
          const int o = itemOffset[it / nChunks], c = it % nChunks;
-         int src = -1;
-         if(rowValid) src = vtab[int64_t(tgt) * 316 + o];
-         uint8_t* aHi = sbase + s * stageBytes;
-         uint8_t* aLo = aHi + aBytes;
-         const int k0 = c * KC + half * 32;
+         const int src = tgt >= 0 ? vtab[int64_t(tgt) * 316 + o] : -1;
+         uint8_t* aSt = sbase + s * stageBytes;
+         const int k0 = c * KCH + half * PER;
 #pragma unroll
-         for(int q = 0; q < 4; q++)
+         for(int q = 0; q < PER / 8; q++)
          {
             float v[8];
             const int k = k0 + 8 * q;
@@ -337,19 +376,27 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
 #pragma unroll
                for(int i = 0; i < 8; i++) v[i] = 0.f;
             }
-            uint32_t hw[4], lw[4];
+            uint32_t w[NP][4];
 #pragma unroll
             for(int i = 0; i < 4; i++)
             {
-               const __nv_bfloat16 h0 = __float2bfloat16_rn(v[2 * i]), h1 = __float2bfloat16_rn(v[2 * i + 1]);
-               const __nv_bfloat16 l0 = __float2bfloat16_rn(v[2 * i] - __bfloat162float(h0));
-               const __nv_bfloat16 l1 = __float2bfloat16_rn(v[2 * i + 1] - __bfloat162float(h1));
-               hw[i] = uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
-               lw[i] = uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
+               __nv_bfloat16 p0[NP], p1[NP];
+               // FP32 residuals are exact here: each piece removes the leading bits of the remainder
+               float r0 = v[2 * i], r1 = v[2 * i + 1];
+#pragma unroll
+               for(int j = 0; j < NP; j++)
+               {
+                  p0[j] = __float2bfloat16_rn(r0);
+                  p1[j] = __float2bfloat16_rn(r1);
+                  r0 -= __bfloat162float(p0[j]);
+                  r1 -= __bfloat162float(p1[j]);
+                  w[j][i] = uint32_t(__bfloat16_as_ushort(p0[j])) | (uint32_t(__bfloat16_as_ushort(p1[j])) << 16);
+               }
             }
-            const uint32_t off = swz(uint32_t(row), uint32_t(half * 32 + 8 * q));
-            *reinterpret_cast<uint4*>(aHi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-            *reinterpret_cast<uint4*>(aLo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+            const uint32_t off = Lay::off(uint32_t(row), uint32_t(half * PER + 8 * q));
+#pragma unroll
+            for(int j = 0; j < NP; j++)
+               *reinterpret_cast<uint4*>(aSt + j * aBytes + off) = make_uint4(w[j][0], w[j][1], w[j][2], w[j][3]);
          }
          fenceProxyAsync();
          mbarArrive(fullBar0 + 8 * s);
@@ -361,8 +408,7 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
          fenceAfterSync();
          const int lanes = 32 * (warp & 3);
          const int r = lanes + lane;
-         const int et = t0 + r / 3, ec = r % 3;
-         const bool valid = r < 3 * TT && et < tEnd;
+         const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
          float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
          for(int c0 = 0; c0 < N; c0 += 16)
          {
@@ -370,7 +416,7 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
             if(ok && nItems > 0) tmemLd16(tmem + (uint32_t(lanes) << 16) + uint32_t(c0), v);
             else
                for(int i = 0; i < 16; i++) v[i] = 0.f;
-            if(valid)
+            if(et >= 0)
                for(int i = 0; i < 16; i++) out[c0 + i] = v[i];
          }
       }
@@ -387,38 +433,47 @@ kM2LTc(int firstNode, int nNodes, const int* __restrict__ vtab, int Lp, int nChu
    }
 }
 
-fmm_status m2lTensorCore(Plan& P, cudaStream_t st)
+template <int NP>
+static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
 {
-   if(P.cfg.m2l_mode != FMM_M2L_BF16X3)
-      return setError(FMM_E_INVALID, "tensor-core M2L: only the BF16X3 mode is built");
+   using Lay = tc::Layout<NP>;
    const int L = P.L, Lp = P.Lp;
-   if(Lp > 320) return setError(FMM_E_INVALID, "tensor-core M2L supports p <= 16");
-   if(Lp % 16) return setError(FMM_E_INVALID, "tensor-core M2L needs 16-aligned coefficient rows");
-   const int nChunks = (L + tc::KC - 1) / tc::KC;
-   const size_t imgBytes = size_t(316) * nChunks * 2 * size_t(Lp) * 128;
-   if(P.opImgOrder != P.p)
+   const int nChunks = (L + Lay::KC - 1) / Lay::KC;
+   const size_t imgBytes = size_t(316) * nChunks * NP * size_t(Lp) * Lay::RB;
+   const int tag = P.p * 8 + NP;
+   if(P.opImgOrder != tag)
    {
       FMM_TRY(P.opM2Lbf.reserve(imgBytes));
-      kPrepM2LImage<<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, L, Lp, nChunks, (__nv_bfloat16*)P.opM2Lbf.ptr);
+      kPrepM2LImage<NP><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, L, Lp, nChunks, (uint8_t*)P.opM2Lbf.ptr);
       FMM_TRY(launched(P, "kPrepM2LImage", st));
-      P.opImgOrder = P.p;
+      P.opImgOrder = tag;
    }
-   const int first = 1;
-   const int count = int(P.tree.nNodes - 1);
+   const int count = P.nM2LTargets;
    if(count <= 0) return FMM_OK;
    const int blocks = (count + tc::TT - 1) / tc::TT;
-   const size_t stageBytes = 2 * tc::ROWS * 128 + 2 * size_t(Lp) * 128;
-   const size_t smem = 1024 + 2 * stageBytes + 128 + 4 * 320;
-   FMM_CUDA(cudaFuncSetAttribute(kM2LTc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
+   const size_t smem = 1024 + 2 * stageBytes + 128 + 4 * (320 + 64);
+   if(smem > 232448) return setError(FMM_E_INVALID, "tensor-core M2L: %zu bytes of shared memory needed", smem);
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
-   kM2LTc<<<blocks, tc::NTHREADS, smem, st>>>(first, count, P.lists.vtab, Lp, nChunks, (const uint8_t*)P.opM2Lbf.ptr,
-                                             (const float*)P.mult.ptr, (float*)P.local.ptr, P.err);
+   kM2LTc<NP><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, Lp, nChunks,
+                                                 (const uint8_t*)P.opM2Lbf.ptr, (const float*)P.mult.ptr,
+                                                 (float*)P.local.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    int herr = 0;
    FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
    FMM_CUDA(cudaStreamSynchronize(st));
    if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "tensor-core M2L: a pipeline wait timed out");
    return FMM_OK;
+}
+
+fmm_status m2lTensorCore(Plan& P, cudaStream_t st)
+{
+   if(P.Lp > 320) return setError(FMM_E_INVALID, "tensor-core M2L supports p <= 16");
+   if(P.Lp % 16) return setError(FMM_E_INVALID, "tensor-core M2L needs 16-aligned coefficient rows");
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X3) return launchM2LTc<2>(P, st);
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X6) return launchM2LTc<3>(P, st);
+   return setError(FMM_E_INVALID, "tensor-core M2L: the TF32 mode is not built");
 }
 
 }  // namespace fmm

@@ -56,7 +56,8 @@ class M2LAlg(IntEnum):
 
 
 _PRECISION = {"fp32": _lib.FMM_FP32, "fp64": _lib.FMM_FP64}
-_M2L = {"simt": _lib.FMM_M2L_SIMT, "bf16x3": _lib.FMM_M2L_BF16X3, "tf32": _lib.FMM_M2L_TF32}
+_M2L = {"simt": _lib.FMM_M2L_SIMT, "bf16x3": _lib.FMM_M2L_BF16X3, "tf32": _lib.FMM_M2L_TF32,
+        "bf16x6": _lib.FMM_M2L_BF16X6}
 
 
 def _is_cuda_tensor(x):

@@ -196,12 +196,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--m2l", default="auto", choices=["auto", "simt", "bf16x3", "tf32"])
+    ap.add_argument("--m2l", default="auto", choices=["auto", "simt", "bf16x3", "bf16x6"])
     ap.add_argument("--size", default="512,128,256", help="torus n_phi,n_theta,n_rho")
     ap.add_argument("--order", type=int, default=16)
     ap.add_argument("--leaf", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison solve")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -219,14 +220,7 @@ def main():
     size = tuple(int(v) for v in args.size.split(","))
     xyz, w, J = make_workload(*size)
     n = len(xyz)
-    m2l = args.m2l
-    if m2l == "auto":
-        m2l = "simt"
-        try:
-            from bachelors_b200 import _lib  # noqa: F401
-            m2l = os.environ.get("FMM_BENCH_M2L", "simt")
-        except Exception:
-            pass
+    m2l = "bf16x6" if args.m2l == "auto" else args.m2l
     dev = f"cuda:{local}"
     d_xyz = torch.from_numpy(xyz).to(dev)
     d_w = torch.from_numpy(w).to(dev)
@@ -297,6 +291,38 @@ def main():
                      "note": "algorithmic FLOPs = V pairs x 3 components x 2 (p+1)^4; peak = measured bf16 dense"},
         "clocks": clk,
     }
+
+    # the other M2L forms on the same workload (one warm-up and one timed solve each): the plain
+    # FP32 FMM (M2L on the CUDA cores) for the split-BF16 ratio, and the cheaper BF16X3 split
+    def one_mode(mode):
+        pplan = Plan(order=args.order, leaf_capacity=args.leaf, precision="fp32", m2l=mode, device=local)
+        pplan.set_sources(d_xyz, d_w, d_J)
+        pplan.set_targets(d_xyz)
+        Bp, _ = pplan.solve(1.0, 1)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        Bp, _ = pplan.solve(1.0, 1)
+        e1.record()
+        torch.cuda.synchronize()
+        pms = max_over_ranks(e0.elapsed_time(e1), world)
+        Bph = Bp.cpu().numpy().astype(np.float64)
+        res = {"value": world * n / (pms / 1000.0), "ms_per_step": pms, "steps": 1, "warmup": 1,
+               "rel_l2_vs_fp64_direct": float(np.linalg.norm(Bph[idx] - Bd) / np.linalg.norm(Bd)),
+               "ms_m2l": pplan.stats()["ms_m2l"]}
+        pplan.close()
+        return res
+
+    if not args.no_plain:
+        for mode in ("simt", "bf16x3", "bf16x6"):
+            if mode == m2l:
+                continue
+            key = "plain_fp32" if mode == "simt" else f"m2l_{mode}"
+            line[key] = one_mode(mode)
+        if "plain_fp32" in line:
+            line["speedup_vs_plain_fp32"] = line["value"] / line["plain_fp32"]["value"]
 
     if rank == 0:
         try:

@@ -46,9 +46,16 @@ typedef enum fmm_precision { FMM_FP32 = 0, FMM_FP64 = 1 } fmm_precision;
 /* How the M2L contraction is computed (FP32 plans only; FP64 plans always use FMM_M2L_SIMT).
  *   SIMT    FP32 (or FP64) FMA on the CUDA cores.
  *   BF16X3  tcgen05 tensor cores, operands split x = hi + lo in bf16, hi*hi + hi*lo + lo*hi,
- *           FP32 accumulation in tensor memory.
- *   TF32    tcgen05 tensor cores, one TF32 pass, FP32 accumulation. */
-typedef enum fmm_m2l_mode { FMM_M2L_SIMT = 0, FMM_M2L_BF16X3 = 1, FMM_M2L_TF32 = 2 } fmm_m2l_mode;
+ *           FP32 accumulation in tensor memory (about 16 bits per product).
+ *   TF32    tcgen05 tensor cores, one TF32 pass, FP32 accumulation.
+ *   BF16X6  tcgen05 tensor cores, operands split x = hi + mid + lo in bf16 and the six products
+ *           down to 2^-16 relative kept (about FP32 accuracy). */
+typedef enum fmm_m2l_mode {
+   FMM_M2L_SIMT = 0,
+   FMM_M2L_BF16X3 = 1,
+   FMM_M2L_TF32 = 2,
+   FMM_M2L_BF16X6 = 3
+} fmm_m2l_mode;
 
 typedef struct fmm_config {
    int order;          /* expansion order p, 1..16 ((p+1)^2 harmonics) */
