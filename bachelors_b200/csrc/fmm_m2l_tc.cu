@@ -17,11 +17,15 @@
 // Warp roles (320 threads):
 //   warp 0      TMEM allocation; lane 0 issues the tcgen05.mma instructions
 //   warp 1      lane 0 streams the pre-swizzled operator image with cp.async.bulk (no multicast)
-//   warps 2..9  gather source rows (FP32), split to bf16 hi/lo, store in the SW128 K-major layout
-//   warps 2..5  epilogue: tcgen05.ld of the accumulator, store of the local expansions
+//   warps 2..9  gather source rows (FP32), split to bf16 pieces, store in the swizzled K-major layout
+//   warps 10-13 drain: every few offsets tcgen05.ld the accumulator and add it to the FP32 local
+//               expansions in global memory (the tensor-core accumulation truncates; long chains
+//               into one TMEM value lose accuracy), then release TMEM for a fresh accumulation
 // Stages hold one K chunk (64 wide with two pieces, 32 with three) of every piece of A and of T_o; two stages rotate through
 // mbarriers (full: producers + bulk-copy bytes, empty: tcgen05.commit). Every wait is bounded by
 // a 2 s global-timer limit; on expiry the CTA records FMM timeout in the error word and stops.
+#include <cstdlib>
+
 #include <cuda_bf16.h>
 
 #include "fmm_internal.cuh"
@@ -34,7 +38,7 @@ constexpr int TT = 42;               // target boxes per tile
 constexpr int ROWS = 128;            // MMA M
 // (the K chunk width depends on the number of bf16 pieces, see Layout)
 constexpr int NPROD = 256;           // producer threads
-constexpr int NTHREADS = 320;
+constexpr int NTHREADS = 448;
 constexpr uint64_t TIMEOUT_NS = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
@@ -216,7 +220,7 @@ __global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int
 template <int NP>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int Lp, int nChunks,
-       const uint8_t* __restrict__ img, const float* __restrict__ M, float* __restrict__ Lc, int* err)
+       const uint8_t* __restrict__ img, const float* __restrict__ M, float* __restrict__ Lc, int drainEvery, int* err)
 {
    using namespace tc;
    using Lay = Layout<NP>;
@@ -236,7 +240,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    const uint32_t base = (rawAddr + 1023u) & ~1023u;
    uint8_t* sbase = smraw + (base - rawAddr);
    uint8_t* ctrl = sbase + 2 * stageBytes;
-   uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);          // full[2], empty[2], done
+   uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);          // full[2], empty[2], done, drainFull, drainEmpty
    uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 64);
    volatile int* abortFlag = reinterpret_cast<volatile int*>(ctrl + 68);
    uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 72);  // 10 words: offsets present in the tile
@@ -248,6 +252,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    const int first = blockIdx.x * TT;
    const int nTile = min(TT, nTargets - first);
    const uint32_t fullBar0 = smemAddr(&bars[0]), emptyBar0 = smemAddr(&bars[2]), doneBar = smemAddr(&bars[4]);
+   const uint32_t drainFull = smemAddr(&bars[5]), drainEmpty = smemAddr(&bars[6]);
 
    if(tid < 10) present[tid] = 0;
    if(tid < TT) tileNode[tid] = tid < nTile ? targets[first + tid] : -1;
@@ -259,6 +264,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       mbarInit(emptyBar0, 1);
       mbarInit(emptyBar0 + 8, 1);
       mbarInit(doneBar, 1);
+      mbarInit(drainFull, 1);
+      mbarInit(drainEmpty, 128);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
    if(warp == 0)
@@ -297,6 +304,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          const uint32_t idA = instrDescBf16(ROWS, N <= 256 ? N : 256);
          const uint32_t idB = nB > 0 ? instrDescBf16(ROWS, nB) : 0u;
          bool firstMma = true;
+         int drains = 0;
          for(int it = 0; it < nItems; it++)
          {
             const int s = it & 1;
@@ -322,6 +330,24 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                }
             }
             mmaCommit(emptyBar0 + 8 * s);
+            // every drainEvery offsets (and after the last) hand the accumulator to the drain warps
+            // and start a fresh one: the tensor cores' FP32 accumulation truncates, so long chains
+            // of accumulations into one TMEM value drift; the running sum is kept in FP32 instead
+            if(it % nChunks == nChunks - 1)
+            {
+               const int oi = it / nChunks;
+               if((oi + 1) % drainEvery == 0 || oi == nOff - 1)
+               {
+                  mmaCommit(drainFull);
+                  if(oi != nOff - 1)
+                  {
+                     if(!mbarWait(drainEmpty, drains & 1, err, abortFlag)) break;
+                     fenceAfterSync();
+                  }
+                  drains++;
+                  firstMma = true;
+               }
+            }
          }
          mmaCommit(doneBar);
       }
@@ -344,9 +370,39 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       }
       __syncwarp();
    }
+   else if(warp >= 10)
+   {
+      // drain warps 10..13: TMEM lanes 32 (warp % 4) .. + 31, one accumulator row per thread
+      const int lanes = 32 * (warp & 3);
+      const int r = lanes + lane;
+      const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
+      float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
+      const int nDrains = (nOff + drainEvery - 1) / drainEvery;
+      for(int d = 0; d < nDrains; d++)
+      {
+         if(!mbarWait(drainFull, d & 1, err, abortFlag)) break;
+         fenceAfterSync();
+         for(int c0 = 0; c0 < N; c0 += 16)
+         {
+            float v[16];
+            tmemLd16(tmem + (uint32_t(lanes) << 16) + uint32_t(c0), v);
+            if(et >= 0)
+            {
+               if(d == 0)
+                  for(int i = 0; i < 16; i++) out[c0 + i] = v[i];
+               else
+                  for(int i = 0; i < 16; i++) out[c0 + i] += v[i];
+            }
+         }
+         fenceBeforeSync();
+         mbarArrive(drainEmpty);
+      }
+      if(nOff == 0 && et >= 0)
+         for(int c = 0; c < N; c++) out[c] = 0.f;
+   }
    else
    {
-      // producers: two threads per row, KCH / 2 K-elements each
+      // producers (warps 2..9): two threads per row, KCH / 2 K-elements each
       constexpr int PER = KCH / 2;
       const int ptid = tid - 64;
       const int row = ptid >> 1, half = ptid & 1;
@@ -401,25 +457,6 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          fenceProxyAsync();
          mbarArrive(fullBar0 + 8 * s);
       }
-      // epilogue on warps 2..5: TMEM lanes 32 (warp % 4) .. + 31
-      if(warp < 6)
-      {
-         const bool ok = mbarWait(doneBar, 0, err, abortFlag);
-         fenceAfterSync();
-         const int lanes = 32 * (warp & 3);
-         const int r = lanes + lane;
-         const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
-         float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
-         for(int c0 = 0; c0 < N; c0 += 16)
-         {
-            float v[16];
-            if(ok && nItems > 0) tmemLd16(tmem + (uint32_t(lanes) << 16) + uint32_t(c0), v);
-            else
-               for(int i = 0; i < 16; i++) v[i] = 0.f;
-            if(et >= 0)
-               for(int i = 0; i < 16; i++) out[c0 + i] = v[i];
-         }
-      }
    }
    fenceBeforeSync();
    __syncthreads();
@@ -456,9 +493,11 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(smem > 232448) return setError(FMM_E_INVALID, "tensor-core M2L: %zu bytes of shared memory needed", smem);
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   int drainEvery = 8;
+   if(const char* e = getenv("FMM_TC_DRAIN")) drainEvery = std::max(1, atoi(e));
    kM2LTc<NP><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, Lp, nChunks,
                                                  (const uint8_t*)P.opM2Lbf.ptr, (const float*)P.mult.ptr,
-                                                 (float*)P.local.ptr, P.err);
+                                                 (float*)P.local.ptr, drainEvery, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    int herr = 0;
    FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));

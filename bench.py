@@ -220,7 +220,7 @@ def main():
     size = tuple(int(v) for v in args.size.split(","))
     xyz, w, J = make_workload(*size)
     n = len(xyz)
-    m2l = "bf16x6" if args.m2l == "auto" else args.m2l
+    m2l = "bf16x3" if args.m2l == "auto" else args.m2l
     dev = f"cuda:{local}"
     d_xyz = torch.from_numpy(xyz).to(dev)
     d_w = torch.from_numpy(w).to(dev)
