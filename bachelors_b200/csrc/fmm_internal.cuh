@@ -43,6 +43,7 @@ enum : int {
 
 extern __constant__ int d_m2lIndex[NOFF];   // offset index (0..342) -> M2L slot (0..315) or -1
 extern __constant__ int d_m2lOffset[316];   // M2L slot -> offset index
+extern __constant__ int d_m2lFarFirst[316]; // M2L slots by decreasing offset length
 
 // A growable device allocation.
 struct DevBuf

@@ -14,6 +14,8 @@
 //   L2P   CalculationPointOctreeNode::calcA / calcRot        calculation_point_octree.cpp:192-275
 //         (B from analytic gradients here, finite differences there)
 //   near  bioSavartLaplaceFunction                           integration.cpp:113-120
+#include <algorithm>
+
 #include <cuda_bf16.h>
 
 #include "fmm_internal.cuh"
@@ -22,6 +24,7 @@ namespace fmm {
 
 __constant__ int d_m2lIndex[NOFF];
 __constant__ int d_m2lOffset[316];
+__constant__ int d_m2lFarFirst[316];
 
 // Constant memory is per device context: fill it once on every device that uses the library.
 fmm_status initOffsetTables()
@@ -40,6 +43,15 @@ fmm_status initOffsetTables()
             if(abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1) idx[o] = -1;
             else { idx[o] = k; off[k] = o; k++; }
          }
+   int far[316];
+   for(int i = 0; i < 316; i++) far[i] = i;
+   auto len2 = [&](int slot) {
+      int o = off[slot];
+      int ox = o % 7 - 3, oy = (o / 7) % 7 - 3, oz = o / 49 - 3;
+      return ox * ox + oy * oy + oz * oz;
+   };
+   std::stable_sort(far, far + 316, [&](int a, int b) { return len2(a) > len2(b); });
+   FMM_CUDA(cudaMemcpyToSymbol(d_m2lFarFirst, far, sizeof(far)));
    FMM_CUDA(cudaMemcpyToSymbol(d_m2lIndex, idx, sizeof(idx)));
    FMM_CUDA(cudaMemcpyToSymbol(d_m2lOffset, off, sizeof(off)));
    if(dev < 64) done[dev] = true;
@@ -584,7 +596,9 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
          });
          for(int d = 0; d < 3; d++) { B[d] *= ih2; A[d] *= ih; }
       }
-      // direct near field
+      // direct near field: each source tile is summed in T, the tile sums in FP64, so no
+      // single-precision chain is longer than one tile
+      double Bs[3] = {double(B[0]), double(B[1]), double(B[2])}, As[3] = {double(A[0]), double(A[1]), double(A[2])};
       for(int e = e0; e < e1; e++)
       {
          const int S = p2pList[e];
@@ -596,6 +610,8 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
             if(threadIdx.x < cnt) { Sp[threadIdx.x] = spos[sb + threadIdx.x]; Sq[threadIdx.x] = sq[sb + threadIdx.x]; }
             __syncthreads();
             if(active)
+            {
+               T pb[3] = {T(0), T(0), T(0)}, pa[3] = {T(0), T(0), T(0)};
                for(int i = 0; i < cnt; i++)
                {
                   const V4 y = Sp[i], w = Sq[i];
@@ -606,18 +622,20 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
                   if constexpr(sizeof(T) == 4) ri = rsqrtf(r2);
                   else ri = rsqrt(r2);
                   const T ri3 = ri * ri * ri;
-                  B[0] += (w.y * dz - w.z * dy) * ri3;
-                  B[1] += (w.z * dx - w.x * dz) * ri3;
-                  B[2] += (w.x * dy - w.y * dx) * ri3;
-                  A[0] += w.x * ri; A[1] += w.y * ri; A[2] += w.z * ri;
+                  pb[0] += (w.y * dz - w.z * dy) * ri3;
+                  pb[1] += (w.z * dx - w.x * dz) * ri3;
+                  pb[2] += (w.x * dy - w.y * dx) * ri3;
+                  pa[0] += w.x * ri; pa[1] += w.y * ri; pa[2] += w.z * ri;
                }
+               for(int d = 0; d < 3; d++) { Bs[d] += double(pb[d]); As[d] += double(pa[d]); }
+            }
          }
       }
       if(active)
       {
          const int o = tOrder[ti];
-         if(want & 1) for(int d = 0; d < 3; d++) outB[3 * int64_t(o) + d] = B[d] * scaleB;
-         if(want & 2) for(int d = 0; d < 3; d++) outA[3 * int64_t(o) + d] = A[d] * scaleA;
+         if(want & 1) for(int d = 0; d < 3; d++) outB[3 * int64_t(o) + d] = T(Bs[d] * double(scaleB));
+         if(want & 2) for(int d = 0; d < 3; d++) outA[3 * int64_t(o) + d] = T(As[d] * double(scaleA));
       }
    }
 }

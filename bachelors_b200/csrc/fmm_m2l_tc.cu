@@ -286,9 +286,13 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    fenceAfterSync();
    if(tid == 0)
    {
+      // far offsets first: the smaller contributions enter the accumulator before the large ones
       int k = 0;
-      for(int o = 0; o < 316; o++)
+      for(int i = 0; i < 316; i++)
+      {
+         const int o = d_m2lFarFirst[i];
          if(present[o >> 5] & (1u << (o & 31))) itemOffset[k++] = o;
+      }
       itemOffset[316] = k;
    }
    __syncthreads();
@@ -361,7 +365,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          {
             const int s = it & 1;
             if(it >= 2 && !mbarWait(emptyBar0 + 8 * s, ((it >> 1) - 1) & 1, err, abortFlag)) break;
-            const int o = itemOffset[it / nChunks], c = it % nChunks;
+            const int o = itemOffset[it / nChunks], c = nChunks - 1 - it % nChunks;
             const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
             const uint32_t dst = base + s * stageBytes + NP * aBytes;
             mbarArriveExpectTx(fullBar0 + 8 * s, NP * bBytes);
@@ -378,6 +382,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
       float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
       const int nDrains = (nOff + drainEvery - 1) / drainEvery;
+      // The running sum lives in the (zero-initialised) local expansions: fire-and-forget FP32
+      // vector adds, rounded to nearest. Each row has one writer, this thread, and same-address
+      // operations of one thread stay in program order, so the result is deterministic.
       for(int d = 0; d < nDrains; d++)
       {
          if(!mbarWait(drainFull, d & 1, err, abortFlag)) break;
@@ -388,17 +395,14 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             tmemLd16(tmem + (uint32_t(lanes) << 16) + uint32_t(c0), v);
             if(et >= 0)
             {
-               if(d == 0)
-                  for(int i = 0; i < 16; i++) out[c0 + i] = v[i];
-               else
-                  for(int i = 0; i < 16; i++) out[c0 + i] += v[i];
+               float4* o4 = reinterpret_cast<float4*>(out + c0);
+#pragma unroll
+               for(int i = 0; i < 4; i++) atomicAdd(o4 + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
             }
          }
          fenceBeforeSync();
          mbarArrive(drainEmpty);
       }
-      if(nOff == 0 && et >= 0)
-         for(int c = 0; c < N; c++) out[c] = 0.f;
    }
    else
    {
@@ -412,7 +416,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       {
          const int s = it & 1;
          if(it >= 2 && !mbarWait(emptyBar0 + 8 * s, ((it >> 1) - 1) & 1, err, abortFlag)) break;
-         const int o = itemOffset[it / nChunks], c = it % nChunks;
+         const int o = itemOffset[it / nChunks], c = nChunks - 1 - it % nChunks;
          const int src = tgt >= 0 ? vtab[int64_t(tgt) * 316 + o] : -1;
          uint8_t* aSt = sbase + s * stageBytes;
          const int k0 = c * KCH + half * PER;
@@ -493,7 +497,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(smem > 232448) return setError(FMM_E_INVALID, "tensor-core M2L: %zu bytes of shared memory needed", smem);
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
-   int drainEvery = 8;
+   int drainEvery = 4;
    if(const char* e = getenv("FMM_TC_DRAIN")) drainEvery = std::max(1, atoi(e));
    kM2LTc<NP><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, Lp, nChunks,
                                                  (const uint8_t*)P.opM2Lbf.ptr, (const float*)P.mult.ptr,
