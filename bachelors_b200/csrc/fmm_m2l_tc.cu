@@ -497,7 +497,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(smem > 232448) return setError(FMM_E_INVALID, "tensor-core M2L: %zu bytes of shared memory needed", smem);
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
-   int drainEvery = 4;
+   int drainEvery = 8;
    if(const char* e = getenv("FMM_TC_DRAIN")) drainEvery = std::max(1, atoi(e));
    kM2LTc<NP><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, Lp, nChunks,
                                                  (const uint8_t*)P.opM2Lbf.ptr, (const float*)P.mult.ptr,

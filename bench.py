@@ -203,6 +203,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison solve")
+    ap.add_argument("--no-launch-count", action="store_true", help="skip the profiler-based launch count")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -324,7 +325,7 @@ def main():
         if "plain_fp32" in line:
             line["speedup_vs_plain_fp32"] = line["value"] / line["plain_fp32"]["value"]
 
-    if rank == 0:
+    if rank == 0 and not args.no_launch_count:
         try:
             total, ours, names = count_launches(plan)
             line["gpu_launches"] = ours * args.steps
