@@ -133,6 +133,19 @@ fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats);
  * box-size-scaled basis the pipeline uses. */
 fmm_status fmm_get_operator(fmm_plan* plan, int kind, int index, double* out);
 
+/* No counterpart in the reference. The direct FP32 sum of fmm_direct (B only, coincident pairs
+ * skipped, J == NULL: azimuthal direction) for callers that cannot let a library allocate device
+ * memory: their GPU memory belongs to another allocator, or their host loop cannot afford a
+ * cudaMalloc that may synchronise the device or fail. Inputs xyz[3n], w[n], J[3n] (or NULL) and
+ * tgt[3m] and the output out_B[3m] are device pointers on the current device; work is queued on
+ * `stream` and the call does not wait for it. The only scratch, the packed sources, lives in a
+ * fixed 8 MiB device array inside the library, present on every GPU that loads it until the
+ * process exits: n is limited to 262,144 sources (FMM_E_LIMIT beyond). The first call on a device
+ * looks up that array's address (make it before any stream capture). All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. Never allocates. */
+fmm_status fmm_direct_B_noalloc(const float* xyz, const float* w, const float* J, int64_t n, const float* tgt,
+                                int64_t m, double current, float* out_B, void* stream);
+
 /* kernels::addVectors (FMMCUDADLL/kernel_callers.hpp:7-9): c = a + b for host arrays of n floats. */
 fmm_status fmm_add_vectors(const float* a, const float* b, float* c, int64_t n);
 

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "fmmcuda.h")).read()
-    return sorted(set(re.findall(r"\b(fmm_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(fmm_[A-Za-z0-9_]+)\s*\(", text)))
 
 
 def test_header_and_binding_agree():
