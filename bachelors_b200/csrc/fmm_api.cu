@@ -64,6 +64,45 @@ fmm_status Plan::ensureNodes(int64_t cap, cudaStream_t st)
    return FMM_OK;
 }
 
+fmm_status Plan::init(const fmm_config& c)
+{
+   cfg = c;
+   p = c.order;
+   L = nharm(p);
+   Lp = padded(L);
+   fp64 = c.precision == FMM_FP64;
+   const char* dbg = getenv("FMM_DEBUG_SYNC");
+   debugSync = dbg && dbg[0] == '1';
+   FMM_TRY(rootb.reserve(sizeof(RootBox)));
+   FMM_TRY(errb.reserve(sizeof(int)));
+   FMM_TRY(initOffsetTables());
+   root = (RootBox*)rootb.ptr;
+   err = (int*)errb.ptr;
+   for(int i = 0; i < 8; i++) cudaEventCreate(&ev[i]);
+   eventsMade = true;
+   return FMM_OK;
+}
+
+void Plan::release()
+{
+   if(adj)
+   {
+      adj->release();
+      delete adj;
+      adj = nullptr;
+   }
+   DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
+                     &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &m2lTargets, &m2lKeys, &errb,
+                     &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf,
+                     &adjG, &adjOut};
+   for(DevBuf* b : bufs) b->release();
+   for(auto& b : nodeBufs) b.release();
+   for(auto& b : listBufs) b.release();
+   if(eventsMade)
+      for(int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+   eventsMade = false;
+}
+
 fmm_status Plan::ensureLists(int64_t cap)
 {
    if(cap <= listCap) return FMM_OK;
@@ -173,25 +212,8 @@ fmm_status fmm_plan_create(const fmm_config* cfg, fmm_plan** plan)
    if(cfg->device < 0 || cfg->device >= ndev) return setError(FMM_E_INVALID, "device %d out of range", cfg->device);
    DeviceGuard g(cfg->device);
    fmm_plan* h = new fmm_plan();
-   Plan& P = h->P;
-   P.cfg = *cfg;
-   P.p = cfg->order;
-   P.L = nharm(P.p);
-   P.Lp = padded(P.L);
-   P.fp64 = cfg->precision == FMM_FP64;
-   {
-      const char* dbg = getenv("FMM_DEBUG_SYNC");
-      P.debugSync = dbg && dbg[0] == '1';
-   }
-   fmm_status s = P.rootb.reserve(sizeof(RootBox));
-   if(s == FMM_OK) s = P.errb.reserve(sizeof(int));
+   fmm_status s = h->P.init(*cfg);
    if(s != FMM_OK) { delete h; return s; }
-   if(s == FMM_OK) s = initOffsetTables();
-   if(s != FMM_OK) { delete h; return s; }
-   P.root = (RootBox*)P.rootb.ptr;
-   P.err = (int*)P.errb.ptr;
-   for(int i = 0; i < 8; i++) cudaEventCreate(&P.ev[i]);
-   P.eventsMade = true;
    *plan = h;
    return FMM_OK;
 }
@@ -199,17 +221,8 @@ fmm_status fmm_plan_create(const fmm_config* cfg, fmm_plan** plan)
 fmm_status fmm_plan_destroy(fmm_plan* plan)
 {
    if(!plan) return FMM_OK;
-   Plan& P = plan->P;
-   DeviceGuard g(P.cfg.device);
-   DevBuf* bufs[] = {&P.srcXYZb, &P.srcWb, &P.srcJb, &P.tgtXYZb, &P.rootb, &P.sKeys, &P.tKeys, &P.sIdx, &P.tIdx,
-                     &P.sPos, &P.sQ, &P.tPos, &P.cubTmp, &P.scratch, &P.lvlBounds, &P.lvlCnt, &P.lvlOff,
-                     &P.p2pOff, &P.p2pList, &P.m2lTargets, &P.m2lKeys, &P.errb, &P.mult, &P.local, &P.outB, &P.outA, &P.opM2M64,
-                     &P.opL2L64, &P.opM2L64, &P.opM2Mw, &P.opL2Lw, &P.opM2Lw, &P.opM2Lbf};
-   for(DevBuf* b : bufs) b->release();
-   for(auto& b : P.nodeBufs) b.release();
-   for(auto& b : P.listBufs) b.release();
-   if(P.eventsMade)
-      for(int i = 0; i < 8; i++) cudaEventDestroy(P.ev[i]);
+   DeviceGuard g(plan->P.cfg.device);
+   plan->P.release();
    delete plan;
    return FMM_OK;
 }
@@ -380,6 +393,52 @@ fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* 
    return s;
 }
 
+fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx, int on_device,
+                       void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(P.n == 0 || P.m == 0) return setError(FMM_E_INVALID, "fmm_adjoint: sources and targets must be set");
+   if(!dL_dB || (!dL_dJ && !dL_dx)) return setError(FMM_E_INVALID, "fmm_adjoint: null argument");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   if(!P.adj)
+   {
+      fmm_config c = P.cfg;
+      // roles swap: the forward targets are the adjoint sources
+      c.leaf_capacity = P.cfg.target_leaf_capacity > 0 ? P.cfg.target_leaf_capacity : P.cfg.leaf_capacity;
+      c.target_leaf_capacity = P.cfg.leaf_capacity;
+      P.adj = new Plan();
+      fmm_status s = P.adj->init(c);
+      if(s != FMM_OK) { P.adj->release(); delete P.adj; P.adj = nullptr; return s; }
+   }
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   const void* gDev = dL_dB;
+   void* dJ = dL_dJ;
+   void* dx = dL_dx;
+   if(!on_device)
+   {
+      FMM_TRY(P.adjG.reserve(es * 3 * P.m));
+      FMM_CUDA(cudaMemcpyAsync(P.adjG.ptr, dL_dB, es * 3 * P.m, cudaMemcpyHostToDevice, st));
+      gDev = P.adjG.ptr;
+      FMM_TRY(P.adjOut.reserve(2 * es * 3 * P.n));
+      dJ = dL_dJ ? P.adjOut.ptr : nullptr;
+      dx = dL_dx ? (char*)P.adjOut.ptr + es * 3 * P.n : nullptr;
+   }
+   cudaEventRecord(P.ev[6], st);
+   FMM_TRY(P.fp64 ? adjointT<double>(P, *P.adj, current, gDev, dJ, dx, st)
+                  : adjointT<float>(P, *P.adj, current, gDev, dJ, dx, st));
+   cudaEventRecord(P.ev[7], st);
+   P.adjointDone = true;
+   if(!on_device)
+   {
+      if(dL_dJ) FMM_CUDA(cudaMemcpyAsync(dL_dJ, dJ, es * 3 * P.n, cudaMemcpyDeviceToHost, st));
+      if(dL_dx) FMM_CUDA(cudaMemcpyAsync(dL_dx, dx, es * 3 * P.n, cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+   }
+   return FMM_OK;
+}
+
 fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats)
 {
    if(!plan || !stats) return setError(FMM_E_INVALID, "null argument");
@@ -393,6 +452,11 @@ fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats)
    s.ms_downward = elapsed(P.ev[2], P.ev[4]);
    s.ms_near = elapsed(P.ev[4], P.ev[5]);
    s.ms_total = elapsed(P.ev[0], P.ev[5]);
+   if(P.adjointDone)
+   {
+      cudaEventSynchronize(P.ev[7]);
+      s.ms_adjoint = elapsed(P.ev[6], P.ev[7]);
+   }
    s.nodes = P.tree.nNodes;
    s.levels = P.tree.nLevels;
    s.p2p_pairs = P.nP2P;

@@ -137,6 +137,13 @@ struct Plan
    int64_t launches = 0;      // kernels this plan launched (all phases, cumulative)
    bool debugSync = false;    // FMM_DEBUG_SYNC=1: synchronise and check after every launch
 
+   // adjoint: a plan on the swapped point sets, and staging for host inputs / outputs
+   Plan* adj = nullptr;
+   DevBuf adjG, adjOut;
+   bool adjointDone = false;
+
+   fmm_status init(const fmm_config& c);
+   void release();
    fmm_status ensureNodes(int64_t cap, cudaStream_t st = 0);
    fmm_status ensureLists(int64_t cap);
 };
@@ -162,5 +169,6 @@ template <class T> fmm_status directT(Plan& P, double current, int want, cudaStr
 fmm_status buildOperators(Plan& P, cudaStream_t st);
 fmm_status initOffsetTables();
 fmm_status m2lTensorCore(Plan& P, cudaStream_t st);
+template <class T> fmm_status adjointT(Plan& P, Plan& A, double current, const void* g, void* dJ, void* dx, cudaStream_t st);
 
 }  // namespace fmm

@@ -136,6 +136,7 @@ class Plan:
         wb = _Buffer(w, self.np_dtype, self.torch_dtype, ())
         jb = _Buffer(J, self.np_dtype, self.torch_dtype, (3,)) if J is not None else None
         self.device_mode = x.device
+        self.n = x.n
         _lib.check(self.lib.fmm_set_sources(self.handle, ctypes.c_void_p(x.ptr), ctypes.c_void_p(wb.ptr),
                                             ctypes.c_void_p(jb.ptr) if jb else None, x.n, int(x.device),
                                             self._stream()))
@@ -148,10 +149,11 @@ class Plan:
         self.m = t.n
         self._keep.append(t)
 
-    def _out(self):
+    def _out(self, rows=None):
+        rows = self.m if rows is None else rows
         if self.device_mode:
-            return torch.empty((self.m, 3), dtype=self.torch_dtype, device=f"cuda:{self.cfg.device}")
-        return np.empty((self.m, 3), dtype=self.np_dtype)
+            return torch.empty((rows, 3), dtype=self.torch_dtype, device=f"cuda:{self.cfg.device}")
+        return np.empty((rows, 3), dtype=self.np_dtype)
 
     @staticmethod
     def _ptr(a):
@@ -183,6 +185,18 @@ class Plan:
 
     def direct(self, current=1.0, want=1):
         return self._run(self.lib.fmm_direct, current, want)
+
+    def adjoint(self, g, current=1.0, want_dJ=True, want_dx=True):
+        """Adjoint FMM: for g = dLoss/dB at the targets ([M,3]) returns (dLoss/dJ, dLoss/d(source
+        positions)), each [N,3] or None."""
+        gb = _Buffer(g, self.np_dtype, self.torch_dtype, (3,))
+        if gb.device != self.device_mode:
+            raise ValueError("g must live where the plan's inputs live (host numpy or CUDA tensor)")
+        dJ = self._out(self.n) if want_dJ else None
+        dx = self._out(self.n) if want_dx else None
+        _lib.check(self.lib.fmm_adjoint(self.handle, ctypes.c_double(current), ctypes.c_void_p(gb.ptr), self._ptr(dJ),
+                                        self._ptr(dx), int(self.device_mode), self._stream()))
+        return dJ, dx
 
     def direct_fp64(self, targets, current=1.0):
         t = np.ascontiguousarray(np.asarray(targets, dtype=np.float64).reshape(-1, 3))
@@ -267,6 +281,10 @@ class FastMultipoleSolver(MultipoleSolver):
         B, A = self.plan.solve(current, w)
         self._multipoles = self._locals = True
         return {"B": B, "A": A, "AB": (B, A)}[want]
+
+    def adjoint(self, dL_dB, current=1.0):
+        """(dLoss/dJ, dLoss/d(source positions)) for dLoss/dB at the points."""
+        return self.plan.adjoint(dL_dB, current)
 
     def stats(self):
         return self.plan.stats()

@@ -78,6 +78,7 @@ typedef struct fmm_stats {
    double ms_tree, ms_upward, ms_m2l, ms_downward, ms_near, ms_total;
    int64_t nodes, leaves, levels, v_pairs, p2p_pairs, p2p_interactions;
    int64_t n_sources, n_targets;
+   double ms_adjoint; /* the last fmm_adjoint call */
 } fmm_stats;
 
 void fmm_default_config(fmm_config* cfg);
@@ -124,6 +125,17 @@ fmm_status fmm_direct(fmm_plan* plan, double current, int want, void* out_B, voi
 /* FP64 direct B on the device for an explicit target subset (accuracy checks): tgt[3k]
  * host doubles, out_B[3k] host doubles. Uses the plan's sources. */
 fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* tgt, int64_t k, double* out_B);
+
+/* Adjoint FMM (no counterpart in the reference, which has no gradients). Given dLoss/dB at the
+ * plan's targets, g[3m], returns dLoss/dJ[3n] and dLoss/d(source positions)[3n] (either output may
+ * be NULL) for B as computed by fmm_solve with the same `current`:
+ *   dLoss/dJ_q = MU0 I/(4 PI) w_q sum_t g_t x (q - x_t)/|q - x_t|^3
+ *   dLoss/dq   = MU0 I/(4 PI) w_q grad_q (J_q . C(q)),  C(q) = sum_t g_t x (q - x_t)/|q - x_t|^3
+ * (plus the derivative of the azimuthal direction when J was NULL). It runs one FMM on the
+ * swapped point sets (targets as sources of strength g) with first and second derivatives of the
+ * local expansions. Weights are constants. Element type and on_device as in fmm_evaluate. */
+fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx, int on_device,
+                       void* stream);
 
 fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats);
 

@@ -575,6 +575,55 @@ void orc_direct(int64_t n, const double* src, const double* w, const double* J, 
    }
 }
 
+// Adjoint of the direct Biot-Savart sum (no reference counterpart: the reference has no
+// gradients). With g_t = dLoss/dB(x_t) and c = mu0/(4 pi) I:
+//   dLoss/dJ_q = c w_q sum_t g_t x (q - x_t) / |q - x_t|^3
+//   dLoss/dq   = c w_q sum_t [ a / r^3 - 3 (e . a) e / r^5 ],  e = q - x_t, a = J_q x g_t
+// plus, when J is the azimuthal direction of q (J == nullptr), the term c w_q (dJ/dq)^T C(q)
+// with C(q) = sum_t g_t x (q - x_t) / r^3. Coincident pairs are skipped. Outputs [3n].
+void orc_adjoint_direct(int64_t n, const double* src, const double* w, const double* J, int64_t m,
+                        const double* tgt, const double* g, double current, double* dJ, double* dx)
+{
+   const double c = REF_MU0 / (4 * REF_PI) * current;
+#pragma omp parallel for schedule(dynamic, 8)
+   for(int64_t q = 0; q < n; q++)
+   {
+      double Jq[3];
+      currentOf(J, src, q, Jq);
+      double C[3] = {0, 0, 0}, G[3] = {0, 0, 0};
+      for(int64_t t = 0; t < m; t++)
+      {
+         double e[3] = {src[3 * q] - tgt[3 * t], src[3 * q + 1] - tgt[3 * t + 1], src[3 * q + 2] - tgt[3 * t + 2]};
+         double r2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+         if(r2 == 0) continue;
+         double r = std::sqrt(r2), ir3 = 1.0 / (r2 * r), ir5 = ir3 / r2;
+         const double* gt = g + 3 * t;
+         C[0] += (gt[1] * e[2] - gt[2] * e[1]) * ir3;
+         C[1] += (gt[2] * e[0] - gt[0] * e[2]) * ir3;
+         C[2] += (gt[0] * e[1] - gt[1] * e[0]) * ir3;
+         double a[3] = {Jq[1] * gt[2] - Jq[2] * gt[1], Jq[2] * gt[0] - Jq[0] * gt[2], Jq[0] * gt[1] - Jq[1] * gt[0]};
+         double ea = e[0] * a[0] + e[1] * a[1] + e[2] * a[2];
+         for(int d = 0; d < 3; d++) G[d] += a[d] * ir3 - 3 * ea * e[d] * ir5;
+      }
+      if(!J)
+      {
+         double x = src[3 * q], y = src[3 * q + 1];
+         double rho2 = x * x + y * y;
+         if(rho2 > 0)
+         {
+            double ir = 1.0 / (rho2 * std::sqrt(rho2));
+            G[0] += (x * y * C[0] + y * y * C[1]) * ir;
+            G[1] += (-x * x * C[0] - x * y * C[1]) * ir;
+         }
+      }
+      for(int d = 0; d < 3; d++)
+      {
+         if(dJ) dJ[3 * q + d] = c * w[q] * C[d];
+         if(dx) dx[3 * q + d] = c * w[q] * G[d];
+      }
+   }
+}
+
 // Standard-mode FMM (the B200 pipeline's definition) at order p, leaf capacity `cap`,
 // root cube (center, H). Outputs in input order; either may be null. stats (may be null)
 // receives: [0] nodes, [1] levels, [2] leaves, [3] V entries, [4] U entries, [5] W entries,

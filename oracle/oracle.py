@@ -221,3 +221,17 @@ class Reference:
         found = self.lib.ref_fmm(len(xyzw), _d(xyzw), len(pts), _d(pts), cap_src, cap_tgt, ctypes.c_double(current),
                                  int(want_B), _d(out), _d(times))
         return out, found, times
+
+
+def adjoint_direct(src, w, J, tgt, g, current=1.0):
+    """FP64 direct-sum adjoint: (dLoss/dJ [N,3], dLoss/d(source positions) [N,3]) for g = dLoss/dB."""
+    src = _c64(src).reshape(-1, 3)
+    tgt = _c64(tgt).reshape(-1, 3)
+    g = _c64(g).reshape(-1, 3)
+    w = _c64(w)
+    Jc = _c64(J).reshape(-1, 3) if J is not None else None
+    dJ = np.zeros((len(src), 3))
+    dx = np.zeros((len(src), 3))
+    _load().orc_adjoint_direct(ctypes.c_int64(len(src)), _d(src), _d(w), _d(Jc), ctypes.c_int64(len(tgt)), _d(tgt),
+                               _d(g), ctypes.c_double(current), _d(dJ), _d(dx))
+    return dJ, dx
