@@ -24,7 +24,8 @@ def case(seed=3, azimuthal=False):
     return xyz, w, (None if azimuthal else Jp), tgt
 
 
-@pytest.mark.parametrize("precision,tolJ,tolx", [("fp64", 1e-6, 1e-5), ("fp32", 2e-5, 1e-4)])
+# tolerances: the FMM truncation error at p = 12 (about 1e-6 for B here), loosened for FP32
+@pytest.mark.parametrize("precision,tolJ,tolx", [("fp64", 5e-6, 2e-5), ("fp32", 2e-5, 1e-4)])
 @pytest.mark.parametrize("azimuthal", [False, True])
 def test_adjoint_matches_direct_adjoint(precision, tolJ, tolx, azimuthal):
     xyz, w, J, tgt = case(azimuthal=azimuthal)
