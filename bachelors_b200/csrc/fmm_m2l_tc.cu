@@ -14,15 +14,16 @@
 // products hi*hi + hi*lo + lo*hi (BF16X3), or x = hi + mid + lo with the six products down to
 // 2^-16 relative (BF16X6); all are accumulated in FP32 in tensor memory.
 //
-// Warp roles (320 threads):
+// Warp roles (448 threads):
 //   warp 0      TMEM allocation; lane 0 issues the tcgen05.mma instructions
 //   warp 1      lane 0 streams the pre-swizzled operator image with cp.async.bulk (no multicast)
 //   warps 2..9  gather source rows (FP32), split to bf16 pieces, store in the swizzled K-major layout
 //   warps 10-13 drain: every few offsets tcgen05.ld the accumulator and add it to the FP32 local
 //               expansions in global memory (the tensor-core accumulation truncates; long chains
 //               into one TMEM value lose accuracy), then release TMEM for a fresh accumulation
-// Stages hold one K chunk (64 wide with two pieces, 32 with three) of every piece of A and of T_o; two stages rotate through
-// mbarriers (full: producers + bulk-copy bytes, empty: tcgen05.commit). Every wait is bounded by
+// Stages hold one 32-wide K chunk of every piece of A and of T_o; four (two pieces) or two (three
+// pieces) stages rotate through mbarriers (full: producers + bulk-copy bytes, empty:
+// tcgen05.commit). Every wait is bounded by
 // a 2 s global-timer limit; on expiry the CTA records FMM timeout in the error word and stops.
 #include <cstdlib>
 
@@ -145,19 +146,13 @@ __device__ __forceinline__ void tmemLd16(uint32_t addr, float* v)
 }
 
 
-// Operand layouts. NP bf16 pieces per value (2: hi + lo, 3: hi + mid + lo). With two pieces a
-// K chunk is 64 elements in 128-byte rows (SW128); with three it is 32 elements in 64-byte rows
-// (SW64) so that two pipeline stages still fit in shared memory.
-template <int NP> struct Layout;
-template <> struct Layout<2>
-{
-   static constexpr int KC = 64, RB = 128, SBO = 1024, SWZ = 2;
-   __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
-   { return row * 128u + ((((k >> 3) ^ (row & 7u)) & 7u) << 4) + ((k & 7u) << 1); }
-};
-template <> struct Layout<3>
+// Operand layout for NP bf16 pieces per value (2: hi + lo, 3: hi + mid + lo): 32-element K chunks
+// in 64-byte rows (SW64). With two pieces a stage is 55 KB and four stages are in flight; with
+// three pieces a stage is 83 KB and two are.
+template <int NP> struct Layout
 {
    static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4;
+   static constexpr int NSTAGE = NP == 2 ? 4 : 2;
    __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
    { return row * 64u + ((((k >> 3) ^ ((row >> 1) & 3u)) & 3u) << 4) + ((k & 7u) << 1); }
 };
@@ -239,30 +234,32 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    const uint32_t rawAddr = smemAddr(smraw);
    const uint32_t base = (rawAddr + 1023u) & ~1023u;
    uint8_t* sbase = smraw + (base - rawAddr);
-   uint8_t* ctrl = sbase + 2 * stageBytes;
-   uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);          // full[2], empty[2], done, drainFull, drainEmpty
-   uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 64);
-   volatile int* abortFlag = reinterpret_cast<volatile int*>(ctrl + 68);
-   uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 72);  // 10 words: offsets present in the tile
-   int* itemOffset = reinterpret_cast<int*>(ctrl + 128);        // compacted present offsets [316] + count
+   constexpr int NS = Lay::NSTAGE;
+   uint8_t* ctrl = sbase + NS * stageBytes;
+   uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);          // full[NS], empty[NS], done, drainFull, drainEmpty
+   uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 128);
+   volatile int* abortFlag = reinterpret_cast<volatile int*>(ctrl + 132);
+   uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 136); // 10 words: offsets present in the tile
+   int* itemOffset = reinterpret_cast<int*>(ctrl + 192);        // compacted present offsets [316] + count
    int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
    const int first = blockIdx.x * TT;
    const int nTile = min(TT, nTargets - first);
-   const uint32_t fullBar0 = smemAddr(&bars[0]), emptyBar0 = smemAddr(&bars[2]), doneBar = smemAddr(&bars[4]);
-   const uint32_t drainFull = smemAddr(&bars[5]), drainEmpty = smemAddr(&bars[6]);
+   const uint32_t fullBar0 = smemAddr(&bars[0]), emptyBar0 = smemAddr(&bars[NS]), doneBar = smemAddr(&bars[2 * NS]);
+   const uint32_t drainFull = smemAddr(&bars[2 * NS + 1]), drainEmpty = smemAddr(&bars[2 * NS + 2]);
 
    if(tid < 10) present[tid] = 0;
    if(tid < TT) tileNode[tid] = tid < nTile ? targets[first + tid] : -1;
    if(tid == 0)
    {
       *abortFlag = 0;
-      mbarInit(fullBar0, NPROD + 1);
-      mbarInit(fullBar0 + 8, NPROD + 1);
-      mbarInit(emptyBar0, 1);
-      mbarInit(emptyBar0 + 8, 1);
+      for(int s = 0; s < NS; s++)
+      {
+         mbarInit(fullBar0 + 8 * s, NPROD + 1);
+         mbarInit(emptyBar0 + 8 * s, 1);
+      }
       mbarInit(doneBar, 1);
       mbarInit(drainFull, 1);
       mbarInit(drainEmpty, 128);
@@ -311,8 +308,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          int drains = 0;
          for(int it = 0; it < nItems; it++)
          {
-            const int s = it & 1;
-            if(!mbarWait(fullBar0 + 8 * s, (it >> 1) & 1, err, abortFlag)) break;
+            const int s = it % NS;
+            if(!mbarWait(fullBar0 + 8 * s, (it / NS) & 1, err, abortFlag)) break;
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
             const uint32_t aSt = st, bSt = st + NP * aBytes;
@@ -363,8 +360,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       {
          for(int it = 0; it < nItems; it++)
          {
-            const int s = it & 1;
-            if(it >= 2 && !mbarWait(emptyBar0 + 8 * s, ((it >> 1) - 1) & 1, err, abortFlag)) break;
+            const int s = it % NS;
+            if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag)) break;
             const int o = itemOffset[it / nChunks], c = nChunks - 1 - it % nChunks;
             const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
             const uint32_t dst = base + s * stageBytes + NP * aBytes;
@@ -414,8 +411,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       const int tgt = row < 3 * TT ? tileNode[slot] : -1;
       for(int it = 0; it < nItems; it++)
       {
-         const int s = it & 1;
-         if(it >= 2 && !mbarWait(emptyBar0 + 8 * s, ((it >> 1) - 1) & 1, err, abortFlag)) break;
+         const int s = it % NS;
+         if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag)) break;
          const int o = itemOffset[it / nChunks], c = nChunks - 1 - it % nChunks;
          const int src = tgt >= 0 ? vtab[int64_t(tgt) * 316 + o] : -1;
          uint8_t* aSt = sbase + s * stageBytes;
@@ -493,7 +490,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(count <= 0) return FMM_OK;
    const int blocks = (count + tc::TT - 1) / tc::TT;
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t smem = 1024 + 2 * stageBytes + 128 + 4 * (320 + 64);
+   const size_t smem = 1024 + Lay::NSTAGE * stageBytes + 192 + 4 * (320 + 64);
    if(smem > 232448) return setError(FMM_E_INVALID, "tensor-core M2L: %zu bytes of shared memory needed", smem);
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));

@@ -204,6 +204,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison solve")
     ap.add_argument("--no-launch-count", action="store_true", help="skip the profiler-based launch count")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -292,6 +293,25 @@ def main():
                      "note": "algorithmic FLOPs = V pairs x 3 components x 2 (p+1)^4; peak = measured bf16 dense"},
         "clocks": clk,
     }
+
+    # adjoint FMM (dLoss/dJ and dLoss/d(source positions)) for g = B - B*, with B* = 1.01 B: one
+    # warm-up and K timed adjoint calls, against the forward solve's time
+    if not args.no_adjoint:
+        g = (B * 0.01).contiguous()
+        plan.adjoint(g, 1.0)
+        torch.cuda.synchronize()
+        barrier(world)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(args.steps):
+            dJ, dx = plan.adjoint(g, 1.0)
+        a1.record()
+        torch.cuda.synchronize()
+        ams = max_over_ranks(a0.elapsed_time(a1) / args.steps, world)
+        line["adjoint"] = {"ms_per_step": ams, "adjoint_over_forward": ams / ms_max,
+                           "outputs": "dLoss/dJ and dLoss/d(source positions), 2 x [N,3]"}
+        del dJ, dx, g
 
     # the other M2L forms on the same workload (one warm-up and one timed solve each): the plain
     # FP32 FMM (M2L on the CUDA cores) for the split-BF16 ratio, and the cheaper BF16X3 split
