@@ -21,9 +21,8 @@
 //   warps 10-13 drain: every few offsets tcgen05.ld the accumulator and add it to the FP32 local
 //               expansions in global memory (the tensor-core accumulation truncates; long chains
 //               into one TMEM value lose accuracy), then release TMEM for a fresh accumulation
-// Stages hold one 32-wide K chunk of every piece of A and of T_o; four (two pieces) or two (three
-// pieces) stages rotate through mbarriers (full: producers + bulk-copy bytes, empty:
-// tcgen05.commit). Every wait is bounded by
+// Stages hold one K chunk of every piece of A and of T_o; two stages rotate through mbarriers
+// (full: producers + bulk-copy bytes, empty: tcgen05.commit). Every wait is bounded by
 // a 2 s global-timer limit; on expiry the CTA records FMM timeout in the error word and stops.
 #include <cstdlib>
 
@@ -146,13 +145,20 @@ __device__ __forceinline__ void tmemLd16(uint32_t addr, float* v)
 }
 
 
-// Operand layout for NP bf16 pieces per value (2: hi + lo, 3: hi + mid + lo): 32-element K chunks
-// in 64-byte rows (SW64). With two pieces a stage is 55 KB and four stages are in flight; with
-// three pieces a stage is 83 KB and two are.
-template <int NP> struct Layout
+// Operand layout for NP bf16 pieces per value (2: hi + lo, 3: hi + mid + lo). With two pieces a K
+// chunk is 64 elements in 128-byte rows (SW128, 108 KB per stage); with three it is 32 elements in
+// 64-byte rows (SW64, 83 KB per stage); two stages in both. (Four SW64 stages of two pieces were
+// measured slower than two SW128 stages: more barrier round trips per offset.)
+template <int NP> struct Layout;
+template <> struct Layout<2>
 {
-   static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4;
-   static constexpr int NSTAGE = NP == 2 ? 4 : 2;
+   static constexpr int KC = 64, RB = 128, SBO = 1024, SWZ = 2, NSTAGE = 2;
+   __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
+   { return row * 128u + ((((k >> 3) ^ (row & 7u)) & 7u) << 4) + ((k & 7u) << 1); }
+};
+template <> struct Layout<3>
+{
+   static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4, NSTAGE = 2;
    __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
    { return row * 64u + ((((k >> 3) ^ ((row >> 1) & 3u)) & 3u) << 4) + ((k & 7u) << 1); }
 };
