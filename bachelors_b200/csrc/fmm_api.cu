@@ -85,6 +85,7 @@ fmm_status Plan::init(const fmm_config& c)
 
 void Plan::release()
 {
+   dropGraph();
    if(adj)
    {
       adj->release();
@@ -244,6 +245,7 @@ fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const
    if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
    P.n = n;
    P.treeReady = P.upReady = P.downReady = false;
+   P.dropGraph();
    return FMM_OK;
 }
 
@@ -260,6 +262,7 @@ fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_de
    if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
    P.m = m;
    P.treeReady = P.upReady = P.downReady = false;
+   P.dropGraph();
    return FMM_OK;
 }
 
@@ -270,6 +273,7 @@ fmm_status fmm_build_tree(fmm_plan* plan, void* stream)
    if(P.n + P.m == 0) return setError(FMM_E_INVALID, "no sources or targets set");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   P.dropGraph();
    cudaEventRecord(P.ev[0], st);
    FMM_TRY(P.fp64 ? buildTreeT<double>(P, st) : buildTreeT<float>(P, st));
    cudaEventRecord(P.ev[1], st);
@@ -436,6 +440,116 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
       if(dL_dx) FMM_CUDA(cudaMemcpyAsync(dL_dx, dx, es * 3 * P.n, cudaMemcpyDeviceToHost, st));
       FMM_CUDA(cudaStreamSynchronize(st));
    }
+   return FMM_OK;
+}
+
+fmm_status fmm_update_sources(fmm_plan* plan, const void* w, const void* J, int on_device, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!P.treeReady) return setError(FMM_E_INVALID, "fmm_update_sources: the tree is not built");
+   if(P.n > 0 && !w) return setError(FMM_E_INVALID, "fmm_update_sources: null weights");
+   if((J != nullptr) != P.hasJ)
+      return setError(FMM_E_INVALID, "fmm_update_sources: J must be given exactly when the sources were set with J");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   if(P.n)
+   {
+      FMM_CUDA(cudaMemcpyAsync(P.srcW, w, es * P.n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+      if(J)
+         FMM_CUDA(cudaMemcpyAsync(P.srcJ, J, es * 3 * P.n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  st));
+   }
+   FMM_TRY(P.fp64 ? regatherStrengthsT<double>(P, st) : regatherStrengthsT<float>(P, st));
+   if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
+   P.upReady = P.downReady = false;
+   return FMM_OK;
+}
+
+fmm_status fmm_graph_capture(fmm_plan* plan, int want, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   const bool tcMode = !P.fp64 && P.cfg.m2l_mode != FMM_M2L_SIMT;
+   if(!P.treeReady || P.opOrder != P.p || (tcMode && P.opImgOrder < 0))
+      return setError(FMM_E_INVALID, "fmm_graph_capture: run fmm_solve first");
+   if(want < 1 || want > 3) return setError(FMM_E_INVALID, "want must be 1, 2 or 3");
+   DeviceGuard g(P.cfg.device);
+   P.dropGraph();
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_TRY(P.outB.reserve(es * 3 * std::max<int64_t>(P.m, 1)));
+   FMM_TRY(P.outA.reserve(es * 3 * std::max<int64_t>(P.m, 1)));
+   // warm the lazily built state (operator image, buffers) eagerly, then capture on a private stream
+   cudaStream_t user = (cudaStream_t)stream;
+   FMM_CUDA(cudaStreamSynchronize(user));
+   cudaStream_t cs = nullptr;
+   FMM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+   fmm_status s = FMM_OK;
+   cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+   if(e != cudaSuccess) s = setError(FMM_E_CUDA, "fmm_graph_capture: %s", cudaGetErrorString(e));
+   else
+   {
+      P.capturing = true;
+      s = P.fp64 ? upwardT<double>(P, cs) : upwardT<float>(P, cs);
+      if(s == FMM_OK) s = P.fp64 ? downwardT<double>(P, cs) : downwardT<float>(P, cs);
+      if(s == FMM_OK) s = P.fp64 ? evaluateT<double>(P, 1.0, want, cs) : evaluateT<float>(P, 1.0, want, cs);
+      P.capturing = false;
+      cudaGraph_t gr = nullptr;
+      e = cudaStreamEndCapture(cs, &gr);
+      if(s == FMM_OK && e != cudaSuccess) s = setError(FMM_E_CUDA, "fmm_graph_capture: %s", cudaGetErrorString(e));
+      if(s == FMM_OK)
+      {
+         e = cudaGraphInstantiate(&P.graphExec, gr, 0);
+         if(e != cudaSuccess) s = setError(FMM_E_CUDA, "fmm_graph_capture: instantiate: %s", cudaGetErrorString(e));
+         P.graph = gr;
+      }
+      else if(gr)
+         cudaGraphDestroy(gr);
+   }
+   cudaGetLastError();
+   cudaStreamDestroy(cs);
+   if(s != FMM_OK)
+   {
+      P.dropGraph();
+      return s;
+   }
+   P.graphWant = want;
+   return FMM_OK;
+}
+
+fmm_status fmm_graph_launch(fmm_plan* plan, double current, void* out_B, void* out_A, int on_device, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!P.graphExec) return setError(FMM_E_INVALID, "fmm_graph_launch: no captured graph (fmm_graph_capture)");
+   if(((P.graphWant & 1) && !out_B) || ((P.graphWant & 2) && !out_A))
+      return setError(FMM_E_INVALID, "fmm_graph_launch: null output buffer");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   FMM_CUDA(cudaGraphLaunch(P.graphExec, st));
+   const int64_t cnt = 3 * P.m;
+   if(on_device)
+   {
+      if(P.graphWant & 1) FMM_TRY(P.fp64 ? scaleCopyT<double>(P, P.outB.ptr, out_B, cnt, current, st)
+                                         : scaleCopyT<float>(P, P.outB.ptr, out_B, cnt, current, st));
+      if(P.graphWant & 2) FMM_TRY(P.fp64 ? scaleCopyT<double>(P, P.outA.ptr, out_A, cnt, current, st)
+                                         : scaleCopyT<float>(P, P.outA.ptr, out_A, cnt, current, st));
+      return FMM_OK;
+   }
+   // host outputs: scale in place on the device, copy back, and check the error word
+   if(P.graphWant & 1) FMM_TRY(P.fp64 ? scaleCopyT<double>(P, P.outB.ptr, P.outB.ptr, cnt, current, st)
+                                      : scaleCopyT<float>(P, P.outB.ptr, P.outB.ptr, cnt, current, st));
+   if(P.graphWant & 2) FMM_TRY(P.fp64 ? scaleCopyT<double>(P, P.outA.ptr, P.outA.ptr, cnt, current, st)
+                                      : scaleCopyT<float>(P, P.outA.ptr, P.outA.ptr, cnt, current, st));
+   if(P.graphWant & 1) FMM_CUDA(cudaMemcpyAsync(out_B, P.outB.ptr, es * cnt, cudaMemcpyDeviceToHost, st));
+   if(P.graphWant & 2) FMM_CUDA(cudaMemcpyAsync(out_A, P.outA.ptr, es * cnt, cudaMemcpyDeviceToHost, st));
+   int herr = 0;
+   FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+   FMM_CUDA(cudaStreamSynchronize(st));
+   if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "graph solve: a tensor-core pipeline wait timed out");
    return FMM_OK;
 }
 

@@ -137,6 +137,20 @@ struct Plan
    int64_t launches = 0;      // kernels this plan launched (all phases, cumulative)
    bool debugSync = false;    // FMM_DEBUG_SYNC=1: synchronise and check after every launch
 
+   // CUDA graph of upward + downward + evaluation for the current tree (fmm_graph_capture)
+   bool capturing = false;
+   cudaGraph_t graph = nullptr;
+   cudaGraphExec_t graphExec = nullptr;
+   int graphWant = 0;
+   void dropGraph()
+   {
+      if(graphExec) cudaGraphExecDestroy(graphExec);
+      if(graph) cudaGraphDestroy(graph);
+      graphExec = nullptr;
+      graph = nullptr;
+      graphWant = 0;
+   }
+
    // adjoint: a plan on the swapped point sets, and staging for host inputs / outputs
    Plan* adj = nullptr;
    DevBuf adjG, adjOut;
@@ -169,6 +183,8 @@ template <class T> fmm_status directT(Plan& P, double current, int want, cudaStr
 fmm_status buildOperators(Plan& P, cudaStream_t st);
 fmm_status initOffsetTables();
 fmm_status m2lTensorCore(Plan& P, cudaStream_t st);
+template <class T> fmm_status regatherStrengthsT(Plan& P, cudaStream_t st);
+template <class T> fmm_status scaleCopyT(Plan& P, const void* src, void* dst, int64_t count, double scale, cudaStream_t st);
 template <class T> fmm_status adjointT(Plan& P, Plan& A, double current, const void* g, void* dJ, void* dx, cudaStream_t st);
 
 }  // namespace fmm

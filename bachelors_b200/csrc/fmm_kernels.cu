@@ -748,7 +748,7 @@ fmm_status downwardT(Plan& P, cudaStream_t st)
    FMM_CUDA(cudaMemsetAsync(P.local.ptr, 0, sizeof(T) * N * 3 * Lp, st));
    if(sizeof(T) == 4 && P.cfg.m2l_mode != FMM_M2L_SIMT) FMM_TRY(m2lTensorCore(P, st));
    else FMM_TRY(m2lSimt<T>(P, st));
-   if(P.eventsMade) cudaEventRecord(P.ev[3], st);
+   if(P.eventsMade && !P.capturing) cudaEventRecord(P.ev[3], st);
    size_t shm = sizeof(T) * 3 * Lp;
    for(int level = 1; level < P.tree.nLevels; level++)
    {
@@ -816,6 +816,61 @@ fmm_status directFp64Subset(Plan& P, double current, const double* tgtDev, int k
    FMM_CHECK_LAUNCH();
    return FMM_OK;
 }
+
+// New strengths w J for the same source positions, in the tree's sorted order.
+template <class T>
+__global__ void kRegatherStrengths(const T* __restrict__ xyz, const T* __restrict__ w, const T* __restrict__ J,
+                                   const int* __restrict__ order, int64_t n, typename Vec4<T>::type* q)
+{
+   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+   if(i >= n) return;
+   int64_t s = order[i];
+   T jx, jy, jz;
+   if(J) { jx = J[3 * s]; jy = J[3 * s + 1]; jz = J[3 * s + 2]; }
+   else
+   {
+      const T x = xyz[3 * s], y = xyz[3 * s + 1];
+      const T l = sqrt(x * x + y * y);
+      jx = l != T(0) ? -y / l : T(0);
+      jy = l != T(0) ? x / l : T(0);
+      jz = T(0);
+   }
+   const T ww = w[s];
+   q[i] = {ww * jx, ww * jy, ww * jz, T(0)};
+}
+
+template <class T>
+__global__ void kScaleCopy(const T* __restrict__ src, T* __restrict__ dst, int64_t count, T scale)
+{
+   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+   if(i < count) dst[i] = src[i] * scale;
+}
+
+template <class T>
+fmm_status regatherStrengthsT(Plan& P, cudaStream_t st)
+{
+   typedef typename Vec4<T>::type V4;
+   if(P.n == 0) return FMM_OK;
+   kRegatherStrengths<T><<<int((P.n + 255) / 256), 256, 0, st>>>((const T*)P.srcXYZ, (const T*)P.srcW,
+                                                                 (const T*)(P.hasJ ? P.srcJ : nullptr),
+                                                                 (const int*)P.sIdx.ptr, P.n, (V4*)P.sQ.ptr);
+   FMM_TRY(launched(P, "kRegatherStrengths", st));
+   return FMM_OK;
+}
+
+template <class T>
+fmm_status scaleCopyT(Plan& P, const void* src, void* dst, int64_t count, double scale, cudaStream_t st)
+{
+   if(count == 0) return FMM_OK;
+   kScaleCopy<T><<<int((count + 255) / 256), 256, 0, st>>>((const T*)src, (T*)dst, count, T(scale));
+   FMM_TRY(launched(P, "kScaleCopy", st));
+   return FMM_OK;
+}
+
+template fmm_status regatherStrengthsT<float>(Plan&, cudaStream_t);
+template fmm_status regatherStrengthsT<double>(Plan&, cudaStream_t);
+template fmm_status scaleCopyT<float>(Plan&, const void*, void*, int64_t, double, cudaStream_t);
+template fmm_status scaleCopyT<double>(Plan&, const void*, void*, int64_t, double, cudaStream_t);
 
 template fmm_status upwardT<float>(Plan&, cudaStream_t);
 template fmm_status upwardT<double>(Plan&, cudaStream_t);

@@ -506,6 +506,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
                                                  (const uint8_t*)P.opM2Lbf.ptr, (const float*)P.mult.ptr,
                                                  (float*)P.local.ptr, drainEvery, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
+   if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
    int herr = 0;
    FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
    FMM_CUDA(cudaStreamSynchronize(st));

@@ -198,6 +198,27 @@ class Plan:
                                         self._ptr(dx), int(self.device_mode), self._stream()))
         return dJ, dx
 
+    def update_sources(self, w, J=None):
+        """New weights / currents for the same source positions; keeps the tree."""
+        wb = _Buffer(w, self.np_dtype, self.torch_dtype, ())
+        jb = _Buffer(J, self.np_dtype, self.torch_dtype, (3,)) if J is not None else None
+        _lib.check(self.lib.fmm_update_sources(self.handle, ctypes.c_void_p(wb.ptr),
+                                               ctypes.c_void_p(jb.ptr) if jb else None, int(wb.device),
+                                               self._stream()))
+        self._keep += [wb, jb]
+
+    def graph_capture(self, want=1):
+        """Capture P2M .. L2P + near field on the current tree as a CUDA graph."""
+        _lib.check(self.lib.fmm_graph_capture(self.handle, int(want), self._stream()))
+        self.graph_want = int(want)
+
+    def graph_launch(self, current=1.0):
+        B = self._out() if self.graph_want & 1 else None
+        A = self._out() if self.graph_want & 2 else None
+        _lib.check(self.lib.fmm_graph_launch(self.handle, ctypes.c_double(current), self._ptr(B), self._ptr(A),
+                                             int(self.device_mode), self._stream()))
+        return B, A
+
     def direct_fp64(self, targets, current=1.0):
         t = np.ascontiguousarray(np.asarray(targets, dtype=np.float64).reshape(-1, 3))
         out = np.zeros_like(t)

@@ -137,6 +137,18 @@ fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* 
 fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx, int on_device,
                        void* stream);
 
+/* New weights w[n] and currents J[3n] for the same source positions (J must be NULL exactly when
+ * the sources were set without J). Keeps the tree; the next solve or graph launch uses them. */
+fmm_status fmm_update_sources(fmm_plan* plan, const void* w, const void* J, int on_device, void* stream);
+
+/* CUDA graph of one solve on the current tree: P2M, M2M, M2L, L2L and L2P + near field, captured
+ * once (after an fmm_solve, which builds the tree, operators and buffers) and replayed by
+ * fmm_graph_launch, typically after fmm_update_sources. want: 1 = B, 2 = A, 3 = both. The graph is
+ * dropped when sources, targets or the tree change. fmm_graph_launch scales by `current` and writes
+ * out_B / out_A (device or host as on_device says). */
+fmm_status fmm_graph_capture(fmm_plan* plan, int want, void* stream);
+fmm_status fmm_graph_launch(fmm_plan* plan, double current, void* out_B, void* out_A, int on_device, void* stream);
+
 fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats);
 
 /* Operator tables, for verification. kind 0 = M2M (index = child octant 0..7), 1 = L2L
