@@ -1,6 +1,7 @@
 """CUDA-graph replay of a solve on a fixed tree (fmm_graph_capture / fmm_graph_launch) after new
 source strengths (fmm_update_sources): the replay runs the same kernels as an eager solve with the
-new strengths, so the results agree bit for bit."""
+new strengths, so at current 1 the results agree bit for bit. Other currents scale the replayed
+result once more at the end (one extra rounding), so those agree to the last bit or so."""
 import numpy as np
 import pytest
 
@@ -25,16 +26,20 @@ def test_graph_replay_matches_eager_solve(precision, m2l):
     plan.solve(1.0, 3)
     plan.graph_capture(3)
     plan.update_sources(d(w2), d(J2))
-    Bg, Ag = plan.graph_launch(2.5)
+    Bg, Ag = plan.graph_launch(1.0)
     torch.cuda.synchronize()
     eager = Plan(order=10, leaf_capacity=32, precision=precision, m2l=m2l)
     eager.set_sources(d(xyz), d(w2), d(J2))
     eager.set_targets(d(tgt))
-    Be, Ae = eager.solve(2.5, 3)
+    Be, Ae = eager.solve(1.0, 3)
     torch.cuda.synchronize()
     assert torch.equal(Bg, Be) and torch.equal(Ag, Ae)
-    # replays are repeatable
+    # replays are repeatable; the current scales the replayed result (one extra rounding)
     Bg2, _ = plan.graph_launch(2.5)
-    assert torch.equal(Bg2, Bg)
+    Be2, _ = eager.solve(2.5, 1)
+    tol = 1e-6 if precision == "fp32" else 1e-14
+    assert (torch.linalg.norm(Bg2 - Be2) / torch.linalg.norm(Be2)).item() < tol
+    Bg3, _ = plan.graph_launch(2.5)
+    assert torch.equal(Bg3, Bg2)
     plan.close()
     eager.close()
