@@ -20,7 +20,8 @@ EXPORTS = [
     "fmm_default_config", "fmm_plan_create", "fmm_plan_destroy", "fmm_set_sources", "fmm_set_targets",
     "fmm_build_tree", "fmm_upward", "fmm_downward", "fmm_evaluate", "fmm_solve", "fmm_direct",
     "fmm_direct_fp64_subset", "fmm_adjoint", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
-    "fmm_get_stats", "fmm_get_operator", "fmm_direct_B_noalloc", "fmm_add_vectors",
+    "fmm_get_stats", "fmm_get_operator", "fmm_direct_B_noalloc", "fmm_translate_all", "fmm_translate_all_matrix",
+    "fmm_translate_all_matrix_complex", "fmm_add_vectors",
     "fmm_last_error_string", "fmm_version",
 ]
 
@@ -87,6 +88,11 @@ def load():
         "fmm_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(FmmStats)]),
         "fmm_get_operator": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
         "fmm_direct_B_noalloc": (ctypes.c_int, [vp, vp, vp, i64, vp, i64, dbl, vp, vp]),
+        "fmm_translate_all": (ctypes.c_int, [vp, vp, vp, i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
+        "fmm_translate_all_matrix": (ctypes.c_int, [vp, vp, vp, i64, ctypes.c_int, i64, ctypes.c_int, ctypes.c_int,
+                                                    vp]),
+        "fmm_translate_all_matrix_complex": (ctypes.c_int, [vp, vp, vp, i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                            vp]),
         "fmm_add_vectors": (ctypes.c_int, [vp, vp, vp, i64]),
         "fmm_last_error_string": (ctypes.c_char_p, []),
         "fmm_version": (ctypes.c_char_p, []),

@@ -170,6 +170,33 @@ fmm_status fmm_get_operator(fmm_plan* plan, int kind, int index, double* out);
 fmm_status fmm_direct_B_noalloc(const float* xyz, const float* w, const float* J, int64_t n, const float* tgt,
                                 int64_t m, double current, float* out_B, void* stream);
 
+/* The reference's translation seam, kernels::translateAll* (FMM/FMMGPU/translation_algorithms.hpp:13-61),
+ * plan-free, on the current device. Element type: float (precision FMM_FP32) or double (FMM_FP64),
+ * matching the reference's `real`. on_device != 0: every pointer is device memory and the call only
+ * queues work on `stream`; otherwise host memory, staged through stream-ordered allocations, and the
+ * call waits for the result.
+ *
+ * fmm_translate_all <- translateAllCPU / translateAllGPU (translation_algorithms.hpp:13-25): for each
+ * of `count` items, result[i] = M2M of the vector expansion expansions[i] ((order+1)^2 x 3 reals,
+ * Vector3 AoS) by the real regular harmonics harmonics[i] ((order+1)^2 reals), with the reference's
+ * real-form arithmetic (MultipoleTranslator::translateMultipole, multipole_translator.cpp:34-109).
+ * All degrees 0..order are written (the reference's translateAllGPU leaves degree `order` unwritten,
+ * translation_algorithms_gpu.cu:45-48; its translateAllCPU writes it). order <= 32. */
+fmm_status fmm_translate_all(void* result, const void* harmonics, const void* expansions, int64_t count, int order,
+                             int precision, int on_device, void* stream);
+/* <- translateAllCPUMatrixBLAS / translateAllGPUMatrixCuBLAS (translation_algorithms.hpp:41-61): with
+ * L = (order+1)^2, result (count x L) = a (count x L) * b (L x L), row-major, which is the reference's
+ * column-major C = B * A. `batch` products share b: a and result hold `batch` consecutive count x L
+ * blocks (the RealMatrix overload, three components, is batch = 3). batch <= 65535. */
+fmm_status fmm_translate_all_matrix(void* result, const void* a, const void* b, int64_t count, int order,
+                                    int64_t batch, int precision, int on_device, void* stream);
+/* <- translateAllCPUMatrix / translateAllGPUMatrix (translation_algorithms.hpp:27-39): the same product
+ * in complex arithmetic, elements (re, im) pairs (cuComplex / cuDoubleComplex layout). The reference's
+ * GPU version launches a kernel whose body is commented out (kernels.cu:87-121) and returns zeros; this
+ * computes what its CPU twin computes (math::multMatricesAsVectors, math.hpp:84-105). */
+fmm_status fmm_translate_all_matrix_complex(void* result, const void* a, const void* b, int64_t count, int order,
+                                            int precision, int on_device, void* stream);
+
 /* kernels::addVectors (FMMCUDADLL/kernel_callers.hpp:7-9): c = a + b for host arrays of n floats. */
 fmm_status fmm_add_vectors(const float* a, const float* b, float* c, int64_t n);
 

@@ -548,6 +548,81 @@ void orc_m2l(int p, int compat, const double* in, const double* t, double* out)
 void orc_l2l(int p, int compat, const double* in, const double* t, double* out)
 { translate(Op::L2L, p, compat != 0, in, t, out); }
 
+// Batched real-form M2M with caller-supplied translation harmonics, the operation of the
+// reference's kernels::translateAllCPU / translateAllGPU (translation_algorithms_cpu.cpp:9-95,
+// MultipoleTranslator::translateMultipole multipole_translator.cpp:34-109). Per item i:
+// a[i] holds the real regular harmonics of the translation ((p+1)^2), b[i] the vector
+// expansion ((p+1)^2 x 3, AoS) and result[i] the translated expansion. The reference reads a
+// real-form entry (l, m != 0) as the complex number s (h[l,|m|] + i sign(m) h[l,-|m|]) with
+// s = R_SQRT_2 = 0.70710678118 (kernels.cuh:84-112); its m = 0 outputs sum the raw real-form
+// products; its m > 0 outputs add the (l, m) and conjugated (l, -m) complex sums and scale by s.
+// The sign factor is (-1)^((|m - mu| + |mu| - |m|) / 2) (multipole_translator.cpp:143-146).
+void orc_translate_all(int64_t count, int p, const double* a, const double* b, double* result)
+{
+   const int L = nharm(p);
+   const double s = REF_R_SQRT_2;
+   auto factor = [](int m, int mu) { return ((std::abs(m - mu) + std::abs(mu) - std::abs(m)) / 2) % 2 ? -1.0 : 1.0; };
+   auto view = [&](const double* h, int l, int m) -> cplx {
+      if(m == 0) return cplx(h[idx(l, 0)], 0.0);
+      return cplx(h[idx(l, std::abs(m))] * s, h[idx(l, -std::abs(m))] * s * (m > 0 ? 1.0 : -1.0));
+   };
+#pragma omp parallel for schedule(static)
+   for(int64_t it = 0; it < count; it++)
+   {
+      const double* ai = a + it * L;
+      const double* bi = b + it * 3 * L;
+      double* ri = result + it * 3 * L;
+      std::vector<double> bc(L);
+      for(int c = 0; c < 3; c++)
+      {
+         for(int k = 0; k < L; k++) bc[k] = bi[3 * k + c];
+         for(int l = 0; l <= p; l++)
+         {
+            double zero = 0;
+            for(int lam = 0; lam <= l; lam++)
+            {
+               const int dl = l - lam;
+               for(int mu = -std::min(lam, dl); mu <= std::min(lam, dl); mu++)
+                  zero += bc[idx(lam, mu)] * ai[idx(dl, mu)] * factor(0, mu);
+            }
+            ri[3 * idx(l, 0) + c] = zero;
+            for(int m = 1; m <= l; m++)
+            {
+               cplx acc = 0;
+               for(int lam = 0; lam <= l; lam++)
+               {
+                  const int dl = l - lam;
+                  for(int mu = -lam; mu <= lam; mu++)
+                  {
+                     const cplx B = view(bc.data(), lam, mu);
+                     if(std::abs(m - mu) <= dl) acc += B * view(ai, dl, m - mu) * factor(m, mu);
+                     if(std::abs(-m - mu) <= dl) acc += std::conj(B * view(ai, dl, -m - mu)) * factor(-m, mu);
+                  }
+               }
+               ri[3 * idx(l, m) + c] = acc.real() * s;
+               ri[3 * idx(l, -m) + c] = acc.imag() * s;
+            }
+         }
+      }
+   }
+}
+
+// The matrix forms of the same seam (translateAllCPUMatrixBLAS / translateAllGPUMatrixCuBLAS,
+// translation_algorithms_cpu.cpp:114-135, and translateAllCPUMatrix :98-112): with items stored
+// one after another, result (count x L) = a (count x L) * b (L x L), all row-major. The column-major
+// BLAS call C = B * A of the reference is this product read in the transposed layout.
+void orc_translate_all_matrix(int64_t count, int L, const double* a, const double* b, double* result)
+{
+#pragma omp parallel for schedule(static)
+   for(int64_t i = 0; i < count; i++)
+      for(int j = 0; j < L; j++)
+      {
+         double acc = 0;
+         for(int k = 0; k < L; k++) acc += a[i * L + k] * b[int64_t(k) * L + j];
+         result[i * L + j] = acc;
+      }
+}
+
 // A = sum_k coef_k H_k(d) and curl A (analytic), H regular (local) or irregular (multipole).
 void orc_eval_expansion(int p, int regular, int compat, const double* coef, const double* d, double* A, double* curl)
 { evalExpansion(p, regular != 0, coef, d, A, curl, compat != 0); }

@@ -87,6 +87,25 @@ def l2l(p, expansion, t, compat=False):
     return _translate("orc_l2l", p, expansion, t, compat)
 
 
+def translate_all(p, a, b):
+    """Batched real-form M2M with given harmonics: a [count, L], b [count, L, 3] -> [count, L, 3]."""
+    a = _c64(a).reshape(-1, nharm(p))
+    b = _c64(b).reshape(len(a), nharm(p), 3)
+    out = np.zeros_like(b)
+    _load().orc_translate_all(ctypes.c_int64(len(a)), p, _d(a), _d(b), _d(out))
+    return out
+
+
+def translate_all_matrix(a, b):
+    """result [count, L] = a [count, L] @ b [L, L] in FP64 (the matrix forms of the same seam)."""
+    b = _c64(b)
+    L = b.shape[0]
+    a = _c64(a).reshape(-1, L)
+    out = np.zeros_like(a)
+    _load().orc_translate_all_matrix(ctypes.c_int64(len(a)), L, _d(a), _d(b), _d(out))
+    return out
+
+
 def eval_expansion(p, coef, d, regular=True, compat=False):
     A = np.zeros(3)
     curl = np.zeros(3)
@@ -200,6 +219,20 @@ class Reference:
 
     def l2l(self, p, e, t):
         return self._tr("ref_l2l", p, e, t)
+
+    def translate_all(self, p, a, b):
+        a = _c64(a).reshape(-1, nharm(p))
+        b = _c64(b).reshape(len(a), nharm(p), 3)
+        out = np.zeros_like(b)
+        self.lib.ref_translate_all(len(a), p, _d(a), _d(b), _d(out))
+        return out
+
+    def translate_all_matrix(self, p, a, b):
+        L = nharm(p)
+        a = _c64(a).reshape(-1, L)
+        out = np.zeros_like(a)
+        self.lib.ref_translate_all_matrix(len(a), p, _d(a), _d(_c64(b).reshape(L, L)), _d(out))
+        return out
 
     def eval_local(self, p, local, d):
         out = np.zeros(3)

@@ -13,6 +13,7 @@
 //   MultipoleTranslator::translateLocalWithComplex (L2L)                  multipole_translator.cpp:234-249
 //   mult(local, regular) (A from a local expansion)                       calculation_point_octree.cpp:192-212
 //   math::calcBioSavartLaplace (direct sum)                               integration.cpp:101-120
+//   kernels::translateAllCPU, translateAllCPUMatrixBLAS                   translation_algorithms_cpu.cpp:9-135
 //   FastMultipoleSolver full B / A pipeline                               fast_multipole_solver.cpp:12-231
 #include <chrono>
 #include <cstdint>
@@ -25,6 +26,7 @@
 #include "harmonics.hpp"
 #include "integration.hpp"
 #include "multipole_translator.hpp"
+#include "translation_algorithms.hpp"
 
 namespace {
 HarmonicSeries<Vector3> toSeries(int order, const double* in)
@@ -111,6 +113,34 @@ void ref_l2l(int order, const double* in, const double* t, double* out)
    auto res = MultipoleTranslator::translateLocalWithComplex(toSeries(order, in),
                                                             Vector3(real(t[0]), real(t[1]), real(t[2])));
    fromSeries(res, out);
+}
+
+// kernels::translateAllCPU over `count` items: result[i] = M2M of the vector expansion b[i]
+// ((order+1)^2 x 3, AoS) by the real regular harmonics a[i] ((order+1)^2).
+void ref_translate_all(int count, int order, const double* a, const double* b, double* result)
+{
+   const size_t L = size_t(order + 1) * (order + 1);
+   std::vector<real> ar(L * count);
+   std::vector<Vector3> br(L * count), res(L * count);
+   for(size_t i = 0; i < L * count; i++)
+   {
+      ar[i] = real(a[i]);
+      br[i] = Vector3(real(b[3 * i]), real(b[3 * i + 1]), real(b[3 * i + 2]));
+   }
+   kernels::translateAllCPU(res.data(), ar.data(), br.data(), size_t(count), size_t(order));
+   for(size_t i = 0; i < L * count; i++)
+   {
+      result[3 * i] = res[i].x; result[3 * i + 1] = res[i].y; result[3 * i + 2] = res[i].z;
+   }
+}
+
+// kernels::translateAllCPUMatrixBLAS: column-major C (L x count) = B (L x L) * A (L x count).
+void ref_translate_all_matrix(int count, int order, const double* a, const double* b, double* result)
+{
+   const size_t L = size_t(order + 1) * (order + 1);
+   std::vector<real> ar(a, a + L * count), br(b, b + L * L), res(L * count);
+   kernels::translateAllCPUMatrixBLAS(res.data(), ar.data(), br.data(), size_t(count), size_t(order));
+   for(size_t i = 0; i < L * count; i++) result[i] = res[i];
 }
 
 // A(x) = sum_k local_k * R_k(d), d = x - center (no 1/(4 pi) or current factor).

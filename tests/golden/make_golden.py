@@ -4,7 +4,7 @@ Runs the patched reference build (oracle/_ref/libref_fmm_*.so, made by oracle/re
 from the reference sources) on seeded inputs and stores inputs and outputs as .npz. The
 reference is not needed afterwards: the tests read only the .npz files.
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [main] [seam]   (default: all)
 """
 import os
 import sys
@@ -64,5 +64,34 @@ def main():
     print("wrote", os.path.join(HERE, "reference_p4_p10_p16.npz"), len(out), "arrays")
 
 
+def seam():
+    """kernels::translateAllCPU and translateAllCPUMatrixBLAS (translation_algorithms_cpu.cpp:9-135)."""
+    rng = np.random.default_rng(20260002)
+    ref = Reference("f64", 10)
+    out = {}
+    for p in (1, 4, 10, 16):
+        L = (p + 1) ** 2
+        t = rng.normal(size=(4, 3)) * 0.4
+        a = np.stack([ref.regular(p, x) for x in t])
+        b = rng.normal(size=(4, L, 3))
+        out[f"ta_p{p}_a"] = a
+        out[f"ta_p{p}_b"] = b
+        out[f"ta_p{p}_out"] = ref.translate_all(p, a, b)
+        if p > 10:
+            continue
+        A = rng.normal(size=(5, L))
+        Bm = rng.normal(size=(L, L))
+        out[f"tam_p{p}_a"] = A
+        out[f"tam_p{p}_b"] = Bm
+        out[f"tam_p{p}_out"] = ref.translate_all_matrix(p, A, Bm)
+    path = os.path.join(HERE, "reference_seam.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, len(out), "arrays")
+
+
 if __name__ == "__main__":
-    main()
+    what = sys.argv[1:] or ["main", "seam"]
+    if "main" in what:
+        main()
+    if "seam" in what:
+        seam()
