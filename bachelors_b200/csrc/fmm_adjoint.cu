@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(NT) kAdjointEval(Tree t, const RootBox* __rest
          Ds[e] = gradCoeffA(Cs + c * L1, j, lp, mu);
       }
    __syncthreads();
-   const RootBox rb = *rootp;
+   const RootBox rb = rootp[rootOf(t, node)];
    double ctr[3], h;
    {
       const int lev = t.level[node];

@@ -377,6 +377,8 @@ fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* 
 {
    if(!plan || (k > 0 && (!tgt || !out_B))) return setError(FMM_E_INVALID, "null argument");
    Plan& P = plan->P;
+   if(P.batch)
+      return setError(FMM_E_INVALID, "fmm_direct_fp64_subset: explicit targets belong to no coil of a batched plan");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = 0;
    if(!P.treeReady) FMM_TRY(fmm_build_tree(plan, nullptr));
@@ -417,6 +419,11 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
       if(s != FMM_OK) { P.adj->release(); delete P.adj; P.adj = nullptr; return s; }
    }
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   // the coils keep their pairing with the roles swapped
+   P.adj->nCoils = P.nCoils;
+   P.adj->batch = P.batch;
+   P.adj->srcOff = P.tgtOff;
+   P.adj->tgtOff = P.srcOff;
    const void* gDev = dL_dB;
    void* dJ = dL_dJ;
    void* dx = dL_dx;
@@ -440,6 +447,37 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
       if(dL_dx) FMM_CUDA(cudaMemcpyAsync(dL_dx, dx, es * 3 * P.n, cudaMemcpyDeviceToHost, st));
       FMM_CUDA(cudaStreamSynchronize(st));
    }
+   return FMM_OK;
+}
+
+fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* src_offsets, const int64_t* tgt_offsets)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(ncoils == 0)
+   {
+      P.batch = false;
+      P.nCoils = 1;
+   }
+   else
+   {
+      if(ncoils < 0 || ncoils > FMM_MAX_COILS)
+         return setError(FMM_E_INVALID, "fmm_batch_set_coils: %lld coils outside 0..%d", (long long)ncoils, FMM_MAX_COILS);
+      if(!src_offsets || !tgt_offsets) return setError(FMM_E_INVALID, "fmm_batch_set_coils: null offsets");
+      if(src_offsets[0] != 0 || tgt_offsets[0] != 0 || src_offsets[ncoils] != P.n || tgt_offsets[ncoils] != P.m)
+         return setError(FMM_E_INVALID, "fmm_batch_set_coils: offsets must run from 0 to the source (%lld) and "
+                                        "target (%lld) counts; set sources and targets first",
+                         (long long)P.n, (long long)P.m);
+      for(int64_t c = 0; c < ncoils; c++)
+         if(src_offsets[c + 1] < src_offsets[c] || tgt_offsets[c + 1] < tgt_offsets[c])
+            return setError(FMM_E_INVALID, "fmm_batch_set_coils: offsets decrease at coil %lld", (long long)c);
+      P.srcOff.assign(src_offsets, src_offsets + ncoils + 1);
+      P.tgtOff.assign(tgt_offsets, tgt_offsets + ncoils + 1);
+      P.nCoils = int(ncoils);
+      P.batch = true;
+   }
+   P.treeReady = P.upReady = P.downReady = false;
+   P.dropGraph();
    return FMM_OK;
 }
 
@@ -577,6 +615,7 @@ fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats)
    s.v_pairs = P.nV;
    s.n_sources = P.n;
    s.n_targets = P.m;
+   s.coils = P.nCoils;
    *stats = s;
    return FMM_OK;
 }

@@ -23,8 +23,9 @@ __host__ __device__ constexpr int hidx(int l, int m) { return l * l + l + m; }
 __host__ __device__ constexpr int padded(int L) { return (L + 15) & ~15; }
 __host__ __device__ inline int offsetIndex(int ox, int oy, int oz) { return (ox + 3) + 7 * (oy + 3) + 49 * (oz + 3); }
 
-// Device tree, structure of arrays. Nodes are numbered level by level, Morton order within a
-// level; children of a node are contiguous.
+// Device forest, structure of arrays. Level-0 nodes are the roots, one per coil (independent
+// problem); nodes are numbered level by level, by key within a level; children of a node are
+// contiguous. A node's key is (coil << 3 level) | (its Morton path below the root).
 struct Tree
 {
    int64_t nNodes;
@@ -39,6 +40,12 @@ struct Tree
    int* child0;
    int* nchild;
 };
+
+// Root (coil) index of a node.
+__device__ __forceinline__ int rootOf(const Tree& t, int node)
+{
+   return int(t.key[node] >> (3 * t.level[node]));
+}
 
 // ---------------------------------------------------------------------------------------
 // Solid harmonics by Cartesian recurrence (no square roots or divisions by r).

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cuda_runtime.h>
+#include <vector>
 
 #include "../../include/fmmcuda.h"
 #include "fmm_common.cuh"
@@ -104,8 +105,17 @@ struct Plan
    void* srcXYZ = nullptr; void* srcW = nullptr; void* srcJ = nullptr; void* tgtXYZ = nullptr;
    bool hasJ = false;
    int64_t n = 0, m = 0;
+   // independent problems ("coils"): coil c owns sources [srcOff[c], srcOff[c+1]) and targets
+   // [tgtOff[c], tgtOff[c+1]); one coil by default. Each coil is a root of the forest; node keys
+   // carry the coil index above the Morton bits, so keys of different coils never mix.
+   int nCoils = 1;
+   bool batch = false;                   // set by fmm_batch_set_coils
+   std::vector<int> srcOff, tgtOff;      // host copies, nCoils + 1 entries each
+   DevBuf segb;                          // device copies: srcOff then tgtOff
+   int maxLevel = MAXLEVEL;              // deepest level the keys resolve
+   int coilBits = 0;                     // key bits above the Morton bits
    // tree
-   RootBox* root = nullptr;
+   RootBox* root = nullptr;              // [nCoils]
    DevBuf rootb, sKeys, tKeys, sIdx, tIdx, sPos, sQ, tPos, cubTmp, scratch, lvlBounds, lvlCnt, lvlOff;
    DevBuf nodeBufs[12];
    int64_t nodeCap = 0;

@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(CH) kP2M(Tree t, const RootBox* __restrict__ r
    const int LS = L | 1;  // odd row stride: conflict-free column access
    T* R = (T*)smraw;                   // [CH][LS]
    T* Q = R + CH * LS;                 // [CH][3]
-   const RootBox rb = *rootp;
+   const RootBox rb = rootp[rootOf(t, node)];
    double c[3], h;
    nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], c, h);
    const double ih = 1.0 / h;
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
       Cs[e] = gradCoeff(Ls + cp * L, jp, lp, mu) - gradCoeff(Ls + cm * L, jm, lp, mu);
    }
    __syncthreads();
-   const RootBox rb = *rootp;
+   const RootBox rb = rootp[rootOf(t, node)];
    double c[3], h;
    nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], c, h);
    const T ih = T(1.0 / h), ih2 = T(1.0 / (h * h));
@@ -647,19 +647,26 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
 template <class T, class U, int NT>
 __global__ void __launch_bounds__(NT) kDirect(const typename Vec4<T>::type* __restrict__ spos,
                                               const typename Vec4<T>::type* __restrict__ sq, int n,
-                                              const U* __restrict__ tgt, int m, U scaleB, U scaleA, int want,
+                                              const U* __restrict__ tgt, int m, const int* __restrict__ sseg,
+                                              const int* __restrict__ tseg, U scaleB, U scaleA, int want,
                                               U* __restrict__ outB, U* __restrict__ outA)
 {
    __shared__ U Sp[NT][4];
    __shared__ U Sq[NT][3];
-   const int ti = blockIdx.x * NT + threadIdx.x;
-   const bool active = ti < m;
+   // blockIdx.y selects a coil: its targets [tseg[c], tseg[c+1]) see only its sources
+   // [sseg[c], sseg[c+1]); without segments every target sees every source
+   const int c = blockIdx.y;
+   const int tBeg = tseg ? tseg[c] : 0, tEnd = tseg ? tseg[c + 1] : m;
+   const int sBeg = sseg ? sseg[c] : 0, sEnd = sseg ? sseg[c + 1] : n;
+   const int ti = tBeg + blockIdx.x * NT + threadIdx.x;
+   if(tBeg + int(blockIdx.x) * NT >= tEnd) return;
+   const bool active = ti < tEnd;
    U x = 0, y = 0, z = 0;
    if(active) { x = tgt[3 * ti]; y = tgt[3 * ti + 1]; z = tgt[3 * ti + 2]; }
    U B[3] = {0, 0, 0}, A[3] = {0, 0, 0};
-   for(int sb = 0; sb < n; sb += NT)
+   for(int sb = sBeg; sb < sEnd; sb += NT)
    {
-      const int cnt = min(NT, n - sb);
+      const int cnt = min(NT, sEnd - sb);
       __syncthreads();
       if(threadIdx.x < cnt)
       {
@@ -727,8 +734,8 @@ template <class T>
 fmm_status m2lSimt(Plan& P, cudaStream_t st)
 {
    const int64_t N = P.tree.nNodes;
-   int first = 1;
-   int count = int(N - 1);
+   int first = P.tree.levelStart[1];   // roots have no M2L list
+   int count = int(N - first);
    if(count <= 0) return FMM_OK;
    int blocks = (count + M2L_TT - 1) / M2L_TT;
    constexpr int KC = sizeof(T) == 4 ? 32 : 16;
@@ -785,11 +792,14 @@ fmm_status directT(Plan& P, double current, int want, cudaStream_t st)
    typedef typename Vec4<T>::type V4;
    constexpr int NT = 128;
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
-   int blocks = int((P.m + NT - 1) / NT);
+   int maxT = 0;
+   for(int c = 0; c < P.nCoils; c++) maxT = std::max(maxT, P.tgtOff[c + 1] - P.tgtOff[c]);
+   const int blocks = (maxT + NT - 1) / NT;
    if(blocks == 0) return FMM_OK;
-   kDirect<T, T, NT><<<blocks, NT, 0, st>>>((const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, int(P.n),
-                                           (const T*)P.tgtXYZ, int(P.m), scaleB, scaleA, want, (T*)P.outB.ptr,
-                                           (T*)P.outA.ptr);
+   const int* seg = (const int*)P.segb.ptr;   // srcOff then tgtOff, uploaded by the tree build
+   kDirect<T, T, NT><<<dim3(blocks, P.nCoils), NT, 0, st>>>((const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, int(P.n),
+                                                           (const T*)P.tgtXYZ, int(P.m), seg, seg + P.nCoils + 1,
+                                                           scaleB, scaleA, want, (T*)P.outB.ptr, (T*)P.outA.ptr);
    FMM_TRY(launched(P, "kDirect", st));
    FMM_CHECK_LAUNCH();
    return FMM_OK;
@@ -804,13 +814,14 @@ fmm_status directFp64Subset(Plan& P, double current, const double* tgtDev, int k
    if(P.fp64)
    {
       kDirect<double, double, NT><<<blocks, NT, 0, st>>>((const double4*)P.sPos.ptr, (const double4*)P.sQ.ptr,
-                                                         int(P.n), tgtDev, k, scaleB, 0.0, 1, outDev, nullptr);
+                                                         int(P.n), tgtDev, k, nullptr, nullptr, scaleB, 0.0, 1,
+                                                         outDev, nullptr);
       FMM_TRY(launched(P, "kDirect", st));
    }
    else
    {
       kDirect<float, double, NT><<<blocks, NT, 0, st>>>((const float4*)P.sPos.ptr, (const float4*)P.sQ.ptr, int(P.n),
-                                                        tgtDev, k, scaleB, 0.0, 1, outDev, nullptr);
+                                                        tgtDev, k, nullptr, nullptr, scaleB, 0.0, 1, outDev, nullptr);
       FMM_TRY(launched(P, "kDirect", st));
    }
    FMM_CHECK_LAUNCH();

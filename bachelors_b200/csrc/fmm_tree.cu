@@ -4,11 +4,13 @@
 // (FMM/FMMGPU/quadrature_octree.cpp:23-97, calculation_point_octree.cpp:26-97,
 // fast_multipole_solver.cpp:105-184) with one Morton-ordered octree over sources and targets,
 // built level by level on the device:
-//   keys      63-bit Morton codes, 21 bits per axis, x in the lowest bit of each triple
+//   keys      Morton codes, up to 21 bits per axis, x in the lowest bit of each triple, with
+//             the coil index above them when several independent coils share the plan
 //   sort      CUB radix sort of (key, index) for sources and for targets
-//   nodes     a node at level l holds the points whose key prefix matches; it splits when it
-//             holds more than `cap` sources or more than `cap` targets (and l < 21); its
-//             children are the non-empty octants, found by binary search in the sorted keys
+//   nodes     one root per coil (its own bounding cube); a node at level l holds the points
+//             whose key prefix matches; it splits when it holds more than `cap` sources or more
+//             than `capT` targets (and l < the deepest key level); its children are the non-empty
+//             octants, found by binary search in the sorted keys
 //   lists     Col (same-level adjacent), A (coarser adjacent leaves), X (coarser non-adjacent
 //             leaves), V (same-level M2L sources, dense table over the 316 offsets), and for
 //             each target leaf the CSR list of source nodes whose points it sums directly.
@@ -46,17 +48,10 @@ __global__ void kBBox(const T* __restrict__ a, int64_t na, const T* __restrict__
    }
 }
 
-// Root cube around the bounding box: center = (lo + hi) / 2, H = max half extent * (1 + 2^-20) + 1e-300.
-__global__ void kRootFromBBox(const double* partial, int nblocks, RootBox* root)
+// Root cube around a bounding box: center = (lo + hi) / 2, H = max half extent * (1 + 2^-20) + 1e-300;
+// keys resolve 2^maxLevel cells per axis.
+__device__ void setRootBox(const double lo[3], const double hi[3], int maxLevel, RootBox* root)
 {
-   if(threadIdx.x != 0 || blockIdx.x != 0) return;
-   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-   for(int b = 0; b < nblocks; b++)
-      for(int d = 0; d < 3; d++)
-      {
-         lo[d] = fmin(lo[d], partial[6 * b + d]);
-         hi[d] = fmax(hi[d], partial[6 * b + 3 + d]);
-      }
    double H = 0;
    for(int d = 0; d < 3; d++)
    {
@@ -67,16 +62,64 @@ __global__ void kRootFromBBox(const double* partial, int nblocks, RootBox* root)
    H = __dadd_rn(__dmul_rn(H, 1.0 + 9.5367431640625e-07), 1e-300);
    root->H = H;
    for(int d = 0; d < 3; d++) root->lo[d] = root->center[d] - H;
-   root->scale = double(1 << MAXLEVEL) / (2.0 * H);
+   root->scale = double(int64_t(1) << maxLevel) / (2.0 * H);
 }
 
-__global__ void kRootFromConfig(double cx, double cy, double cz, double H, RootBox* root)
+__global__ void kRootFromBBox(const double* partial, int nblocks, int maxLevel, RootBox* root)
+{
+   if(threadIdx.x != 0 || blockIdx.x != 0) return;
+   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+   for(int b = 0; b < nblocks; b++)
+      for(int d = 0; d < 3; d++)
+      {
+         lo[d] = fmin(lo[d], partial[6 * b + d]);
+         hi[d] = fmax(hi[d], partial[6 * b + 3 + d]);
+      }
+   setRootBox(lo, hi, maxLevel, root);
+}
+
+__global__ void kRootFromConfig(double cx, double cy, double cz, double H, int maxLevel, RootBox* root)
 {
    if(threadIdx.x != 0 || blockIdx.x != 0) return;
    root->center[0] = cx; root->center[1] = cy; root->center[2] = cz;
    root->H = H;
    for(int d = 0; d < 3; d++) root->lo[d] = root->center[d] - H;
-   root->scale = double(1 << MAXLEVEL) / (2.0 * H);
+   root->scale = double(int64_t(1) << maxLevel) / (2.0 * H);
+}
+
+// One block per coil: the cube around that coil's sources and targets (an empty coil gets a unit cube).
+template <class T>
+__global__ void kRootsPerCoil(const T* __restrict__ src, const T* __restrict__ tgt, const int* __restrict__ srcOff,
+                              const int* __restrict__ tgtOff, int maxLevel, RootBox* roots)
+{
+   const int c = blockIdx.x;
+   const int64_t sa = srcOff[c], sn = srcOff[c + 1] - sa, ta = tgtOff[c], tn = tgtOff[c + 1] - ta;
+   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+   for(int64_t i = threadIdx.x; i < sn + tn; i += blockDim.x)
+   {
+      const T* p = i < sn ? src + 3 * (sa + i) : tgt + 3 * (ta + i - sn);
+      for(int d = 0; d < 3; d++)
+      {
+         double v = double(p[d]);
+         lo[d] = fmin(lo[d], v);
+         hi[d] = fmax(hi[d], v);
+      }
+   }
+   typedef cub::BlockReduce<double, 256> BR;
+   __shared__ typename BR::TempStorage tmp;
+   __shared__ double blo[3], bhi[3];
+   for(int d = 0; d < 3; d++)
+   {
+      double l = BR(tmp).Reduce(lo[d], cub::Min());
+      __syncthreads();
+      double h = BR(tmp).Reduce(hi[d], cub::Max());
+      __syncthreads();
+      if(threadIdx.x == 0) { blo[d] = l; bhi[d] = h; }
+   }
+   if(threadIdx.x != 0) return;
+   if(sn + tn == 0)
+      for(int d = 0; d < 3; d++) { blo[d] = -1; bhi[d] = 1; }
+   setRootBox(blo, bhi, maxLevel, roots + c);
 }
 
 // ------------------------------------------------------------------------------ Morton keys
@@ -91,23 +134,35 @@ __device__ __forceinline__ uint64_t spread3(uint64_t v)
    return v;
 }
 
-__device__ __forceinline__ int64_t quantize(double x, double lo, double scale)
+__device__ __forceinline__ int64_t quantize(double x, double lo, double scale, int maxLevel)
 {
    double u = floor(__dmul_rn(__dsub_rn(x, lo), scale));
    u = fmax(u, 0.0);
-   u = fmin(u, double((1 << MAXLEVEL) - 1));
+   u = fmin(u, double((int64_t(1) << maxLevel) - 1));
    return int64_t(u);
 }
 
+// Key of point i: its coil (the segment of `off` that holds i) above the Morton code of its
+// cell in that coil's root cube.
 template <class T>
-__global__ void kKeys(const T* __restrict__ xyz, int64_t n, const RootBox* __restrict__ root, uint64_t* keys, int* idx)
+__global__ void kKeys(const T* __restrict__ xyz, int64_t n, const RootBox* __restrict__ roots,
+                      const int* __restrict__ off, int nCoils, int maxLevel, uint64_t* keys, int* idx)
 {
    int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
    if(i >= n) return;
-   int64_t ux = quantize(double(xyz[3 * i]), root->lo[0], root->scale);
-   int64_t uy = quantize(double(xyz[3 * i + 1]), root->lo[1], root->scale);
-   int64_t uz = quantize(double(xyz[3 * i + 2]), root->lo[2], root->scale);
-   keys[i] = spread3(uint64_t(ux)) | (spread3(uint64_t(uy)) << 1) | (spread3(uint64_t(uz)) << 2);
+   int lo = 0, hi = nCoils;  // largest c with off[c] <= i
+   while(hi - lo > 1)
+   {
+      int mid = (lo + hi) >> 1;
+      if(off[mid] <= i) lo = mid;
+      else hi = mid;
+   }
+   const RootBox& rb = roots[lo];
+   int64_t ux = quantize(double(xyz[3 * i]), rb.lo[0], rb.scale, maxLevel);
+   int64_t uy = quantize(double(xyz[3 * i + 1]), rb.lo[1], rb.scale, maxLevel);
+   int64_t uz = quantize(double(xyz[3 * i + 2]), rb.lo[2], rb.scale, maxLevel);
+   keys[i] = (uint64_t(lo) << (3 * maxLevel)) | spread3(uint64_t(ux)) | (spread3(uint64_t(uy)) << 1) |
+             (spread3(uint64_t(uz)) << 2);
    idx[i] = int(i);
 }
 
@@ -146,10 +201,14 @@ __global__ void kGatherTargets(const T* __restrict__ xyz, const int* __restrict_
 }
 
 // ------------------------------------------------------------------------------ nodes
-__global__ void kInitRoot(Tree t, int n, int m)
+// Root c spans its coil's segments of the sorted sources and targets (the sort is by coil first).
+__global__ void kInitRoots(Tree t, int nCoils, const int* __restrict__ srcOff, const int* __restrict__ tgtOff)
 {
-   t.key[0] = 0; t.level[0] = 0; t.ix[0] = t.iy[0] = t.iz[0] = 0;
-   t.s0[0] = 0; t.s1[0] = n; t.t0[0] = 0; t.t1[0] = m; t.parent[0] = -1; t.child0[0] = -1; t.nchild[0] = 0;
+   int c = blockIdx.x * blockDim.x + threadIdx.x;
+   if(c >= nCoils) return;
+   t.key[c] = uint64_t(c); t.level[c] = 0; t.ix[c] = t.iy[c] = t.iz[c] = 0;
+   t.s0[c] = srcOff[c]; t.s1[c] = srcOff[c + 1]; t.t0[c] = tgtOff[c]; t.t1[c] = tgtOff[c + 1];
+   t.parent[c] = -1; t.child0[c] = -1; t.nchild[c] = 0;
 }
 
 __device__ __forceinline__ int lowerBound(const uint64_t* __restrict__ keys, int a, int b, uint64_t v)
@@ -164,8 +223,9 @@ __device__ __forceinline__ int lowerBound(const uint64_t* __restrict__ keys, int
 }
 
 // For nodes [a, b) of `level`: decide the split and find the 8 children's ranges.
-__global__ void kCountChildren(Tree t, int a, int b, int level, int cap, int capT, const uint64_t* __restrict__ skeys,
-                               const uint64_t* __restrict__ tkeys, int* bounds, int* cnt)
+__global__ void kCountChildren(Tree t, int a, int b, int level, int maxLevel, int cap, int capT,
+                               const uint64_t* __restrict__ skeys, const uint64_t* __restrict__ tkeys, int* bounds,
+                               int* cnt)
 {
    int i = a + blockIdx.x * blockDim.x + threadIdx.x;
    if(i >= b) return;
@@ -173,9 +233,9 @@ __global__ void kCountChildren(Tree t, int a, int b, int level, int cap, int cap
    int s0 = t.s0[i], s1 = t.s1[i], t0 = t.t0[i], t1 = t.t1[i];
    t.child0[i] = -1;
    t.nchild[i] = 0;
-   if(!((s1 - s0 > cap || t1 - t0 > capT) && level < MAXLEVEL)) { cnt[j] = 0; return; }
+   if(!((s1 - s0 > cap || t1 - t0 > capT) && level < maxLevel)) { cnt[j] = 0; return; }
    uint64_t key = t.key[i];
-   int shift = 3 * (MAXLEVEL - level - 1);
+   int shift = 3 * (maxLevel - level - 1);
    int sb[9], tb[9];
    for(int c = 0; c < 8; c++)
    {
@@ -240,9 +300,13 @@ __device__ __forceinline__ bool adjacentNodes(const Tree& t, int a, int b)
    return true;
 }
 
-__global__ void kInitRootLists(Lists L)
+// Each root is its own only colleague: nothing links different coils.
+__global__ void kInitRootLists(Lists L, int nCoils)
 {
-   L.col[0] = 0; L.ncol[0] = 1; L.na[0] = 0; L.nx[0] = 0; L.nv[0] = 0;
+   int c = blockIdx.x * blockDim.x + threadIdx.x;
+   if(c >= nCoils) return;
+   L.col[int64_t(c) * COLCAP] = c; L.ncol[c] = 1; L.na[c] = 0; L.nx[c] = 0; L.nv[c] = 0;
+   for(int k = 0; k < 316; k++) L.vtab[int64_t(c) * 316 + k] = -1;
 }
 
 // One thread per node D of a level >= 1; the parent's lists are complete.
@@ -375,11 +439,38 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
 {
    const int64_t n = P.n, m = P.m;
    const int threads = 256;
-   // root cube
-   if(P.cfg.root_half_width > 0)
+   // coils: one by default; the key keeps ceil(log2(coils)) bits above the Morton bits
+   const int K = P.nCoils;
+   if(!P.batch)
+   {
+      P.srcOff.assign({0, int(n)});
+      P.tgtOff.assign({0, int(m)});
+   }
+   if(int(P.srcOff.size()) != K + 1 || int(P.tgtOff.size()) != K + 1 || P.srcOff[K] != n || P.tgtOff[K] != m)
+      return setError(FMM_E_INVALID, "coil offsets do not match the source/target counts (%lld, %lld); "
+                                     "call fmm_batch_set_coils after setting sources and targets",
+                      (long long)n, (long long)m);
+   P.coilBits = 0;
+   while((int64_t(1) << P.coilBits) < K) P.coilBits++;
+   P.maxLevel = std::min(MAXLEVEL, (63 - P.coilBits) / 3);
+   FMM_TRY(P.segb.reserve(sizeof(int) * 2 * (K + 1)));
+   int* dSrcOff = (int*)P.segb.ptr;
+   int* dTgtOff = dSrcOff + K + 1;
+   FMM_CUDA(cudaMemcpyAsync(dSrcOff, P.srcOff.data(), sizeof(int) * (K + 1), cudaMemcpyHostToDevice, st));
+   FMM_CUDA(cudaMemcpyAsync(dTgtOff, P.tgtOff.data(), sizeof(int) * (K + 1), cudaMemcpyHostToDevice, st));
+   // root cubes
+   FMM_TRY(P.rootb.reserve(sizeof(RootBox) * K));
+   P.root = (RootBox*)P.rootb.ptr;
+   if(P.batch)
+   {
+      kRootsPerCoil<T><<<K, 256, 0, st>>>((const T*)P.srcXYZ, (const T*)P.tgtXYZ, dSrcOff, dTgtOff, P.maxLevel,
+                                          P.root);
+      FMM_TRY(launched(P, "kRootsPerCoil", st));
+   }
+   else if(P.cfg.root_half_width > 0)
    {
       kRootFromConfig<<<1, 1, 0, st>>>(P.cfg.root_center[0], P.cfg.root_center[1], P.cfg.root_center[2],
-                                       P.cfg.root_half_width, P.root);
+                                       P.cfg.root_half_width, P.maxLevel, P.root);
       FMM_TRY(launched(P, "kRootFromConfig", st));
    }
    else
@@ -389,7 +480,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       FMM_TRY(P.scratch.reserve(sizeof(double) * 6 * nb));
       kBBox<T><<<nb, threads, 0, st>>>((const T*)P.srcXYZ, n, (const T*)P.tgtXYZ, m, (double*)P.scratch.ptr);
       FMM_TRY(launched(P, "kBBox", st));
-      kRootFromBBox<<<1, 1, 0, st>>>((const double*)P.scratch.ptr, nb, P.root);
+      kRootFromBBox<<<1, 1, 0, st>>>((const double*)P.scratch.ptr, nb, P.maxLevel, P.root);
       FMM_TRY(launched(P, "kRootFromBBox", st));
    }
    FMM_CHECK_LAUNCH();
@@ -403,24 +494,27 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    int* si = (int*)P.sIdx.ptr;
    int* ti = (int*)P.tIdx.ptr;
    if(n) {
-      kKeys<T><<<(n + threads - 1) / threads, threads, 0, st>>>((const T*)P.srcXYZ, n, P.root, sk + n, si + n);
+      kKeys<T><<<(n + threads - 1) / threads, threads, 0, st>>>((const T*)P.srcXYZ, n, P.root, dSrcOff, K,
+                                                                P.maxLevel, sk + n, si + n);
       FMM_TRY(launched(P, "kKeys", st));
    }
    if(m) {
-      kKeys<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, m, P.root, tk + m, ti + m);
+      kKeys<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, m, P.root, dTgtOff, K,
+                                                                P.maxLevel, tk + m, ti + m);
       FMM_TRY(launched(P, "kKeys", st));
    }
    FMM_CHECK_LAUNCH();
+   const int keyBits = 3 * P.maxLevel + P.coilBits;
    size_t need = 0, tmp = 0;
-   cub::DeviceRadixSort::SortPairs(nullptr, tmp, sk + n, sk, si + n, si, int(n), 0, 63, st);
+   cub::DeviceRadixSort::SortPairs(nullptr, tmp, sk + n, sk, si + n, si, int(n), 0, keyBits, st);
    need = std::max(need, tmp);
-   cub::DeviceRadixSort::SortPairs(nullptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, 63, st);
+   cub::DeviceRadixSort::SortPairs(nullptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, keyBits, st);
    need = std::max(need, tmp);
    FMM_TRY(P.cubTmp.reserve(need));
    tmp = P.cubTmp.bytes;
-   if(n) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, sk + n, sk, si + n, si, int(n), 0, 63, st));
+   if(n) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, sk + n, sk, si + n, si, int(n), 0, keyBits, st));
    tmp = P.cubTmp.bytes;
-   if(m) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, 63, st));
+   if(m) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, keyBits, st));
    if(P.debugSync) FMM_CUDA(cudaStreamSynchronize(st));
    // sorted point data
    typedef typename Vec4<T>::type V4;
@@ -441,16 +535,16 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    FMM_CHECK_LAUNCH();
 
    // nodes, level by level
-   int64_t capNodes = std::max<int64_t>(1024, 2 * (n + m) / std::max(1, P.cfg.leaf_capacity) + 64);
+   int64_t capNodes = std::max<int64_t>(1024, 2 * (n + m) / std::max(1, P.cfg.leaf_capacity) + 64 + 2 * K);
    FMM_TRY(P.ensureNodes(capNodes));
    Tree& t = P.tree;
-   kInitRoot<<<1, 1, 0, st>>>(t, int(n), int(m));
-   FMM_TRY(launched(P, "kInitRoot", st));
+   kInitRoots<<<(K + 255) / 256, 256, 0, st>>>(t, K, dSrcOff, dTgtOff);
+   FMM_TRY(launched(P, "kInitRoots", st));
    t.levelStart[0] = 0;
-   t.levelStart[1] = 1;
+   t.levelStart[1] = K;
    int nLevels = 1;
-   int64_t total = 1;
-   for(int level = 0; level < MAXLEVEL; level++)
+   int64_t total = K;
+   for(int level = 0; level < P.maxLevel; level++)
    {
       int a = t.levelStart[level], b = t.levelStart[level + 1];
       int cnt = b - a;
@@ -462,7 +556,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       int* cc = (int*)P.lvlCnt.ptr;
       int* off = (int*)P.lvlOff.ptr;
       kCountChildren<<<(cnt + threads - 1) / threads, threads, 0, st>>>(
-         t, a, b, level, P.cfg.leaf_capacity,
+         t, a, b, level, P.maxLevel, P.cfg.leaf_capacity,
          P.cfg.target_leaf_capacity > 0 ? P.cfg.target_leaf_capacity : P.cfg.leaf_capacity, sk, tk, bounds, cc);
       FMM_TRY(launched(P, "kCountChildren", st));
       FMM_CHECK_LAUNCH();
@@ -497,7 +591,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    FMM_TRY(P.ensureLists(total));
    Lists& Ls = P.lists;
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
-   kInitRootLists<<<1, 1, 0, st>>>(Ls);
+   kInitRootLists<<<(K + 255) / 256, 256, 0, st>>>(Ls, K);
    FMM_TRY(launched(P, "kInitRootLists", st));
    for(int level = 1; level < nLevels; level++)
    {

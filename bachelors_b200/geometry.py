@@ -84,3 +84,40 @@ def root_cube(*point_sets):
     H = 0.5 * float(np.max(hi - lo))
     H = H * (1.0 + 2.0 ** -20) + 1e-300
     return center, H
+
+
+def random_axis(rng):
+    """A direction uniform on the unit sphere."""
+    v = rng.normal(size=3)
+    return v / np.linalg.norm(v)
+
+
+def torus_batch(n_coils=256, seed=20260004, count_range=(2 ** 12, 2 ** 18), targets_per_coil=2 ** 14,
+                major_range=(1.0, 3.0), minor_range=(0.2, 0.6), center_range=(-10.0, 10.0),
+                magnitude_range=(0.5, 2.0), n_theta=16, n_rho=4):
+    """Many independent coils for the batched solver: coil i is a torus with major radius
+    R ~ U(major_range), minor radius a ~ U(minor_range), an axis uniform on the sphere, a centre
+    uniform in center_range^3, a point count log-uniform in count_range (n_phi x n_theta x n_rho
+    with n_phi chosen to come closest), a poloidal current of magnitude ~ U(magnitude_range), and
+    `targets_per_coil` targets uniform in the cube of side 3R around its centre.
+
+    Returns (xyz[N,3], w[N], J[N,3], tgt[M,3], src_offsets[K+1], tgt_offsets[K+1]) with each coil's
+    points contiguous."""
+    rng = np.random.default_rng(seed)
+    xs, ws, Js, ts = [], [], [], []
+    so, to = [0], [0]
+    lo, hi = np.log(count_range[0]), np.log(count_range[1])
+    for _ in range(n_coils):
+        R = rng.uniform(*major_range)
+        a = rng.uniform(*minor_range)
+        axis = random_axis(rng)
+        c = rng.uniform(*center_range, size=3)
+        count = float(np.exp(rng.uniform(lo, hi)))
+        mag = rng.uniform(*magnitude_range)
+        n_phi = max(4, int(round(count / (n_theta * n_rho))))
+        x, w, J = torus(n_phi, n_theta, n_rho, R, a, c, axis, "poloidal", mag)
+        t = c + rng.uniform(-1.5 * R, 1.5 * R, size=(targets_per_coil, 3))
+        xs.append(x); ws.append(w); Js.append(J); ts.append(t)
+        so.append(so[-1] + len(w)); to.append(to[-1] + len(t))
+    return (np.concatenate(xs), np.concatenate(ws), np.concatenate(Js), np.concatenate(ts),
+            np.array(so, dtype=np.int64), np.array(to, dtype=np.int64))

@@ -161,6 +161,20 @@ class Plan:
             return None
         return ctypes.c_void_p(a.data_ptr() if _is_cuda_tensor(a) else a.ctypes.data)
 
+    def set_coils(self, src_offsets, tgt_offsets):
+        """Independent problems in one plan (fmm_batch_set_coils): coil c owns sources
+        src_offsets[c]:src_offsets[c+1] and targets tgt_offsets[c]:tgt_offsets[c+1]. Call after
+        set_sources / set_targets; set_coils(None, None) returns to a single problem."""
+        if src_offsets is None:
+            _lib.check(self.lib.fmm_batch_set_coils(self.handle, 0, None, None))
+            return
+        so = np.ascontiguousarray(np.asarray(src_offsets, dtype=np.int64))
+        to = np.ascontiguousarray(np.asarray(tgt_offsets, dtype=np.int64))
+        if so.shape != to.shape or so.ndim != 1 or len(so) < 2:
+            raise ValueError("src_offsets and tgt_offsets must be 1-D with ncoils + 1 entries")
+        _lib.check(self.lib.fmm_batch_set_coils(self.handle, len(so) - 1, ctypes.c_void_p(so.ctypes.data),
+                                                ctypes.c_void_p(to.ctypes.data)))
+
     def build_tree(self):
         _lib.check(self.lib.fmm_build_tree(self.handle, self._stream()))
 

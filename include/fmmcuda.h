@@ -79,6 +79,7 @@ typedef struct fmm_stats {
    int64_t nodes, leaves, levels, v_pairs, p2p_pairs, p2p_interactions;
    int64_t n_sources, n_targets;
    double ms_adjoint; /* the last fmm_adjoint call */
+   int64_t coils;     /* independent problems in the plan (1 unless batched) */
 } fmm_stats;
 
 void fmm_default_config(fmm_config* cfg);
@@ -136,6 +137,18 @@ fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* 
  * local expansions. Weights are constants. Element type and on_device as in fmm_evaluate. */
 fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx, int on_device,
                        void* stream);
+
+/* Batching (no counterpart in the reference, which solves one coil per solver object): many
+ * independent problems ("coils") in one plan. Coil c owns the sources [src_offsets[c], src_offsets[c+1])
+ * and the targets [tgt_offsets[c], tgt_offsets[c+1]) of the arrays given to fmm_set_sources /
+ * fmm_set_targets (so each coil's points are contiguous there); its sources act only on its targets.
+ * Each coil gets its own root cube (around its own points; root_center / root_half_width are
+ * ignored) and every phase processes all coils in the same launches, level by level. Offsets are
+ * host arrays of ncoils + 1 entries from 0 to n (resp. m); call after fmm_set_sources and
+ * fmm_set_targets. ncoils = 0 returns the plan to a single problem. fmm_direct, fmm_adjoint and the
+ * graph calls respect the coils; fmm_direct_fp64_subset is not available on a batched plan. */
+#define FMM_MAX_COILS 65536
+fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* src_offsets, const int64_t* tgt_offsets);
 
 /* New weights w[n] and currents J[3n] for the same source positions (J must be NULL exactly when
  * the sources were set without J). Keeps the tree; the next solve or graph launch uses them. */
