@@ -213,6 +213,114 @@ __global__ void __launch_bounds__(NT) kAdjointEval(Tree t, const RootBox* __rest
    }
 }
 
+// Direct-sum adjoint, one thread per source (input order); the targets and their g stream through
+// shared memory in tiles; C and grad(J . C) accumulate in FP64. blockIdx.y selects a coil: its
+// sources [srcOff[c], srcOff[c+1]) see only its targets [tgtOff[c], tgtOff[c+1]).
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) kAdjointDirect(const T* __restrict__ sxyz, const T* __restrict__ sw,
+                                                     const T* __restrict__ sJ, const T* __restrict__ txyz,
+                                                     const T* __restrict__ g, const int* __restrict__ srcOff,
+                                                     const int* __restrict__ tgtOff, double scale, T* __restrict__ dJ,
+                                                     T* __restrict__ dx)
+{
+   __shared__ double Tx[NT][3], Tg[NT][3];
+   const int c = blockIdx.y;
+   const int sBeg = srcOff[c], sEnd = srcOff[c + 1], tBeg = tgtOff[c], tEnd = tgtOff[c + 1];
+   if(sBeg + int(blockIdx.x) * NT >= sEnd) return;
+   const int q = sBeg + blockIdx.x * NT + threadIdx.x;
+   const bool active = q < sEnd;
+   double X = 0, Y = 0, Z = 0, j[3] = {0, 0, 0};
+   if(active)
+   {
+      X = double(sxyz[3 * q]); Y = double(sxyz[3 * q + 1]); Z = double(sxyz[3 * q + 2]);
+      if(sJ) { j[0] = double(sJ[3 * q]); j[1] = double(sJ[3 * q + 1]); j[2] = double(sJ[3 * q + 2]); }
+      else
+      {
+         const double rho = sqrt(X * X + Y * Y);
+         if(rho > 0) { j[0] = -Y / rho; j[1] = X / rho; }
+      }
+   }
+   double C[3] = {0, 0, 0}, G[3] = {0, 0, 0};
+   for(int tb = tBeg; tb < tEnd; tb += NT)
+   {
+      const int cnt = min(NT, tEnd - tb);
+      __syncthreads();
+      if(threadIdx.x < cnt)
+         for(int d = 0; d < 3; d++)
+         {
+            Tx[threadIdx.x][d] = double(txyz[3 * (tb + threadIdx.x) + d]);
+            Tg[threadIdx.x][d] = double(g[3 * (tb + threadIdx.x) + d]);
+         }
+      __syncthreads();
+      if(!active) continue;
+      for(int i = 0; i < cnt; i++)
+      {
+         const double ex = X - Tx[i][0], ey = Y - Tx[i][1], ez = Z - Tx[i][2];
+         const double r2 = ex * ex + ey * ey + ez * ez;
+         if(r2 == 0) continue;
+         const double ri = 1.0 / sqrt(r2), ri3 = ri * ri * ri, ri5 = ri3 * ri * ri;
+         const double gx = Tg[i][0], gy = Tg[i][1], gz = Tg[i][2];
+         C[0] += (gy * ez - gz * ey) * ri3;
+         C[1] += (gz * ex - gx * ez) * ri3;
+         C[2] += (gx * ey - gy * ex) * ri3;
+         const double ax = j[1] * gz - j[2] * gy, ay = j[2] * gx - j[0] * gz, az = j[0] * gy - j[1] * gx;
+         const double ea3 = 3.0 * (ex * ax + ey * ay + ez * az) * ri5;
+         G[0] += ax * ri3 - ea3 * ex;
+         G[1] += ay * ri3 - ea3 * ey;
+         G[2] += az * ri3 - ea3 * ez;
+      }
+   }
+   if(!active) return;
+   if(!sJ)
+   {
+      // derivative of the azimuthal direction (-y, x, 0) / rho
+      const double rho2 = X * X + Y * Y;
+      if(rho2 > 0)
+      {
+         const double ir = 1.0 / (rho2 * sqrt(rho2));
+         G[0] += (X * Y * C[0] + Y * Y * C[1]) * ir;
+         G[1] += (-X * X * C[0] - X * Y * C[1]) * ir;
+      }
+   }
+   const double s = scale * double(sw[q]);
+   for(int d = 0; d < 3; d++)
+   {
+      if(dJ) dJ[3 * int64_t(q) + d] = T(s * C[d]);
+      if(dx) dx[3 * int64_t(q) + d] = T(s * G[d]);
+   }
+}
+
+template <class T>
+fmm_status adjointDirectT(Plan& P, double current, const void* g, void* dJ, void* dx, cudaStream_t st)
+{
+   constexpr int NT = 128;
+   const int K = P.nCoils;
+   if(!P.batch)
+   {
+      P.srcOff.assign({0, int(P.n)});
+      P.tgtOff.assign({0, int(P.m)});
+   }
+   if(int(P.srcOff.size()) != K + 1 || P.srcOff[K] != P.n || P.tgtOff[K] != P.m)
+      return setError(FMM_E_INVALID, "coil offsets do not match the source/target counts");
+   FMM_TRY(P.segb.reserve(sizeof(int) * 2 * (K + 1)));
+   int* so = (int*)P.segb.ptr;
+   int* to = so + K + 1;
+   FMM_CUDA(cudaMemcpyAsync(so, P.srcOff.data(), sizeof(int) * (K + 1), cudaMemcpyHostToDevice, st));
+   FMM_CUDA(cudaMemcpyAsync(to, P.tgtOff.data(), sizeof(int) * (K + 1), cudaMemcpyHostToDevice, st));
+   int maxS = 0;
+   for(int c = 0; c < K; c++) maxS = std::max(maxS, P.srcOff[c + 1] - P.srcOff[c]);
+   if(maxS == 0) return FMM_OK;
+   const double scale = REF_MU0 / (4 * REF_PI) * current;
+   kAdjointDirect<T, NT><<<dim3((maxS + NT - 1) / NT, K), NT, 0, st>>>(
+      (const T*)P.srcXYZ, (const T*)P.srcW, P.hasJ ? (const T*)P.srcJ : nullptr, (const T*)P.tgtXYZ, (const T*)g, so,
+      to, scale, (T*)dJ, (T*)dx);
+   FMM_TRY(launched(P, "kAdjointDirect", st));
+   return FMM_OK;
+}
+
+template fmm_status adjointDirectT<float>(Plan&, double, const void*, void*, void*, cudaStream_t);
+template fmm_status adjointDirectT<double>(Plan&, double, const void*, void*, void*, cudaStream_t);
+
 template <class T>
 __global__ void kFill(T* a, int64_t n, T v)
 {

@@ -450,6 +450,43 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
    return FMM_OK;
 }
 
+fmm_status fmm_adjoint_direct(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx,
+                              int on_device, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!dL_dB || (!dL_dJ && !dL_dx)) return setError(FMM_E_INVALID, "fmm_adjoint_direct: null argument");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   const void* gDev = dL_dB;
+   void* dJ = dL_dJ;
+   void* dx = dL_dx;
+   if(!on_device)
+   {
+      FMM_TRY(P.adjG.reserve(es * 3 * std::max<int64_t>(P.m, 1)));
+      if(P.m) FMM_CUDA(cudaMemcpyAsync(P.adjG.ptr, dL_dB, es * 3 * P.m, cudaMemcpyHostToDevice, st));
+      gDev = P.adjG.ptr;
+      FMM_TRY(P.adjOut.reserve(2 * es * 3 * std::max<int64_t>(P.n, 1)));
+      dJ = dL_dJ ? P.adjOut.ptr : nullptr;
+      dx = dL_dx ? (char*)P.adjOut.ptr + es * 3 * P.n : nullptr;
+   }
+   if(P.n)
+   {
+      if(dJ) FMM_CUDA(cudaMemsetAsync(dJ, 0, es * 3 * P.n, st));
+      if(dx) FMM_CUDA(cudaMemsetAsync(dx, 0, es * 3 * P.n, st));
+   }
+   FMM_TRY(P.fp64 ? adjointDirectT<double>(P, current, gDev, dJ, dx, st)
+                  : adjointDirectT<float>(P, current, gDev, dJ, dx, st));
+   if(!on_device)
+   {
+      if(dL_dJ && P.n) FMM_CUDA(cudaMemcpyAsync(dL_dJ, dJ, es * 3 * P.n, cudaMemcpyDeviceToHost, st));
+      if(dL_dx && P.n) FMM_CUDA(cudaMemcpyAsync(dL_dx, dx, es * 3 * P.n, cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+   }
+   return FMM_OK;
+}
+
 fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* src_offsets, const int64_t* tgt_offsets)
 {
    if(!plan) return setError(FMM_E_INVALID, "null plan");

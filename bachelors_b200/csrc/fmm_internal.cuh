@@ -196,5 +196,6 @@ fmm_status m2lTensorCore(Plan& P, cudaStream_t st);
 template <class T> fmm_status regatherStrengthsT(Plan& P, cudaStream_t st);
 template <class T> fmm_status scaleCopyT(Plan& P, const void* src, void* dst, int64_t count, double scale, cudaStream_t st);
 template <class T> fmm_status adjointT(Plan& P, Plan& A, double current, const void* g, void* dJ, void* dx, cudaStream_t st);
+template <class T> fmm_status adjointDirectT(Plan& P, double current, const void* g, void* dJ, void* dx, cudaStream_t st);
 
 }  // namespace fmm

@@ -212,6 +212,17 @@ class Plan:
                                         self._ptr(dx), int(self.device_mode), self._stream()))
         return dJ, dx
 
+    def adjoint_direct(self, g, current=1.0, want_dJ=True, want_dx=True):
+        """The same gradients as adjoint() by direct summation (FP64 accumulation); no tree needed."""
+        gb = _Buffer(g, self.np_dtype, self.torch_dtype, (3,))
+        if gb.device != self.device_mode:
+            raise ValueError("g must live where the plan's inputs live (host numpy or CUDA tensor)")
+        dJ = self._out(self.n) if want_dJ else None
+        dx = self._out(self.n) if want_dx else None
+        _lib.check(self.lib.fmm_adjoint_direct(self.handle, ctypes.c_double(current), ctypes.c_void_p(gb.ptr),
+                                               self._ptr(dJ), self._ptr(dx), int(self.device_mode), self._stream()))
+        return dJ, dx
+
     def update_sources(self, w, J=None):
         """New weights / currents for the same source positions; keeps the tree."""
         wb = _Buffer(w, self.np_dtype, self.torch_dtype, ())

@@ -12,6 +12,15 @@ aggregate is the units all ranks processed divided by the slowest rank's time.
 
 `--impl reference` times the reference's own CPU FMM (FastMultipoleSolver, FP32, p = 16,
 built from the reference sources into oracle/_ref/) on a bounded sample of the workload.
+
+`--extra` adds the other workload families to the same JSON line under "workloads" (each with
+its own timing, accuracy against the FP64 direct sum and tree statistics):
+  c1     FP64, torus 128x32x16 = 65,536 sources (azimuthal J), 32^3 grid on [-3,3]^3, p = 10, leaf 32
+  c2     FP32, torus 256x64x64 = 2^20 sources, 2^20 seeded targets in [-3,3]^3, p = 12, leaf 64
+  batch  FP32 + split-BF16 M2L, 256 independent tori (log-uniform 2^12..2^18 points, random pose,
+         2^14 targets each), p = 8, leaf 32: eager solve and CUDA-graph replay on the fixed forest
+  c5     FP32 differentiation: loss = 1/2 sum |B - B*|^2 on 2^18 targets, N = 2^20, p = 12; forward
+         + adjoint (dLoss/dJ, dLoss/dx) against the FP64 direct-sum adjoint on 64 seeded sources
 """
 from __future__ import annotations
 
@@ -177,6 +186,181 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _timed(fn, steps, world):
+    """Device time per call of fn() (CUDA events, max over ranks)."""
+    import torch
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return max_over_ranks(e0.elapsed_time(e1) / steps, world), out
+
+
+def _tree_stats(plan):
+    st = plan.stats()
+    return {k: st[k] for k in ("nodes", "levels", "v_pairs", "p2p_pairs", "coils")}
+
+
+def extra_c1(local, world, steps):
+    """FP64 plain FMM: torus 128x32x16 (azimuthal current, the reference's direction), 32^3 grid."""
+    import torch
+    from bachelors_b200 import Plan, geometry as G
+    xyz, w, _ = G.torus(128, 32, 16, 2.0, 0.5, current="azimuthal")
+    tgt = G.cube_grid(32, -3.0, 3.0)
+    dev = f"cuda:{local}"
+    plan = Plan(order=10, leaf_capacity=32, precision="fp64", device=local)
+    plan.set_sources(torch.from_numpy(xyz).to(dev), torch.from_numpy(w).to(dev), None)
+    plan.set_targets(torch.from_numpy(tgt).to(dev))
+    for _ in range(3):
+        B, _ = plan.solve(1.0, 1)
+    ms, (B, _) = _timed(lambda: plan.solve(1.0, 1), steps, world)
+    D, _ = plan.direct(1.0, 1)
+    err = float(torch.linalg.norm(B - D) / torch.linalg.norm(D))
+    res = {"workload": "FP64 torus 128x32x16 = 65536 sources (azimuthal J), 32^3 grid on [-3,3]^3, p=10, leaf 32",
+           "value": world * len(tgt) / (ms / 1000), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+           "rel_l2_vs_fp64_direct": err, "error_samples": "all 32768 targets", "tree": _tree_stats(plan)}
+    plan.close()
+    return res
+
+
+def extra_c2(local, world, steps):
+    """FP32 plain FMM at 2^20 sources and 2^20 seeded targets, p = 12, leaf 64 (CUDA-core and split-BF16 M2L)."""
+    import torch
+    from bachelors_b200 import Plan, geometry as G
+    xyz, w, J = make_workload(256, 64, 64)
+    tgt = G.uniform_points(1 << 20, -3.0, 3.0, 20260002).astype(np.float32)
+    dev = f"cuda:{local}"
+    dx, dw, dJ, dt = (torch.from_numpy(a).to(dev) for a in (xyz, w, J, tgt))
+    rng = np.random.default_rng(20260002)
+    idx = rng.choice(len(tgt), size=4096, replace=False)
+    out = {"workload": "FP32 torus 256x64x64 = 2^20 sources, 2^20 targets U[-3,3]^3 (seed 20260002), p=12, leaf 64",
+           "unit": UNIT, "error_samples": "4096 seeded targets vs FP64 direct"}
+    Bd = None
+    for mode in ("simt", "bf16x3"):
+        plan = Plan(order=12, leaf_capacity=64, precision="fp32", m2l=mode, device=local)
+        plan.set_sources(dx, dw, dJ)
+        plan.set_targets(dt)
+        for _ in range(3):
+            plan.solve(1.0, 1)
+        ms, (B, _) = _timed(lambda: plan.solve(1.0, 1), steps, world)
+        if Bd is None:
+            Bd = plan.direct_fp64(tgt[idx].astype(np.float64), current=1.0)
+        Bh = B.cpu().numpy().astype(np.float64)[idx]
+        out[f"m2l_{mode}"] = {"value": world * len(tgt) / (ms / 1000), "ms_per_step": ms, "steps": steps,
+                              "rel_l2_vs_fp64_direct": float(np.linalg.norm(Bh - Bd) / np.linalg.norm(Bd)),
+                              "phases_ms": {k: plan.stats()[k] for k in ("ms_tree", "ms_upward", "ms_m2l",
+                                                                         "ms_downward", "ms_near")}}
+        out["tree"] = _tree_stats(plan)
+        plan.close()
+    out["value"] = out["m2l_simt"]["value"]
+    return out
+
+
+def extra_batch(local, world, steps):
+    """256 independent tori in one plan: eager full solves and CUDA-graph replays on the fixed forest."""
+    import torch
+    from bachelors_b200 import Plan, geometry as G
+    xyz, w, J, tgt, so, to = G.torus_batch(256, seed=20260004)
+    dev = f"cuda:{local}"
+    dx, dw, dJ, dt = (torch.from_numpy(a.astype(np.float32)).to(dev) for a in (xyz, w, J, tgt))
+    plan = Plan(order=8, leaf_capacity=32, precision="fp32", m2l="bf16x3", device=local)
+    plan.set_sources(dx, dw, dJ)
+    plan.set_targets(dt)
+    plan.set_coils(so, to)
+    for _ in range(3):
+        plan.solve(1.0, 1)
+    ms, (B, _) = _timed(lambda: plan.solve(1.0, 1), steps, world)
+    phases = {k: plan.stats()[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_near", "ms_total")}
+    plan.graph_capture(1)
+    for _ in range(3):
+        plan.graph_launch(1.0)
+    gms, (Bg, _) = _timed(lambda: plan.graph_launch(1.0), steps, world)
+    # accuracy: 16 seeded targets per coil against the FP64 direct sum over that coil's sources
+    rng = np.random.default_rng(20260004)
+    pick = np.concatenate([rng.choice(np.arange(to[c], to[c + 1]), size=16, replace=False) for c in range(256)])
+    ref = Plan(order=1, leaf_capacity=1 << 30, precision="fp64", device=local)
+    ref.set_sources(xyz, w, J)
+    ref.set_targets(tgt[pick])
+    ref.set_coils(so, np.arange(0, 16 * 257, 16))
+    Bd, _ = ref.direct(1.0, 1)
+    ref.close()
+    Bh = B.cpu().numpy().astype(np.float64)[pick]
+    err = float(np.linalg.norm(Bh - Bd) / np.linalg.norm(Bd))
+    per_coil = [float(np.linalg.norm(Bh[16 * c:16 * c + 16] - Bd[16 * c:16 * c + 16]) /
+                      max(np.linalg.norm(Bd[16 * c:16 * c + 16]), 1e-300)) for c in range(256)]
+    res = {"workload": f"256 tori (R~U(1,3), a~U(0.2,0.6), random axis, centre U[-10,10]^3, log-uniform "
+                       f"2^12..2^18 points, J poloidal |J|~U(0.5,2)), {len(w)} sources, 2^14 targets each = "
+                       f"{len(tgt)} targets; p=8, leaf 32, FP32 + BF16X3 M2L; seed 20260004",
+           "value": world * len(tgt) / (ms / 1000), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+           "graph_replay": {"value": world * len(tgt) / (gms / 1000), "ms_per_step": gms,
+                            "note": "P2M..L2P + near field replayed on the fixed forest (new strengths, same points)"},
+           "rel_l2_vs_fp64_direct": err, "max_coil_rel_l2": max(per_coil),
+           "error_samples": "16 seeded targets per coil (4096) vs FP64 direct over the coil's sources",
+           "phases_ms": phases, "tree": _tree_stats(plan)}
+    plan.close()
+    return res
+
+
+def extra_c5(local, world, steps):
+    """Differentiation workload: forward + adjoint of loss = 1/2 sum |B - B*|^2."""
+    import torch
+    from bachelors_b200 import Plan, geometry as G
+    xyz, w, J = G.torus(256, 64, 64, 2.0, 0.5, current="poloidal")
+    rng = np.random.default_rng(20260005)
+    Jstar = J * (1 + 0.05 * rng.normal(size=(len(J), 1)))
+    tgt = G.uniform_points(1 << 18, -3.0, 3.0, 20260005)
+    dev = f"cuda:{local}"
+    f32 = lambda a: torch.from_numpy(a.astype(np.float32)).to(dev)
+    plan = Plan(order=12, leaf_capacity=64, precision="fp32", m2l="bf16x3", device=local)
+    plan.set_sources(f32(xyz), f32(w), f32(Jstar))
+    plan.set_targets(f32(tgt))
+    Bstar, _ = plan.solve(1.0, 1)
+    Bstar = Bstar.clone()
+    plan.update_sources(f32(w), f32(J))
+
+    def step():
+        B, _ = plan.solve(1.0, 1)
+        g = B - Bstar
+        return plan.adjoint(g, 1.0)
+    for _ in range(3):
+        step()
+    ms, (dJ, dX) = _timed(step, steps, world)
+    fms, _ = _timed(lambda: plan.solve(1.0, 1), steps, world)
+    B, _ = plan.solve(1.0, 1)
+    g = (B - Bstar).cpu().numpy().astype(np.float64)
+    # FP64 direct-sum adjoint for 64 seeded sources (each source's gradient involves only itself
+    # and the targets, so a plan holding just those sources gives their exact gradients)
+    pick = rng.choice(len(xyz), size=64, replace=False)
+    ref = Plan(order=1, leaf_capacity=1 << 30, precision="fp64", device=local)
+    ref.set_sources(xyz[pick], w[pick], J[pick])
+    ref.set_targets(tgt)
+    rJ, rX = ref.adjoint_direct(g, 1.0)
+    ref.close()
+    gJ = dJ.cpu().numpy().astype(np.float64)[pick]
+    gX = dX.cpu().numpy().astype(np.float64)[pick]
+    res = {"workload": "FP32 torus 256x64x64 = 2^20 sources, 2^18 targets U[-3,3]^3, loss 1/2 sum|B - B*|^2 with "
+                       "B* from J (1 + 0.05 N(0,1)), p=12, leaf 64, BF16X3 M2L; seed 20260005",
+           "value": world * len(tgt) / (ms / 1000), "unit": "loss+gradient evals/s (targets)", "ms_per_step": ms,
+           "forward_ms": fms, "adjoint_over_forward": (ms - fms) / fms, "steps": steps,
+           "rel_l2_dLdJ_vs_fp64_direct_adjoint": float(np.linalg.norm(gJ - rJ) / np.linalg.norm(rJ)),
+           "rel_l2_dLdx_vs_fp64_direct_adjoint": float(np.linalg.norm(gX - rX) / np.linalg.norm(rX)),
+           "error_samples": "64 seeded sources (g from this run's B)"}
+    plan.close()
+    return res
+
+
+EXTRAS = {"c1": extra_c1, "c2": extra_c2, "batch": extra_batch, "c5": extra_c5}
+
+
 def count_launches(plan):
     """Kernels one solve launches (from the CUDA profiler), excluding library kernels."""
     import torch
@@ -205,6 +389,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison solve")
     ap.add_argument("--no-launch-count", action="store_true", help="skip the profiler-based launch count")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing")
+    ap.add_argument("--extra", default="c1,c2,batch,c5",
+                    help="comma list of further workloads to measure into 'workloads' (c1, c2, batch, c5; '' = none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -378,6 +564,15 @@ def main():
                        "h2d_bytes_per_step": int(xyz.nbytes + w.nbytes + J.nbytes + xyz.nbytes),
                        "d2h_bytes_per_step": int(Bh2.nbytes), "ms_per_step": e2e_ms}
         s.plan.close()
+
+    extras = [e for e in args.extra.split(",") if e]
+    if extras:
+        line["workloads"] = {}
+        for e in extras:
+            try:
+                line["workloads"][e] = EXTRAS[e](local, world, args.steps)
+            except Exception as ex:  # keep the headline line even if a secondary workload fails
+                line["workloads"][e] = {"error": f"{type(ex).__name__}: {str(ex)[:300]}"}
 
     if rank == 0 and world == 1 and not args.no_cpu:
         try:

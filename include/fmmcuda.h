@@ -138,6 +138,12 @@ fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* 
 fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx, int on_device,
                        void* stream);
 
+/* The same gradients as fmm_adjoint by direct O(N M) summation (FP64 accumulation, results in the
+ * plan's element type), for checking the adjoint FMM and for small problems. Needs only sources and
+ * targets (no tree); respects the coils of a batched plan. */
+fmm_status fmm_adjoint_direct(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx,
+                              int on_device, void* stream);
+
 /* Batching (no counterpart in the reference, which solves one coil per solver object): many
  * independent problems ("coils") in one plan. Coil c owns the sources [src_offsets[c], src_offsets[c+1])
  * and the targets [tgt_offsets[c], tgt_offsets[c+1]) of the arrays given to fmm_set_sources /

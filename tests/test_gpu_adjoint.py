@@ -98,3 +98,22 @@ def test_autograd_wrapper_against_finite_differences():
             vals.append((lossf(xp, J) - lossf(xm, J)) / (2 * hh))
         fd = (4 * vals[1] - vals[0]) / 3
         assert abs(fd - gx[q, d]) <= 1e-5 * abs(fd) + 1e-9 * np.abs(gx).max()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+@pytest.mark.parametrize("with_J", [True, False])
+def test_adjoint_direct_matches_oracle(precision, tol, with_J):
+    from bachelors_b200 import Plan, geometry as G
+    from oracle import oracle as O
+    xyz, w, J = G.torus(16, 8, 4, 2.0, 0.5)
+    tgt = G.uniform_points(700, -3, 3, 4)
+    g = np.random.default_rng(8).normal(size=tgt.shape)
+    dt = np.float64 if precision == "fp64" else np.float32
+    plan = Plan(order=4, leaf_capacity=32, precision=precision)
+    plan.set_sources(xyz.astype(dt), w.astype(dt), J.astype(dt) if with_J else None)
+    plan.set_targets(tgt.astype(dt))
+    dJ, dx = plan.adjoint_direct(g.astype(dt), 1.7)
+    rJ, rx = O.adjoint_direct(xyz, w, J if with_J else None, tgt, g, current=1.7)
+    assert np.linalg.norm(dJ - rJ) / np.linalg.norm(rJ) < tol
+    assert np.linalg.norm(dx - rx) / np.linalg.norm(rx) < tol
+    plan.close()
