@@ -44,7 +44,8 @@ class FmmStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_near", "ms_total")] + [
         (k, ctypes.c_int64)
         for k in ("nodes", "leaves", "levels", "v_pairs", "p2p_pairs", "p2p_interactions", "n_sources", "n_targets")
-    ] + [("ms_adjoint", ctypes.c_double), ("coils", ctypes.c_int64)]
+    ] + [("ms_adjoint", ctypes.c_double), ("coils", ctypes.c_int64), ("m2l_tiles", ctypes.c_int64),
+         ("m2l_tile_offsets", ctypes.c_int64)]
 
 
 class FmmError(RuntimeError):

@@ -73,6 +73,11 @@ fmm_status Plan::init(const fmm_config& c)
    fp64 = c.precision == FMM_FP64;
    const char* dbg = getenv("FMM_DEBUG_SYNC");
    debugSync = dbg && dbg[0] == '1';
+   if(const char* e = getenv("FMM_TC_KC")) tcKChunk = atoi(e) == 32 ? 32 : 64;
+   if(const char* e = getenv("FMM_TC_DRAIN")) tcDrainEvery = std::max(1, atoi(e));
+   if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(2, std::max(0, atoi(e)));
+   if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
+   if(const char* e = getenv("FMM_TC_BALANCED")) tcBalancedN = atoi(e) != 0;
    FMM_TRY(rootb.reserve(sizeof(RootBox)));
    FMM_TRY(errb.reserve(sizeof(int)));
    FMM_TRY(initOffsetTables());
@@ -94,7 +99,7 @@ void Plan::release()
    }
    DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
                      &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &m2lTargets, &m2lKeys, &errb,
-                     &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf,
+                     &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf, &multBf, &tcCounters,
                      &adjG, &adjOut};
    for(DevBuf* b : bufs) b->release();
    for(auto& b : nodeBufs) b.release();
@@ -653,6 +658,19 @@ fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats)
    s.n_sources = P.n;
    s.n_targets = P.m;
    s.coils = P.nCoils;
+   s.m2l_tiles = 0;
+   s.m2l_tile_offsets = 0;
+   if(P.downReady && P.tcTiles > 0 && P.tcCounters.ptr && !P.fp64 && P.cfg.m2l_mode != FMM_M2L_SIMT)
+   {
+      unsigned long long c[2] = {0, 0};
+      cudaEventSynchronize(P.ev[4]);
+      if(cudaMemcpy(c, P.tcCounters.ptr, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess)
+      {
+         s.m2l_tiles = P.tcTiles;
+         s.m2l_tile_offsets = int64_t(c[1]);
+      }
+      else cudaGetLastError();
+   }
    *stats = s;
    return FMM_OK;
 }

@@ -136,7 +136,16 @@ struct Plan
    DevBuf opM2M64, opL2L64, opM2L64;     // [8][L][L], [8][L][L], [316][L][L] FP64 row-major
    DevBuf opM2Mw, opL2Lw, opM2Lw;        // transposed working copies, see fmm_kernels.cu
    DevBuf opM2Lbf;                       // bf16 hi/lo split for the tensor-core M2L
+   DevBuf multBf;                        // multipoles split into bf16 pieces for the tensor-core M2L
    int opOrder = -1;
+   // tensor-core M2L tile choices (autotuned per order and leaf capacity, or set by environment)
+   int tcKChunk = 0;                     // K chunk width 32 or 64 (0: 64 for BF16X3, 32 for BF16X6)
+   int tcDrainEvery = 8;                 // offsets accumulated in tensor memory between drains
+   int tcDrainMode = 2;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1
+   int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length
+   int tcBalancedN = 0;                  // split the N output columns into two near-equal MMAs
+   DevBuf tcCounters;                    // [items, tile-offset pairs] of the last tensor-core M2L
+   int64_t tcTiles = 0;
    int opImgOrder = -1;                  // order the tensor-core operator image was built for
    // state
    bool treeReady = false, upReady = false, downReady = false;

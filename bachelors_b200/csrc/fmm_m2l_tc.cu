@@ -17,10 +17,13 @@
 // Warp roles (448 threads):
 //   warp 0      TMEM allocation; lane 0 issues the tcgen05.mma instructions
 //   warp 1      lane 0 streams the pre-swizzled operator image with cp.async.bulk (no multicast)
-//   warps 2..9  gather source rows (FP32), split to bf16 pieces, store in the swizzled K-major layout
-//   warps 10-13 drain: every few offsets tcgen05.ld the accumulator and add it to the FP32 local
-//               expansions in global memory (the tensor-core accumulation truncates; long chains
-//               into one TMEM value lose accuracy), then release TMEM for a fresh accumulation
+//   warps 2..9  gather the source rows, already split into bf16 pieces once per solve
+//               (kSplitMultipoles), with 16-byte cp.async copies into the swizzled K-major layout
+//   warps 10-13 drain: every few offsets tcgen05.ld the accumulator and add it to FP32 running
+//               sums (the tensor-core accumulation truncates; long chains into one TMEM value lose
+//               accuracy), then release the accumulator for a fresh accumulation. The running sums
+//               live in the tensor-memory columns the accumulator leaves free (208 of 512 at
+//               p = 16, all of them at p <= 12), the rest in the local expansions in global memory
 // Stages hold one K chunk of every piece of A and of T_o; two stages rotate through mbarriers
 // (full: producers + bulk-copy bytes, empty: tcgen05.commit). Every wait is bounded by
 // a 2 s global-timer limit; on expiry the CTA records FMM timeout in the error word and stops.
@@ -96,6 +99,14 @@ __device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity, int* err
    }
 }
 
+// 16-byte global -> shared copy; srcBytes = 0 writes zeros without reading.
+__device__ __forceinline__ void cpAsync16(uint32_t dst, const void* src, uint32_t srcBytes)
+{
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(srcBytes) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void bulkLoad(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
 {
    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -131,6 +142,26 @@ __device__ __forceinline__ void fenceBeforeSync() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void fenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// 32 lanes x 16 columns of FP32 from tensor memory; no wait (tcgen05.wait::ld before use).
+__device__ __forceinline__ void tmemLd16NoWait(uint32_t addr, uint32_t* r)
+{
+   asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+}
+__device__ __forceinline__ void tmemWaitLd() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmemSt16(uint32_t addr, const uint32_t* r)
+{
+   asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+      ::"r"(addr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+        "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void tmemWaitSt() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void tmemLd16(uint32_t addr, float* v)
 {
    uint32_t r[16];
@@ -145,34 +176,35 @@ __device__ __forceinline__ void tmemLd16(uint32_t addr, float* v)
 }
 
 
-// Operand layout for NP bf16 pieces per value (2: hi + lo, 3: hi + mid + lo). With two pieces a K
-// chunk is 64 elements in 128-byte rows (SW128, 108 KB per stage); with three it is 32 elements in
-// 64-byte rows (SW64, 83 KB per stage); two stages in both. (Four SW64 stages of two pieces were
-// measured slower than two SW128 stages: more barrier round trips per offset.)
-template <int NP> struct Layout;
-template <> struct Layout<2>
+// Operand layout of one K chunk of KCW bf16 elements per row: 64 elements in 128-byte rows
+// (128-byte swizzle) or 32 elements in 64-byte rows (64-byte swizzle). A stage holds one chunk
+// of every piece of A (128 rows) and of T_o (N rows); the number of stages is what fits in
+// shared memory (2 with 64-wide chunks of two pieces at p = 16, 4 with 32-wide ones).
+template <int KCW> struct Layout;
+template <> struct Layout<64>
 {
-   static constexpr int KC = 64, RB = 128, SBO = 1024, SWZ = 2, NSTAGE = 2;
+   static constexpr int KC = 64, RB = 128, SBO = 1024, SWZ = 2;
    __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
    { return row * 128u + ((((k >> 3) ^ (row & 7u)) & 7u) << 4) + ((k & 7u) << 1); }
 };
-template <> struct Layout<3>
+template <> struct Layout<32>
 {
-   static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4, NSTAGE = 2;
+   static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4;
    __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
    { return row * 64u + ((((k >> 3) ^ ((row >> 1) & 3u)) & 3u) << 4) + ((k & 7u) << 1); }
 };
+constexpr int MAXSTAGE = 6;
 
 // Shared-memory matrix descriptor: K-major, swizzled rows, 8-row groups SBO bytes apart.
-template <int NP>
+template <int KCW>
 __device__ __forceinline__ uint64_t smemDescT(uint32_t addr)
 {
    uint64_t d = 0;
    d |= uint64_t((addr >> 4) & 0x3FFF);               // start address
    d |= uint64_t(1) << 16;                             // leading byte offset (unused when swizzled)
-   d |= uint64_t(Layout<NP>::SBO >> 4) << 32;         // stride byte offset
+   d |= uint64_t(Layout<KCW>::SBO >> 4) << 32;        // stride byte offset
    d |= uint64_t(1) << 46;                             // descriptor version for sm_100
-   d |= uint64_t(Layout<NP>::SWZ) << 61;              // swizzle mode
+   d |= uint64_t(Layout<KCW>::SWZ) << 61;             // swizzle mode
    return d;
 }
 
@@ -194,10 +226,10 @@ __device__ __forceinline__ void splitBf16(double x, __nv_bfloat16* piece)
 // Operator image for the tensor-core M2L: for every offset slot and K chunk, the NP piece blocks
 // (hi first), each N rows (output coefficients, N = Lp) x KC bf16 (input coefficients) in the
 // swizzled K-major layout, zero outside the (p+1)^2 x (p+1)^2 operator.
-template <int NP>
+template <int NP, int KCW>
 __global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int nChunks, uint8_t* img)
 {
-   using Lay = tc::Layout<NP>;
+   using Lay = tc::Layout<KCW>;
    const int64_t blockBytes = int64_t(N) * Lay::RB;
    const int64_t total = int64_t(316) * nChunks * int64_t(N) * Lay::KC;
    for(int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
@@ -218,13 +250,36 @@ __global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int
    }
 }
 
+// The multipoles split into NP bf16 pieces, once per solve: Mbf[node][comp][piece][Lp], each
+// piece the round-to-nearest of the remaining FP32 residual (exact: every piece removes the
+// leading bits of the remainder).
 template <int NP>
+__global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int Lp, __nv_bfloat16* __restrict__ Mbf)
+{
+   const int64_t total = rows * Lp;
+   for(int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
+   {
+      const int64_t row = e / Lp;
+      const int k = int(e % Lp);
+      float r = M[e];
+#pragma unroll
+      for(int j = 0; j < NP; j++)
+      {
+         const __nv_bfloat16 b = __float2bfloat16_rn(r);
+         Mbf[(row * NP + j) * Lp + k] = b;
+         r -= __bfloat162float(b);
+      }
+   }
+}
+
+template <int NP, int KCW>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
-kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int Lp, int nChunks,
-       const uint8_t* __restrict__ img, const float* __restrict__ M, float* __restrict__ Lc, int drainEvery, int* err)
+kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int L, int Lp, int nChunks,
+       const uint8_t* __restrict__ img, const __nv_bfloat16* __restrict__ Mbf, float* __restrict__ Lc, int drainEvery,
+       int nStages, int drainMode, int nFirst, unsigned long long* counters, int* err)
 {
    using namespace tc;
-   using Lay = Layout<NP>;
+   using Lay = Layout<KCW>;
    constexpr int KCH = Lay::KC;
    constexpr int NPASS = NP == 2 ? 3 : 6;
    // (A piece, B piece) of every product kept: hi*hi, hi*lo, lo*hi  /  down to 2^-16 with three pieces
@@ -240,7 +295,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    const uint32_t rawAddr = smemAddr(smraw);
    const uint32_t base = (rawAddr + 1023u) & ~1023u;
    uint8_t* sbase = smraw + (base - rawAddr);
-   constexpr int NS = Lay::NSTAGE;
+   const int NS = nStages;
    uint8_t* ctrl = sbase + NS * stageBytes;
    uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);          // full[NS], empty[NS], done, drainFull, drainEmpty
    uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 128);
@@ -297,6 +352,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          if(present[o >> 5] & (1u << (o & 31))) itemOffset[k++] = o;
       }
       itemOffset[316] = k;
+      // work accounting: pipeline items (offset x K chunk) and tile-offset pairs
+      atomicAdd(counters, (unsigned long long)(k * nChunks));
+      atomicAdd(counters + 1, (unsigned long long)k);
    }
    __syncthreads();
    const int nOff = itemOffset[316];
@@ -307,8 +365,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    {
       if(lane == 0)
       {
-         const int nB = N - 256;                       // second MMA's width (48 at p = 16)
-         const uint32_t idA = instrDescBf16(ROWS, N <= 256 ? N : 256);
+         // the N output columns in one MMA (N <= 256) or two: nFirst + (N - nFirst), both multiples of 16
+         const int nA = nFirst, nB = N - nFirst;
+         const uint32_t idA = instrDescBf16(ROWS, nA);
          const uint32_t idB = nB > 0 ? instrDescBf16(ROWS, nB) : 0u;
          bool firstMma = true;
          int drains = 0;
@@ -319,9 +378,13 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
             const uint32_t aSt = st, bSt = st + NP * aBytes;
+            // K steps of 16 that reach a coefficient < L (the last chunk is partly padding)
+            const int cItem = nChunks - 1 - it % nChunks;
+            const int kSteps = min(KCH / 16, (L - cItem * KCH + 15) / 16);
 #pragma unroll
             for(int ks = 0; ks < KCH / 16; ks++)
             {
+               if(ks >= kSteps) break;
                const uint32_t koff = ks * 32;
 #pragma unroll
                for(int pass = 0; pass < NPASS; pass++)
@@ -331,8 +394,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                   const uint32_t a = aSt + pa * aBytes + koff;
                   const uint32_t b = bSt + pb * bBytes + koff;
                   const uint32_t acc = firstMma ? 0u : 1u;
-                  mmaBf16(tmem, smemDescT<NP>(a), smemDescT<NP>(b), idA, acc);
-                  if(nB > 0) mmaBf16(tmem + 256, smemDescT<NP>(a), smemDescT<NP>(b + 256 * Lay::RB), idB, acc);
+                  mmaBf16(tmem, smemDescT<KCW>(a), smemDescT<KCW>(b), idA, acc);
+                  if(nB > 0) mmaBf16(tmem + nA, smemDescT<KCW>(a), smemDescT<KCW>(b + nA * Lay::RB), idB, acc);
                   firstMma = false;
                }
             }
@@ -384,23 +447,84 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       const int r = lanes + lane;
       const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
       float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
+      const uint32_t tAcc = tmem + (uint32_t(lanes) << 16);
       const int nDrains = (nOff + drainEvery - 1) / drainEvery;
-      // The running sum lives in the (zero-initialised) local expansions: fire-and-forget FP32
-      // vector adds, rounded to nearest. Each row has one writer, this thread, and same-address
-      // operations of one thread stay in program order, so the result is deterministic.
+      // The running sum is FP32, rounded to nearest, and has one writer per row (this thread); the
+      // locals start at zero and no other CTA touches these rows, so the result is deterministic.
+      //   drainMode 0: every drain adds into the locals with fire-and-forget vector atomics.
+      //   drainMode 1: the first drain stores, later ones load, add and store (prefetched).
+      //   drainMode 2: as 1, but the running sums of the first nS columns stay in the tensor memory
+      //                the accumulator leaves free (columns N .. 511); only the rest, and the final
+      //                result, travel to global memory.
+      const int nS = drainMode == 2 ? (min(N, 512 - N) & ~15) : 0;
+      const uint32_t tSum = tAcc + uint32_t(N);
       for(int d = 0; d < nDrains; d++)
       {
          if(!mbarWait(drainFull, d & 1, err, abortFlag)) break;
          fenceAfterSync();
-         for(int c0 = 0; c0 < N; c0 += 16)
+         const bool last = d == nDrains - 1;
+         // running sums kept in tensor memory: S += acc (d > 0) or S = acc; the last drain writes
+         // S + acc to the locals instead
+         for(int c0 = 0; c0 < nS; c0 += 16)
          {
-            float v[16];
-            tmemLd16(tmem + (uint32_t(lanes) << 16) + uint32_t(c0), v);
-            if(et >= 0)
-            {
-               float4* o4 = reinterpret_cast<float4*>(out + c0);
+            uint32_t a[16], sv[16];
+            tmemLd16NoWait(tAcc + uint32_t(c0), a);
+            if(d > 0) tmemLd16NoWait(tSum + uint32_t(c0), sv);
+            tmemWaitLd();
 #pragma unroll
-               for(int i = 0; i < 4; i++) atomicAdd(o4 + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+            for(int i = 0; i < 16; i++)
+               sv[i] = d > 0 ? __float_as_uint(__uint_as_float(sv[i]) + __uint_as_float(a[i])) : a[i];
+            if(last)
+            {
+               if(et >= 0)
+               {
+                  float4* o4 = reinterpret_cast<float4*>(out + c0);
+#pragma unroll
+                  for(int i = 0; i < 4; i++)
+                     o4[i] = make_float4(__uint_as_float(sv[4 * i]), __uint_as_float(sv[4 * i + 1]),
+                                         __uint_as_float(sv[4 * i + 2]), __uint_as_float(sv[4 * i + 3]));
+               }
+            }
+            else
+               tmemSt16(tSum + uint32_t(c0), sv);
+         }
+         if(nS > 0 && !last) tmemWaitSt();
+         // the remaining columns through global memory, 16 per step; with load-add-store the next
+         // step's running sums are loaded before this step's accumulator values are read
+         const bool rmw = drainMode != 0 && d > 0 && et >= 0;
+         float4 nxt[4];
+         if(rmw && nS < N)
+         {
+            const float4* o4 = reinterpret_cast<const float4*>(out + nS);
+#pragma unroll
+            for(int i = 0; i < 4; i++) nxt[i] = o4[i];
+         }
+         for(int c0 = nS; c0 < N; c0 += 16)
+         {
+            uint32_t u[16];
+            float4 old[4];
+            float4* o4 = reinterpret_cast<float4*>(out + c0);
+            if(rmw)
+            {
+#pragma unroll
+               for(int i = 0; i < 4; i++) old[i] = nxt[i];
+               if(c0 + 16 < N)
+               {
+#pragma unroll
+                  for(int i = 0; i < 4; i++) nxt[i] = o4[4 + i];
+               }
+            }
+            tmemLd16NoWait(tAcc + uint32_t(c0), u);
+            tmemWaitLd();
+            if(et < 0) continue;
+#pragma unroll
+            for(int i = 0; i < 4; i++)
+            {
+               const float4 v = make_float4(__uint_as_float(u[4 * i]), __uint_as_float(u[4 * i + 1]),
+                                            __uint_as_float(u[4 * i + 2]), __uint_as_float(u[4 * i + 3]));
+               if(drainMode == 0) atomicAdd(o4 + i, v);
+               else if(d == 0) o4[i] = v;
+               else o4[i] = make_float4(old[i].x + v.x, old[i].y + v.y, old[i].z + v.z, old[i].w + v.w);
             }
          }
          fenceBeforeSync();
@@ -409,60 +533,53 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    }
    else
    {
-      // producers (warps 2..9): two threads per row, KCH / 2 K-elements each
+      // producers (warps 2..9): two threads per row, KCH / 2 K-elements (KCH / 8 chunks of 16 bytes)
+      // of every piece each. Item it - 1 is signalled as soon as its copies have landed, then the
+      // copies of item it are issued once its stage is free: one item's gather is in flight while
+      // the tensor cores work on the previous one, and issuing never delays a signal.
       constexpr int PER = KCH / 2;
       const int ptid = tid - 64;
       const int row = ptid >> 1, half = ptid & 1;
       const int slot = row / 3, comp = row % 3;
       const int tgt = row < 3 * TT ? tileNode[slot] : -1;
+      int src = (tgt >= 0 && nItems > 0) ? vtab[int64_t(tgt) * 316 + itemOffset[0]] : -1;
+      int srcNext = -1;
+      int pending = -1;
       for(int it = 0; it < nItems; it++)
       {
          const int s = it % NS;
+         const int oi = it / nChunks, c = nChunks - 1 - it % nChunks;
+         if(it % nChunks == 0 && oi + 1 < nOff)
+            srcNext = tgt >= 0 ? vtab[int64_t(tgt) * 316 + itemOffset[oi + 1]] : -1;
+         if(pending >= 0)
+         {
+            cpAsyncWaitAll();
+            fenceProxyAsync();
+            mbarArrive(fullBar0 + 8 * (pending % NS));
+            pending = -1;
+         }
          if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag)) break;
-         const int o = itemOffset[it / nChunks], c = nChunks - 1 - it % nChunks;
-         const int src = tgt >= 0 ? vtab[int64_t(tgt) * 316 + o] : -1;
-         uint8_t* aSt = sbase + s * stageBytes;
+         const uint32_t aSt = base + s * stageBytes;
          const int k0 = c * KCH + half * PER;
+         const __nv_bfloat16* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp;
 #pragma unroll
          for(int q = 0; q < PER / 8; q++)
          {
-            float v[8];
             const int k = k0 + 8 * q;
-            if(src >= 0 && k < Lp)
-            {
-               const float4* p = reinterpret_cast<const float4*>(M + (int64_t(src) * 3 + comp) * Lp + k);
-               const float4 x0 = __ldg(p), x1 = __ldg(p + 1);
-               v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w; v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
-            }
-            else
-            {
-#pragma unroll
-               for(int i = 0; i < 8; i++) v[i] = 0.f;
-            }
-            uint32_t w[NP][4];
-#pragma unroll
-            for(int i = 0; i < 4; i++)
-            {
-               __nv_bfloat16 p0[NP], p1[NP];
-               // FP32 residuals are exact here: each piece removes the leading bits of the remainder
-               float r0 = v[2 * i], r1 = v[2 * i + 1];
-#pragma unroll
-               for(int j = 0; j < NP; j++)
-               {
-                  p0[j] = __float2bfloat16_rn(r0);
-                  p1[j] = __float2bfloat16_rn(r1);
-                  r0 -= __bfloat162float(p0[j]);
-                  r1 -= __bfloat162float(p1[j]);
-                  w[j][i] = uint32_t(__bfloat16_as_ushort(p0[j])) | (uint32_t(__bfloat16_as_ushort(p1[j])) << 16);
-               }
-            }
+            const uint32_t bytes = (src >= 0 && k < Lp) ? 16u : 0u;
             const uint32_t off = Lay::off(uint32_t(row), uint32_t(half * PER + 8 * q));
 #pragma unroll
-            for(int j = 0; j < NP; j++)
-               *reinterpret_cast<uint4*>(aSt + j * aBytes + off) = make_uint4(w[j][0], w[j][1], w[j][2], w[j][3]);
+            for(int j = 0; j < NP; j++) cpAsync16(aSt + j * aBytes + off, rowp + j * Lp + (bytes ? k : 0), bytes);
          }
+         cpAsyncCommit();
+         pending = it;
+         if(it % nChunks == nChunks - 1) src = srcNext;
+      }
+      cpAsyncWaitAll();
+      if(pending >= 0 && !*abortFlag)
+      {
          fenceProxyAsync();
-         mbarArrive(fullBar0 + 8 * s);
+         mbarArrive(fullBar0 + 8 * (pending % NS));
       }
    }
    fenceBeforeSync();
@@ -477,18 +594,19 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    }
 }
 
-template <int NP>
+template <int NP, int KCW>
 static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
 {
-   using Lay = tc::Layout<NP>;
+   using Lay = tc::Layout<KCW>;
    const int L = P.L, Lp = P.Lp;
    const int nChunks = (L + Lay::KC - 1) / Lay::KC;
    const size_t imgBytes = size_t(316) * nChunks * NP * size_t(Lp) * Lay::RB;
-   const int tag = P.p * 8 + NP;
+   const int tag = (P.p * 8 + NP) * 128 + KCW;
    if(P.opImgOrder != tag)
    {
       FMM_TRY(P.opM2Lbf.reserve(imgBytes));
-      kPrepM2LImage<NP><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, L, Lp, nChunks, (uint8_t*)P.opM2Lbf.ptr);
+      kPrepM2LImage<NP, KCW><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, L, Lp, nChunks,
+                                                   (uint8_t*)P.opM2Lbf.ptr);
       FMM_TRY(launched(P, "kPrepM2LImage", st));
       P.opImgOrder = tag;
    }
@@ -496,15 +614,27 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(count <= 0) return FMM_OK;
    const int blocks = (count + tc::TT - 1) / tc::TT;
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t smem = 1024 + Lay::NSTAGE * stageBytes + 192 + 4 * (320 + 64);
-   if(smem > 232448) return setError(FMM_E_INVALID, "tensor-core M2L: %zu bytes of shared memory needed", smem);
-   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   const size_t fixed = 1024 + 192 + 4 * (320 + 64);
+   const size_t budget = 232448;
+   const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
+   if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
+   const size_t smem = fixed + nStages * stageBytes;
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, KCW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
-   int drainEvery = 8;
-   if(const char* e = getenv("FMM_TC_DRAIN")) drainEvery = std::max(1, atoi(e));
-   kM2LTc<NP><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, Lp, nChunks,
-                                                 (const uint8_t*)P.opM2Lbf.ptr, (const float*)P.mult.ptr,
-                                                 (float*)P.local.ptr, drainEvery, P.err);
+   FMM_TRY(P.tcCounters.reserve(2 * sizeof(unsigned long long)));
+   FMM_CUDA(cudaMemsetAsync(P.tcCounters.ptr, 0, 2 * sizeof(unsigned long long), st));
+   P.tcTiles = blocks;
+   // first MMA's width: all of N up to 256, else 256 or (balanced) the multiple of 16 nearest N / 2;
+   // the second starts on an 8-row boundary of the swizzled operator block either way
+   const int nFirst = Lp <= 256 ? Lp : (P.tcBalancedN ? ((Lp / 2 + 15) / 16) * 16 : 256);
+   const int64_t rows = P.tree.nNodes * 3;
+   FMM_TRY(P.multBf.reserve(sizeof(__nv_bfloat16) * rows * NP * Lp));
+   kSplitMultipoles<NP><<<148 * 16, 256, 0, st>>>((const float*)P.mult.ptr, rows, Lp, (__nv_bfloat16*)P.multBf.ptr);
+   FMM_TRY(launched(P, "kSplitMultipoles", st));
+   kM2LTc<NP, KCW><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, L, Lp, nChunks,
+                                                      (const uint8_t*)P.opM2Lbf.ptr, (const __nv_bfloat16*)P.multBf.ptr,
+                                                      (float*)P.local.ptr, P.tcDrainEvery, nStages, P.tcDrainMode,
+                                                      nFirst, (unsigned long long*)P.tcCounters.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
    int herr = 0;
@@ -518,8 +648,10 @@ fmm_status m2lTensorCore(Plan& P, cudaStream_t st)
 {
    if(P.Lp > 320) return setError(FMM_E_INVALID, "tensor-core M2L supports p <= 16");
    if(P.Lp % 16) return setError(FMM_E_INVALID, "tensor-core M2L needs 16-aligned coefficient rows");
-   if(P.cfg.m2l_mode == FMM_M2L_BF16X3) return launchM2LTc<2>(P, st);
-   if(P.cfg.m2l_mode == FMM_M2L_BF16X6) return launchM2LTc<3>(P, st);
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X3)
+      return P.tcKChunk == 32 ? launchM2LTc<2, 32>(P, st) : launchM2LTc<2, 64>(P, st);
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X6)
+      return P.tcKChunk == 64 ? launchM2LTc<3, 64>(P, st) : launchM2LTc<3, 32>(P, st);
    return setError(FMM_E_INVALID, "tensor-core M2L: the TF32 mode is not built");
 }
 

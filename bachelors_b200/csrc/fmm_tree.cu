@@ -423,12 +423,15 @@ __global__ void kP2PLists(Tree t, Lists L, int nNodes, const int* __restrict__ o
 // Keys that group the boxes with an M2L list by their octant in the parent (boxes without one
 // sort last): boxes of one octant can only see the 189 offsets that octant allows, so tiles of
 // same-octant boxes leave fewer rows of the tensor-core M2L empty.
-__global__ void kM2LTargetKeys(Tree t, Lists L, int nNodes, unsigned* keys, int* vals, int* count)
+__global__ void kM2LTargetKeys(Tree t, Lists L, int nNodes, int byCount, unsigned* keys, int* vals, int* count)
 {
    int i = blockIdx.x * blockDim.x + threadIdx.x;
    if(i >= nNodes) return;
    bool has = L.nv[i] > 0;
-   keys[i] = has ? unsigned(t.key[i] & 7) : 8u;
+   // octant, then (optionally) the list length, longest first: boxes with full neighbourhoods fill
+   // whole tiles, sparse boundary boxes share tiles with each other
+   const unsigned sub = byCount ? unsigned(316 - min(L.nv[i], 316)) : 0u;
+   keys[i] = has ? (unsigned(t.key[i] & 7) << 9) | sub : (8u << 9);
    vals[i] = i;
    if(has) atomicAdd(count, 1);
 }
@@ -641,13 +644,13 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       unsigned* kk = (unsigned*)P.m2lKeys.ptr;
       int* vv = (int*)P.m2lTargets.ptr;
       FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
-      kM2LTargetKeys<<<(nn + 255) / 256, 256, 0, st>>>(t, Ls, nn, kk + nn, vv + nn, P.err);
+      kM2LTargetKeys<<<(nn + 255) / 256, 256, 0, st>>>(t, Ls, nn, P.tcGroupByCount, kk + nn, vv + nn, P.err);
       FMM_TRY(launched(P, "kM2LTargetKeys", st));
       tmp = 0;
-      cub::DeviceRadixSort::SortPairs(nullptr, tmp, kk + nn, kk, vv + nn, vv, nn, 0, 4, st);
+      cub::DeviceRadixSort::SortPairs(nullptr, tmp, kk + nn, kk, vv + nn, vv, nn, 0, 13, st);
       FMM_TRY(P.cubTmp.reserve(tmp));
       tmp = P.cubTmp.bytes;
-      FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, kk + nn, kk, vv + nn, vv, nn, 0, 4, st));
+      FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, kk + nn, kk, vv + nn, vv, nn, 0, 13, st));
       int cntT = 0;
       FMM_CUDA(cudaMemcpyAsync(&cntT, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
       FMM_CUDA(cudaStreamSynchronize(st));

@@ -472,7 +472,7 @@ def main():
                    "l2_flush": "inputs larger than L2 (2^24 points)", "parallelism": f"replicas x{world}"},
         "rel_l2_vs_fp64_direct": rel_err,
         "phases_ms": {k: st[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_near", "ms_total")},
-        "tree": {k: st[k] for k in ("nodes", "levels", "v_pairs", "p2p_pairs")},
+        "tree": {k: st[k] for k in ("nodes", "levels", "v_pairs", "p2p_pairs", "m2l_tiles", "m2l_tile_offsets")},
         "roofline": {"kernel": f"M2L ({m2l})", "bound": "tensor", "achieved": achieved, "peak": bf16_peak,
                      "unit": "TFLOP/s", "frac": achieved / bf16_peak, "traffic": None,
                      "flops_per_launch": flops_m2l,

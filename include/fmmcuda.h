@@ -80,6 +80,8 @@ typedef struct fmm_stats {
    int64_t n_sources, n_targets;
    double ms_adjoint; /* the last fmm_adjoint call */
    int64_t coils;     /* independent problems in the plan (1 unless batched) */
+   int64_t m2l_tiles, m2l_tile_offsets; /* tensor-core M2L: 42-box tiles and (tile, offset) steps;
+                                           the row fill is 3 v_pairs / (128 m2l_tile_offsets) */
 } fmm_stats;
 
 void fmm_default_config(fmm_config* cfg);
