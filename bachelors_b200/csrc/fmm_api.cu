@@ -98,7 +98,7 @@ void Plan::release()
       adj = nullptr;
    }
    DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
-                     &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &m2lTargets, &m2lKeys, &errb,
+                     &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &parList, &m2lTargets, &m2lKeys, &errb,
                      &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf, &multBf, &tcCounters,
                      &adjG, &adjOut};
    for(DevBuf* b : bufs) b->release();

@@ -126,6 +126,8 @@ struct Plan
    DevBuf p2pOff, p2pList;
    int nP2P = 0;
    int64_t nV = 0;
+   DevBuf parList;                      // nodes with children, in node order (M2M / L2L tiles)
+   std::vector<int> parStart;           // parList index where each level's parents start [nLevels + 1]
    DevBuf m2lTargets, m2lKeys;          // boxes with an M2L list, grouped by octant
    int nM2LTargets = 0;
    int* err = nullptr;

@@ -226,6 +226,165 @@ fmm_status buildOperators(Plan& P, cudaStream_t st)
 }
 
 // ====================================================================================
+// M2M and L2L as tiled GEMMs over the parents of one level. A block takes 32 parents (96 rows:
+// parent x component) and 64 output coefficients; for each child octant o it streams the rows
+// (children's multipoles, or the parents' locals) and the operator T_o through shared memory in
+// K slices of 32, 6 x 4 outputs per thread. Operator elements are loaded once per tile instead of
+// once per parent. K is limited to the triangle each translation needs: an output of degree l
+// takes inputs of degree <= l (M2M) or >= l (L2L).
+//   M2M: parent = sum_o T_o child_o          (one writer per parent: stored)
+//   L2L: child_o += T_o parent               (one writer per child: load-add-store)
+// ====================================================================================
+constexpr int TG_P = 32, TG_ROWS = 96, TG_N = 64, TG_K = 32;
+
+__device__ __forceinline__ void load4(const float* p, float* v)
+{
+   const float4 x = *reinterpret_cast<const float4*>(p);
+   v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void load4(const double* p, double* v)
+{
+   const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
+   v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
+
+__device__ __forceinline__ int degreeOf(int k)
+{
+   int l = int(sqrtf(float(k)));
+   while(l * l > k) l--;
+   while((l + 1) * (l + 1) <= k) l++;
+   return l;
+}
+
+template <class T, bool UP>
+__global__ void __launch_bounds__(256, 2) kTranslateLevel(Tree t, const int* __restrict__ parList, int pBeg, int pEnd,
+                                                          int p, int Lp, const T* __restrict__ opw, T* __restrict__ X)
+{
+   __shared__ __align__(16) T As[TG_K][TG_ROWS + 1];
+   __shared__ __align__(16) T Bs[TG_K][TG_N];
+   __shared__ int childOf[TG_P][8];
+   __shared__ int parentOf[TG_P];
+   const int tid = threadIdx.x;
+   const int L = nharm(p);
+   const int pt0 = pBeg + blockIdx.x * TG_P;
+   const int n0 = blockIdx.y * TG_N;
+   if(tid < TG_P)
+   {
+      const int par = pt0 + tid < pEnd ? parList[pt0 + tid] : -1;
+      parentOf[tid] = par;
+      for(int o = 0; o < 8; o++) childOf[tid][o] = -1;
+      if(par >= 0)
+      {
+         const int c0 = t.child0[par], nc = t.nchild[par];
+         for(int c = 0; c < nc; c++)
+         {
+            const int ch = c0 + c;
+            // M2M needs children with sources, L2L children with targets
+            const bool use = UP ? t.s1[ch] > t.s0[ch] : t.t1[ch] > t.t0[ch];
+            if(use) childOf[tid][int(t.key[ch] & 7)] = ch;
+         }
+      }
+   }
+   __syncthreads();
+   const int lLo = degreeOf(min(n0, L - 1)), lHi = degreeOf(min(n0 + TG_N - 1, L - 1));
+   const int kLo = UP ? 0 : lLo * lLo;
+   const int kHi = UP ? (lHi + 1) * (lHi + 1) : L;
+   const int tr = tid >> 4, tc = tid & 15;
+   T acc[6][4];
+#pragma unroll
+   for(int i = 0; i < 6; i++)
+#pragma unroll
+      for(int j = 0; j < 4; j++) acc[i][j] = T(0);
+   // steps (octant o, K slice) in order; each step's rows and operator slice are loaded into
+   // registers one step ahead, so the global loads overlap the previous step's arithmetic.
+   // Element q of a thread: row (tid / 32) + 8 q at K offset tid % 32 (k fastest across a warp:
+   // coalesced row reads), and operator row (tid / 64) + 4 q at column tid % 64.
+   const int nK = (kHi - kLo + TG_K - 1) / TG_K;
+   const int nSteps = 8 * nK;
+   constexpr int QA = TG_K * TG_ROWS / 256, QB = TG_K * TG_N / 256;
+   T ra[QA], rb[QB];
+   const int aK = tid & 31, aR = tid >> 5;
+   const int bN = tid & 63, bK = tid >> 6;
+   auto load = [&](int step) {
+      const int o = step / nK, k0 = kLo + (step % nK) * TG_K;
+      const T* op = opw + int64_t(o) * L * Lp + n0 + bN;
+      const bool aIn = k0 + aK < kHi;
+#pragma unroll
+      for(int q = 0; q < QA; q++)
+      {
+         const int r = aR + 8 * q;
+         const int i = r / 3, c = r - 3 * i;
+         const int src = UP ? childOf[i][o] : parentOf[i];
+         ra[q] = (src >= 0 && aIn) ? X[(int64_t(src) * 3 + c) * Lp + k0 + aK] : T(0);
+      }
+      const bool bIn = n0 + bN < Lp;
+#pragma unroll
+      for(int q = 0; q < QB; q++)
+      {
+         const int k = k0 + bK + 4 * q;
+         rb[q] = (k < kHi && bIn) ? op[int64_t(k) * Lp] : T(0);
+      }
+   };
+   if(nSteps > 0) load(0);
+   for(int step = 0; step < nSteps; step++)
+   {
+      __syncthreads();
+#pragma unroll
+      for(int q = 0; q < QA; q++) As[aK][aR + 8 * q] = ra[q];
+#pragma unroll
+      for(int q = 0; q < QB; q++) Bs[bK + 4 * q][bN] = rb[q];
+      __syncthreads();
+      if(step + 1 < nSteps) load(step + 1);
+#pragma unroll 8
+      for(int kk = 0; kk < TG_K; kk++)
+      {
+         T a[6], b[4];
+#pragma unroll
+         for(int i = 0; i < 6; i++) a[i] = As[kk][tr * 6 + i];
+         load4(&Bs[kk][tc * 4], b);
+#pragma unroll
+         for(int i = 0; i < 6; i++)
+#pragma unroll
+            for(int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
+      }
+      if(!UP && step % nK == nK - 1)
+      {
+         // this octant's children: child += acc, then a fresh accumulator for the next octant
+         const int o = step / nK;
+#pragma unroll
+         for(int i = 0; i < 6; i++)
+         {
+            const int r = tr * 6 + i, pi = r / 3, c = r % 3;
+            const int ch = childOf[pi][o];
+            if(ch >= 0)
+               for(int j = 0; j < 4; j++)
+               {
+                  const int n = n0 + tc * 4 + j;
+                  if(n < Lp) X[(int64_t(ch) * 3 + c) * Lp + n] += acc[i][j];
+               }
+#pragma unroll
+            for(int j = 0; j < 4; j++) acc[i][j] = T(0);
+         }
+      }
+   }
+   if(UP)
+   {
+#pragma unroll
+      for(int i = 0; i < 6; i++)
+      {
+         const int r = tr * 6 + i, pi = r / 3, c = r % 3;
+         const int par = parentOf[pi];
+         if(par < 0 || t.s1[par] == t.s0[par]) continue;
+         for(int j = 0; j < 4; j++)
+         {
+            const int n = n0 + tc * 4 + j;
+            if(n < Lp) X[(int64_t(par) * 3 + c) * Lp + n] = acc[i][j];
+         }
+      }
+   }
+}
+
+// ====================================================================================
 // Geometry helpers
 // ====================================================================================
 __device__ __forceinline__ void nodeCenter(const RootBox& rb, int level, int ix, int iy, int iz, double c[3], double& h)
@@ -303,86 +462,11 @@ __global__ void __launch_bounds__(CH) kP2M(Tree t, const RootBox* __restrict__ r
 // translated multipoles of its children. Output coefficient k of degree l only needs input
 // coefficients j < (l+1)^2.
 // ====================================================================================
-template <class T>
-__global__ void __launch_bounds__(256) kM2M(Tree t, int a, int b, int p, int Lp, const T* __restrict__ opw,
-                                            T* __restrict__ M)
-{
-   extern __shared__ unsigned char smraw[];
-   T* Ms = (T*)smraw;  // [8][3][Lp]
-   const int node = a + blockIdx.x;
-   if(node >= b) return;
-   const int nc = t.nchild[node];
-   if(nc == 0 || t.s1[node] == t.s0[node]) return;
-   const int L = nharm(p);
-   const int c0 = t.child0[node];
-   for(int e = threadIdx.x; e < nc * 3 * Lp; e += blockDim.x) Ms[e] = M[int64_t(c0) * 3 * Lp + e];
-   __syncthreads();
-   for(int k = threadIdx.x; k < Lp; k += blockDim.x)
-   {
-      T acc[3] = {T(0), T(0), T(0)};
-      if(k < L)
-      {
-         int l = int(sqrtf(float(k)));
-         while(l * l > k) l--;
-         while((l + 1) * (l + 1) <= k) l++;
-         const int jmax = (l + 1) * (l + 1);
-         for(int c = 0; c < nc; c++)
-         {
-            const int ch = c0 + c;
-            if(t.s1[ch] == t.s0[ch]) continue;
-            const int oct = int(t.key[ch] & 7);
-            const T* op = opw + int64_t(oct) * L * Lp + k;
-            const T* mc = Ms + c * 3 * Lp;
-            for(int j = 0; j < jmax; j++)
-            {
-               const T o = op[int64_t(j) * Lp];
-               acc[0] += o * mc[j];
-               acc[1] += o * mc[Lp + j];
-               acc[2] += o * mc[2 * Lp + j];
-            }
-         }
-      }
-      T* out = M + int64_t(node) * 3 * Lp;
-      out[k] = acc[0]; out[Lp + k] = acc[1]; out[2 * Lp + k] = acc[2];
-   }
-}
 
 // ====================================================================================
 // L2L, one level: one block per node of the level holding targets; adds the parent's
 // translated local expansion. Output coefficient of degree l needs inputs of degree >= l.
 // ====================================================================================
-template <class T>
-__global__ void __launch_bounds__(256) kL2L(Tree t, int a, int b, int p, int Lp, const T* __restrict__ opw,
-                                            T* __restrict__ Lc)
-{
-   extern __shared__ unsigned char smraw[];
-   T* Ps = (T*)smraw;  // [3][Lp]
-   const int node = a + blockIdx.x;
-   if(node >= b) return;
-   if(t.t1[node] == t.t0[node]) return;
-   const int L = nharm(p);
-   const int par = t.parent[node];
-   for(int e = threadIdx.x; e < 3 * Lp; e += blockDim.x) Ps[e] = Lc[int64_t(par) * 3 * Lp + e];
-   __syncthreads();
-   const int oct = int(t.key[node] & 7);
-   T* out = Lc + int64_t(node) * 3 * Lp;
-   for(int k = threadIdx.x; k < L; k += blockDim.x)
-   {
-      int l = int(sqrtf(float(k)));
-      while(l * l > k) l--;
-      while((l + 1) * (l + 1) <= k) l++;
-      T acc[3] = {T(0), T(0), T(0)};
-      const T* op = opw + int64_t(oct) * L * Lp + k;
-      for(int j = l * l; j < L; j++)
-      {
-         const T o = op[int64_t(j) * Lp];
-         acc[0] += o * Ps[j];
-         acc[1] += o * Ps[Lp + j];
-         acc[2] += o * Ps[2 * Lp + j];
-      }
-      out[k] += acc[0]; out[Lp + k] += acc[1]; out[2 * Lp + k] += acc[2];
-   }
-}
 
 // ====================================================================================
 // M2L on the CUDA cores. A block owns TT consecutive target nodes (3 TT rows: node x
@@ -718,13 +802,14 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
                                         (T*)P.mult.ptr);
    FMM_TRY(launched(P, "kP2M", st));
    FMM_CHECK_LAUNCH();
-   size_t shm2 = sizeof(T) * 8 * 3 * Lp;
-   FMM_CUDA(cudaFuncSetAttribute(kM2M<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
+   const int nCol = (Lp + TG_N - 1) / TG_N;
    for(int level = P.tree.nLevels - 2; level >= 0; level--)
    {
-      int a = P.tree.levelStart[level], b = P.tree.levelStart[level + 1];
-      kM2M<T><<<b - a, 256, shm2, st>>>(P.tree, a, b, P.p, Lp, (const T*)P.opM2Mw.ptr, (T*)P.mult.ptr);
-      FMM_TRY(launched(P, "kM2M", st));
+      const int a = P.parStart[level], b = P.parStart[level + 1];
+      if(b <= a) continue;
+      kTranslateLevel<T, true><<<dim3((b - a + TG_P - 1) / TG_P, nCol), 256, 0, st>>>(
+         P.tree, (const int*)P.parList.ptr, a, b, P.p, Lp, (const T*)P.opM2Mw.ptr, (T*)P.mult.ptr);
+      FMM_TRY(launched(P, "kTranslateLevel<M2M>", st));
    }
    FMM_CHECK_LAUNCH();
    return FMM_OK;
@@ -756,12 +841,14 @@ fmm_status downwardT(Plan& P, cudaStream_t st)
    if(sizeof(T) == 4 && P.cfg.m2l_mode != FMM_M2L_SIMT) FMM_TRY(m2lTensorCore(P, st));
    else FMM_TRY(m2lSimt<T>(P, st));
    if(P.eventsMade && !P.capturing) cudaEventRecord(P.ev[3], st);
-   size_t shm = sizeof(T) * 3 * Lp;
-   for(int level = 1; level < P.tree.nLevels; level++)
+   const int nCol = (Lp + TG_N - 1) / TG_N;
+   for(int level = 0; level + 1 < P.tree.nLevels; level++)
    {
-      int a = P.tree.levelStart[level], b = P.tree.levelStart[level + 1];
-      kL2L<T><<<b - a, 256, shm, st>>>(P.tree, a, b, P.p, Lp, (const T*)P.opL2Lw.ptr, (T*)P.local.ptr);
-      FMM_TRY(launched(P, "kL2L", st));
+      const int a = P.parStart[level], b = P.parStart[level + 1];
+      if(b <= a) continue;
+      kTranslateLevel<T, false><<<dim3((b - a + TG_P - 1) / TG_P, nCol), 256, 0, st>>>(
+         P.tree, (const int*)P.parList.ptr, a, b, P.p, Lp, (const T*)P.opL2Lw.ptr, (T*)P.local.ptr);
+      FMM_TRY(launched(P, "kTranslateLevel<L2L>", st));
    }
    FMM_CHECK_LAUNCH();
    return FMM_OK;

@@ -436,6 +436,24 @@ __global__ void kM2LTargetKeys(Tree t, Lists L, int nNodes, int byCount, unsigne
    if(has) atomicAdd(count, 1);
 }
 
+// Nodes with children, compacted in node order (so each level's parents are contiguous), and the
+// compacted index where each level starts.
+__global__ void kParentFlags(Tree t, int nNodes, int* flags)
+{
+   int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if(i < nNodes) flags[i] = t.nchild[i] > 0 ? 1 : 0;
+}
+__global__ void kParentScatter(const int* __restrict__ flags, const int* __restrict__ pos, int nNodes, int* parList)
+{
+   int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if(i < nNodes && flags[i]) parList[pos[i]] = i;
+}
+__global__ void kParentLevelStarts(Tree t, const int* __restrict__ pos, int* out)
+{
+   int l = threadIdx.x;
+   if(l <= t.nLevels) out[l] = pos[t.levelStart[l]];
+}
+
 // ------------------------------------------------------------------------------ host driver
 template <class T>
 fmm_status buildTreeT(Plan& P, cudaStream_t st)
@@ -637,6 +655,30 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    FMM_CHECK_LAUNCH();
    P.nP2P = nP2P;
    P.nV = nV;
+   // parents per level for the M2M / L2L GEMMs
+   {
+      int* flags = (int*)P.lvlCnt.ptr;   // nn + 1 ints, free again once the direct lists are counted
+      FMM_TRY(P.lvlOff.reserve(sizeof(int) * (nn + 1)));
+      int* pos = (int*)P.lvlOff.ptr;
+      FMM_TRY(P.parList.reserve(sizeof(int) * std::max(nn, 1)));
+      kParentFlags<<<(nn + 255) / 256, 256, 0, st>>>(t, nn, flags);
+      FMM_TRY(launched(P, "kParentFlags", st));
+      FMM_CUDA(cudaMemsetAsync(flags + nn, 0, sizeof(int), st));
+      tmp = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tmp, flags, pos, nn + 1, st);
+      FMM_TRY(P.cubTmp.reserve(tmp));
+      tmp = P.cubTmp.bytes;
+      FMM_CUDA(cub::DeviceScan::ExclusiveSum(P.cubTmp.ptr, tmp, flags, pos, nn + 1, st));
+      kParentScatter<<<(nn + 255) / 256, 256, 0, st>>>(flags, pos, nn, (int*)P.parList.ptr);
+      FMM_TRY(launched(P, "kParentScatter", st));
+      FMM_TRY(P.scratch.reserve(sizeof(int) * (MAXLEVEL + 2)));
+      t.levelStart[nLevels] = nn;
+      kParentLevelStarts<<<1, 32, 0, st>>>(t, pos, (int*)P.scratch.ptr);
+      FMM_TRY(launched(P, "kParentLevelStarts", st));
+      P.parStart.assign(nLevels + 1, 0);
+      FMM_CUDA(cudaMemcpyAsync(P.parStart.data(), P.scratch.ptr, sizeof(int) * (nLevels + 1), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+   }
    // M2L targets grouped by octant
    {
       FMM_TRY(P.m2lTargets.reserve(2 * sizeof(int) * nn));
