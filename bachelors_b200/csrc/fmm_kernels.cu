@@ -396,65 +396,132 @@ __device__ __forceinline__ void nodeCenter(const RootBox& rb, int level, int ix,
 }
 
 // ====================================================================================
-// P2M: one block per leaf holding sources. Each thread writes the harmonics of one point
-// into a shared-memory row; then each thread reduces a set of coefficients over the rows.
+// P2M: one block of NT threads per leaf holding sources, one source point per thread. Each
+// thread runs the harmonic recurrence of its point as explicit state in registers (RegularIter,
+// the visit order of visitRegular). Every CV visits the block reduces the values of those
+// visits over its points through a small shared tile (the values of a visit are the same
+// coefficient for every thread, so the tile's columns are coefficients) and adds them to the
+// leaf's multipole, kept in shared memory until the end. Leaves with more than NT points take
+// their points NT at a time.
 // ====================================================================================
-template <class T, int CH>
-__global__ void __launch_bounds__(CH) kP2M(Tree t, const RootBox* __restrict__ rootp,
+template <class T>
+struct RegularIter
+{
+   T x, y, z, r2;
+   T dre, dim;       // S_m^m
+   T are, aim;       // S_l^m (the current visit)
+   T bre, bim;       // S_{l-1}^m
+   int l, m, p;
+   __device__ __forceinline__ void start(int p_, T x_, T y_, T z_)
+   {
+      p = p_; x = x_; y = y_; z = z_; r2 = x * x + y * y + z * z;
+      dre = T(1); dim = T(0); are = T(1); aim = T(0); bre = T(0); bim = T(0); l = 0; m = 0;
+   }
+   // moves to the next (l, m) of the visit order: l = m..p for m = 0..p
+   __device__ __forceinline__ void next()
+   {
+      if(l < p)
+      {
+         T cre, cim;
+         if(l == m) { cre = z * are; cim = z * aim; }
+         else
+         {
+            const T inv = T(1) / T((l - m + 1) * (l + m + 1));
+            const T a = T(2 * l + 1) * inv;
+            cre = a * z * are - inv * r2 * bre;
+            cim = a * z * aim - inv * r2 * bim;
+         }
+         bre = are; bim = aim; are = cre; aim = cim;
+         l++;
+      }
+      else
+      {
+         m++;
+         const T s = T(1) / T(2 * m);
+         const T nre = (dre * x - dim * y) * s;
+         const T nim = (dre * y + dim * x) * s;
+         dre = nre; dim = nim;
+         are = dre; aim = dim; bre = T(0); bim = T(0);
+         l = m;
+      }
+   }
+};
+
+template <class T, int NT, int CV>
+__global__ void __launch_bounds__(NT) kP2M(Tree t, const RootBox* __restrict__ rootp,
                                            const typename Vec4<T>::type* __restrict__ pos,
                                            const typename Vec4<T>::type* __restrict__ q, int p, int Lp, T* __restrict__ M)
 {
+   __shared__ T R[NT][2 * CV + 1];   // the chunk's real-basis values per point (odd stride)
+   __shared__ T Q[NT][3];            // w J per point
+   __shared__ int kOf[2 * CV];       // coefficient index of each column of R (-1: none)
    extern __shared__ unsigned char smraw[];
+   T* Macc = (T*)smraw;              // [3][Lp] the leaf's multipole
    const int node = blockIdx.x;
    if(t.nchild[node] != 0) return;
    const int s0 = t.s0[node], s1 = t.s1[node];
+   if(s1 == s0) return;
+   const int tid = threadIdx.x;
    const int L = nharm(p);
-   const int LS = L | 1;  // odd row stride: conflict-free column access
-   T* R = (T*)smraw;                   // [CH][LS]
-   T* Q = R + CH * LS;                 // [CH][3]
+   const int nVisits = (p + 1) * (p + 2) / 2;
+   for(int e = tid; e < 3 * Lp; e += NT) Macc[e] = T(0);
    const RootBox rb = rootp[rootOf(t, node)];
    double c[3], h;
    nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], c, h);
    const double ih = 1.0 / h;
-   constexpr int SLOTS = (nharm(MAXORDER) + CH - 1) / CH;
-   T acc[SLOTS][3];
-#pragma unroll
-   for(int s = 0; s < SLOTS; s++) acc[s][0] = acc[s][1] = acc[s][2] = T(0);
-   for(int base = s0; base < s1; base += CH)
+   const T sq2 = T(1.4142135623730950488);
+   for(int base = s0; base < s1; base += NT)
    {
-      const int cnt = min(CH, s1 - base);
-      if(threadIdx.x < cnt)
+      const int cnt = min(NT, s1 - base);
+      RegularIter<T> it;
+      T qx = T(0), qy = T(0), qz = T(0);
+      if(tid < cnt)
       {
-         const auto x = pos[base + threadIdx.x];
-         const auto w = q[base + threadIdx.x];
-         T ux = T((double(x.x) - c[0]) * ih), uy = T((double(x.y) - c[1]) * ih), uz = T((double(x.z) - c[2]) * ih);
-         realRegular<T>(p, ux, uy, uz, R + threadIdx.x * LS);
-         Q[3 * threadIdx.x] = w.x; Q[3 * threadIdx.x + 1] = w.y; Q[3 * threadIdx.x + 2] = w.z;
+         const auto xp = pos[base + tid];
+         const auto w = q[base + tid];
+         it.start(p, T((double(xp.x) - c[0]) * ih), T((double(xp.y) - c[1]) * ih), T((double(xp.z) - c[2]) * ih));
+         qx = w.x; qy = w.y; qz = w.z;
       }
-      __syncthreads();
-#pragma unroll
-      for(int s = 0; s < SLOTS; s++)
+      else
+         it.start(p, T(0), T(0), T(0));
+      Q[tid][0] = qx; Q[tid][1] = qy; Q[tid][2] = qz;
+      int vl = 0, vm = 0;   // (l, m) of the chunk's first visit, tracked uniformly by every thread
+      for(int v0 = 0; v0 < nVisits; v0 += CV)
       {
-         int k = threadIdx.x + s * CH;
-         if(k < L)
-            for(int i = 0; i < cnt; i++)
+         const int nv = min(CV, nVisits - v0);
+         // this thread's values for visits v0 .. v0 + nv - 1, and the columns' coefficients
+         int cl = vl, cm = vm;
+         for(int j = 0; j < nv; j++)
+         {
+            const T sgn = (it.l & 1) ? T(-1) : T(1);
+            if(it.m == 0) { R[tid][2 * j] = sgn * it.are; R[tid][2 * j + 1] = T(0); }
+            else { R[tid][2 * j] = sgn * sq2 * it.are; R[tid][2 * j + 1] = sgn * sq2 * it.aim; }
+            if(tid == 0)
             {
-               T r = R[i * LS + k];
-               acc[s][0] += Q[3 * i] * r;
-               acc[s][1] += Q[3 * i + 1] * r;
-               acc[s][2] += Q[3 * i + 2] * r;
+               kOf[2 * j] = hidx(cl, cm);
+               kOf[2 * j + 1] = cm > 0 ? hidx(cl, -cm) : -1;
             }
+            if(v0 + j + 1 < nVisits) it.next();
+            if(cl < p) cl++;
+            else { cm++; cl = cm; }
+         }
+         vl = cl; vm = cm;
+         __syncthreads();
+         // reduce over the points: output (column, component) pairs split over the threads
+         for(int o = tid; o < 2 * nv * 3; o += NT)
+         {
+            const int col = o / 3, comp = o - 3 * col;
+            const int k = kOf[col];
+            if(k < 0) continue;
+            T acc = T(0);
+            for(int i = 0; i < cnt; i++) acc += Q[i][comp] * R[i][col];
+            Macc[comp * Lp + k] += acc;
+         }
+         __syncthreads();
       }
-      __syncthreads();
    }
    T* out = M + int64_t(node) * 3 * Lp;
-#pragma unroll
-   for(int s = 0; s < SLOTS; s++)
-   {
-      int k = threadIdx.x + s * CH;
-      if(k < Lp)
-         for(int d = 0; d < 3; d++) out[d * Lp + k] = k < L ? acc[s][d] : T(0);
-   }
+   for(int e = tid; e < 3 * Lp; e += NT) out[e] = (e % Lp) < L ? Macc[e] : T(0);
 }
 
 // ====================================================================================
@@ -791,15 +858,14 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
 {
    FMM_TRY(buildOperators(P, st));
    const int64_t N = P.tree.nNodes;
-   const int L = P.L, Lp = P.Lp;
+   const int Lp = P.Lp;
    FMM_TRY(P.mult.reserve(sizeof(T) * N * 3 * Lp));
    FMM_CUDA(cudaMemsetAsync(P.mult.ptr, 0, sizeof(T) * N * 3 * Lp, st));
    typedef typename Vec4<T>::type V4;
-   constexpr int CH = sizeof(T) == 4 ? 64 : 32;
-   size_t shm = sizeof(T) * (CH * (L | 1) + 3 * CH);
-   FMM_CUDA(cudaFuncSetAttribute(kP2M<T, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-   kP2M<T, CH><<<int(N), CH, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
-                                        (T*)P.mult.ptr);
+   constexpr int NT = 64, CV = 16;
+   const size_t shm = sizeof(T) * 3 * Lp;
+   kP2M<T, NT, CV><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
+                                           (T*)P.mult.ptr);
    FMM_TRY(launched(P, "kP2M", st));
    FMM_CHECK_LAUNCH();
    const int nCol = (Lp + TG_N - 1) / TG_N;
