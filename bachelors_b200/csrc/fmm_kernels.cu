@@ -18,6 +18,8 @@
 
 #include <cuda_bf16.h>
 
+#include <cub/cub.cuh>
+
 #include "fmm_internal.cuh"
 
 namespace fmm {
@@ -667,7 +669,13 @@ __device__ inline T gradCoeff(const T* Lv, int j, int lp, int mu)
    return h * coefAt(Lv, l, 1 - mu) + h * coefAt(Lv, l, -mu - 1);
 }
 
-template <class T, int NT>
+// L2P and the direct near field: one block of NT threads per target leaf. The far field comes from
+// the leaf's local expansion (analytic curl, one target per thread). The near field packs the
+// points of the leaf's direct-interaction source nodes into shared tiles of TS points; when the
+// leaf has fewer targets than threads, the G = NT / targets thread groups each take every G-th
+// source of a tile and their partial sums are added in a fixed order at the end. Each thread
+// sums one tile in T and the tile sums in FP64, so no single-precision chain is longer than a tile.
+template <class T, int NT, int TS, int NE>
 __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict__ rootp, int p, int Lp,
                                                const T* __restrict__ Lc,
                                                const typename Vec4<T>::type* __restrict__ tpos,
@@ -681,17 +689,23 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
    extern __shared__ __align__(32) unsigned char smraw[];
    const int node = blockIdx.x;
    if(t.nchild[node] != 0 || t.t1[node] == t.t0[node]) return;
+   const int tid = threadIdx.x;
    const int L = nharm(p);
    const int Lb = nharm(p - 1);
    T* Ls = (T*)smraw;          // [3][L] local
    T* Cs = Ls + 3 * L;         // [3][Lb] curl expansion
    // source tiles start on a 32-byte boundary after the two coefficient arrays
    const size_t coefBytes = (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31);
-   V4* Sp = (V4*)(smraw + coefBytes);  // [NT] source tile positions
-   V4* Sq = Sp + NT;           // [NT] source tile strengths
-   for(int e = threadIdx.x; e < 3 * L; e += NT) Ls[e] = Lc[int64_t(node) * 3 * Lp + (e / L) * Lp + e % L];
+   V4* Sp = (V4*)(smraw + coefBytes);  // [TS] source positions
+   V4* Sq = Sp + TS;                   // [TS] source strengths w J
+   double* red = (double*)(Sq + TS);   // [6][NT] group partial sums
+   typedef cub::BlockScan<int, NT> ScanT;
+   __shared__ typename ScanT::TempStorage scanTmp;
+   __shared__ int ePre[NE + 1];        // prefix sums of the batch's source counts
+   __shared__ int eSrc[NE];            // first sorted source of each batch entry
+   for(int e = tid; e < 3 * L; e += NT) Ls[e] = Lc[int64_t(node) * 3 * Lp + (e / L) * Lp + e % L];
    __syncthreads();
-   for(int e = threadIdx.x; e < 3 * Lb; e += NT)
+   for(int e = tid; e < 3 * Lb; e += NT)
    {
       const int c = e / Lb, k = e % Lb;
       int lp = int(sqrtf(float(k)));
@@ -710,17 +724,21 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
    const T ih = T(1.0 / h), ih2 = T(1.0 / (h * h));
    const int t0 = t.t0[node], t1 = t.t1[node];
    const int e0 = p2pOff[node], e1 = p2pOff[node + 1];
+   const bool wantA = (want & 2) != 0;
    for(int base = t0; base < t1; base += NT)
    {
-      const int ti = base + threadIdx.x;
-      const bool active = ti < t1;
-      V4 x = active ? tpos[ti] : V4{T(0), T(0), T(0), T(0)};
-      T B[3] = {T(0), T(0), T(0)}, A[3] = {T(0), T(0), T(0)};
-      if(active)
+      const int nt = min(NT, t1 - base);     // targets in this pass
+      const int G = NT / nt;                 // thread groups sharing a tile's sources
+      const int tt = tid % nt, g = tid / nt;
+      const bool inGroup = g < G;
+      const int ti = base + tt;
+      V4 x = inGroup ? tpos[ti] : V4{T(0), T(0), T(0), T(0)};
+      double Bd[3] = {0, 0, 0}, Ad[3] = {0, 0, 0};
+      if(inGroup && g == 0)
       {
+         T B[3] = {T(0), T(0), T(0)}, A[3] = {T(0), T(0), T(0)};
          const T ux = T((double(x.x) - c[0]) / h), uy = T((double(x.y) - c[1]) / h), uz = T((double(x.z) - c[2]) / h);
          const T sq2 = T(1.4142135623730950488);
-         const bool wantA = (want & 2) != 0;
          visitRegular<T>(p, ux, uy, uz, [&](int l, int m, T re, T im) {
             const T s = (l & 1) ? T(-1) : T(1);
             T r0, r1;
@@ -745,48 +763,97 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
                }
             }
          });
-         for(int d = 0; d < 3; d++) { B[d] *= ih2; A[d] *= ih; }
+         for(int d = 0; d < 3; d++) { Bd[d] = double(B[d] * ih2); Ad[d] = double(A[d] * ih); }
       }
-      // direct near field: each source tile is summed in T, the tile sums in FP64, so no
-      // single-precision chain is longer than one tile
-      double Bs[3] = {double(B[0]), double(B[1]), double(B[2])}, As[3] = {double(A[0]), double(A[1]), double(A[2])};
-      for(int e = e0; e < e1; e++)
-      {
-         const int S = p2pList[e];
-         const int a0 = t.s0[S], a1 = t.s1[S];
-         for(int sb = a0; sb < a1; sb += NT)
+      // near field over packed tiles of the direct-list source nodes
+      auto tileSum = [&](int n) {
+         if(!inGroup) return;
+         T pb[3] = {T(0), T(0), T(0)}, pa[3] = {T(0), T(0), T(0)};
+         for(int i = g; i < n; i += G)
          {
-            const int cnt = min(NT, a1 - sb);
-            __syncthreads();
-            if(threadIdx.x < cnt) { Sp[threadIdx.x] = spos[sb + threadIdx.x]; Sq[threadIdx.x] = sq[sb + threadIdx.x]; }
-            __syncthreads();
-            if(active)
+            const V4 y = Sp[i], w = Sq[i];
+            const T dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+            const T r2 = dx * dx + dy * dy + dz * dz;
+            if(r2 == T(0)) continue;
+            T ri;
+            if constexpr(sizeof(T) == 4) ri = rsqrtf(r2);
+            else ri = rsqrt(r2);
+            const T ri3 = ri * ri * ri;
+            pb[0] += (w.y * dz - w.z * dy) * ri3;
+            pb[1] += (w.z * dx - w.x * dz) * ri3;
+            pb[2] += (w.x * dy - w.y * dx) * ri3;
+            if(wantA) { pa[0] += w.x * ri; pa[1] += w.y * ri; pa[2] += w.z * ri; }
+         }
+         for(int d = 0; d < 3; d++) { Bd[d] += double(pb[d]); Ad[d] += double(pa[d]); }
+      };
+      // the list in batches of NE entries: their point ranges are read together into shared memory
+      // and prefix-summed, so every tile position finds its source by a shared-memory search and
+      // all of a tile's loads are independent
+      for(int eb = e0; eb < e1; eb += NE)
+      {
+         const int ne = min(NE, e1 - eb);
+         int sz[NE / NT];
+#pragma unroll
+         for(int r = 0; r < NE / NT; r++)
+         {
+            const int k = tid * (NE / NT) + r;
+            int a = 0, n = 0;
+            if(k < ne)
             {
-               T pb[3] = {T(0), T(0), T(0)}, pa[3] = {T(0), T(0), T(0)};
-               for(int i = 0; i < cnt; i++)
-               {
-                  const V4 y = Sp[i], w = Sq[i];
-                  const T dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
-                  const T r2 = dx * dx + dy * dy + dz * dz;
-                  if(r2 == T(0)) continue;
-                  T ri;
-                  if constexpr(sizeof(T) == 4) ri = rsqrtf(r2);
-                  else ri = rsqrt(r2);
-                  const T ri3 = ri * ri * ri;
-                  pb[0] += (w.y * dz - w.z * dy) * ri3;
-                  pb[1] += (w.z * dx - w.x * dz) * ri3;
-                  pb[2] += (w.x * dy - w.y * dx) * ri3;
-                  pa[0] += w.x * ri; pa[1] += w.y * ri; pa[2] += w.z * ri;
-               }
-               for(int d = 0; d < 3; d++) { Bs[d] += double(pb[d]); As[d] += double(pa[d]); }
+               const int S = p2pList[eb + k];
+               a = t.s0[S];
+               n = t.s1[S] - a;
             }
+            if(k < NE) eSrc[k] = a;
+            sz[r] = n;
+         }
+         int total;
+         ScanT(scanTmp).ExclusiveSum(sz, sz, total);
+#pragma unroll
+         for(int r = 0; r < NE / NT; r++) ePre[tid * (NE / NT) + r] = sz[r];
+         if(tid == 0) ePre[NE] = total;
+         __syncthreads();
+         for(int pos = 0; pos < total; pos += TS)
+         {
+            const int n = min(TS, total - pos);
+            for(int j = tid; j < n; j += NT)
+            {
+               const int qpos = pos + j;
+               int lo = 0, hi = ne;  // last entry with ePre <= qpos
+               while(hi - lo > 1)
+               {
+                  const int mid = (lo + hi) >> 1;
+                  if(ePre[mid] <= qpos) lo = mid;
+                  else hi = mid;
+               }
+               const int src = eSrc[lo] + (qpos - ePre[lo]);
+               Sp[j] = spos[src];
+               Sq[j] = sq[src];
+            }
+            __syncthreads();
+            tileSum(n);
+            __syncthreads();
          }
       }
-      if(active)
+      // add the groups' partial sums in group order
+      if(G > 1)
+      {
+         for(int d = 0; d < 3; d++) { red[d * NT + tid] = Bd[d]; red[(3 + d) * NT + tid] = Ad[d]; }
+         __syncthreads();
+         if(g == 0)
+            for(int gg = 1; gg < G; gg++)
+               for(int d = 0; d < 3; d++)
+               {
+                  Bd[d] += red[d * NT + gg * nt + tt];
+                  Ad[d] += red[(3 + d) * NT + gg * nt + tt];
+               }
+         __syncthreads();
+      }
+      if(g == 0)
       {
          const int o = tOrder[ti];
-         if(want & 1) for(int d = 0; d < 3; d++) outB[3 * int64_t(o) + d] = T(Bs[d] * double(scaleB));
-         if(want & 2) for(int d = 0; d < 3; d++) outA[3 * int64_t(o) + d] = T(As[d] * double(scaleA));
+         if(want & 1) for(int d = 0; d < 3; d++) outB[3 * int64_t(o) + d] = T(Bd[d] * double(scaleB));
+         if(want & 2) for(int d = 0; d < 3; d++) outA[3 * int64_t(o) + d] = T(Ad[d] * double(scaleA));
       }
    }
 }
@@ -926,11 +993,11 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
    typedef typename Vec4<T>::type V4;
    const int64_t N = P.tree.nNodes;
    const int L = P.L, Lb = nharm(P.p - 1);
-   constexpr int NT = 64;
-   size_t shm = ((sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31)) + 2 * sizeof(V4) * NT;
-   FMM_CUDA(cudaFuncSetAttribute(kL2PNear<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+   constexpr int NT = 64, TS = 256, NE = 128;
+   size_t shm = ((sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31)) + 2 * sizeof(V4) * TS + sizeof(double) * 6 * NT;
+   FMM_CUDA(cudaFuncSetAttribute(kL2PNear<T, NT, TS, NE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
-   kL2PNear<T, NT><<<int(N), NT, shm, st>>>(P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr,
+   kL2PNear<T, NT, TS, NE><<<int(N), NT, shm, st>>>(P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr,
                                             (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, (const int*)P.p2pOff.ptr,
                                             (const int*)P.p2pList.ptr, (const int*)P.tIdx.ptr, scaleB, scaleA, want,
                                             (T*)P.outB.ptr, (T*)P.outA.ptr);
