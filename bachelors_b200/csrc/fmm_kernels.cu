@@ -675,7 +675,7 @@ __device__ inline T gradCoeff(const T* Lv, int j, int lp, int mu)
 // leaf has fewer targets than threads, the G = NT / targets thread groups each take every G-th
 // source of a tile and their partial sums are added in a fixed order at the end. Each thread
 // sums one tile in T and the tile sums in FP64, so no single-precision chain is longer than a tile.
-template <class T, int NT, int TS, int NE>
+template <class T, int NT, int TS, int NE, bool WANTA>
 __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict__ rootp, int p, int Lp,
                                                const T* __restrict__ Lc,
                                                const typename Vec4<T>::type* __restrict__ tpos,
@@ -724,7 +724,7 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
    const T ih = T(1.0 / h), ih2 = T(1.0 / (h * h));
    const int t0 = t.t0[node], t1 = t.t1[node];
    const int e0 = p2pOff[node], e1 = p2pOff[node + 1];
-   const bool wantA = (want & 2) != 0;
+   constexpr bool wantA = WANTA;
    for(int base = t0; base < t1; base += NT)
    {
       const int nt = min(NT, t1 - base);     // targets in this pass
@@ -769,15 +769,16 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
       auto tileSum = [&](int n) {
          if(!inGroup) return;
          T pb[3] = {T(0), T(0), T(0)}, pa[3] = {T(0), T(0), T(0)};
+#pragma unroll 4
          for(int i = g; i < n; i += G)
          {
             const V4 y = Sp[i], w = Sq[i];
             const T dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
             const T r2 = dx * dx + dy * dy + dz * dz;
-            if(r2 == T(0)) continue;
             T ri;
             if constexpr(sizeof(T) == 4) ri = rsqrtf(r2);
             else ri = rsqrt(r2);
+            ri = r2 > T(0) ? ri : T(0);   // coincident pair (the target itself): no contribution
             const T ri3 = ri * ri * ri;
             pb[0] += (w.y * dz - w.z * dy) * ri3;
             pb[1] += (w.z * dx - w.x * dz) * ri3;
@@ -995,12 +996,17 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
    const int L = P.L, Lb = nharm(P.p - 1);
    constexpr int NT = 64, TS = 256, NE = 128;
    size_t shm = ((sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31)) + 2 * sizeof(V4) * TS + sizeof(double) * 6 * NT;
-   FMM_CUDA(cudaFuncSetAttribute(kL2PNear<T, NT, TS, NE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
-   kL2PNear<T, NT, TS, NE><<<int(N), NT, shm, st>>>(P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr,
-                                            (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, (const int*)P.p2pOff.ptr,
-                                            (const int*)P.p2pList.ptr, (const int*)P.tIdx.ptr, scaleB, scaleA, want,
-                                            (T*)P.outB.ptr, (T*)P.outA.ptr);
+   auto run = [&](auto kernel) -> fmm_status {
+      FMM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+      kernel<<<int(N), NT, shm, st>>>(P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr,
+                                      (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, (const int*)P.p2pOff.ptr,
+                                      (const int*)P.p2pList.ptr, (const int*)P.tIdx.ptr, scaleB, scaleA, want,
+                                      (T*)P.outB.ptr, (T*)P.outA.ptr);
+      return FMM_OK;
+   };
+   if(want & 2) FMM_TRY(run(kL2PNear<T, NT, TS, NE, true>));
+   else FMM_TRY(run(kL2PNear<T, NT, TS, NE, false>));
    FMM_TRY(launched(P, "kL2PNear", st));
    FMM_CHECK_LAUNCH();
    return FMM_OK;
