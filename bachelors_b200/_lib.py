@@ -37,6 +37,7 @@ class FmmConfig(ctypes.Structure):
         ("device", ctypes.c_int),
         ("root_center", ctypes.c_double * 3),
         ("root_half_width", ctypes.c_double),
+        ("m2l_tc_degree_cutoff", ctypes.c_int),
     ]
 
 

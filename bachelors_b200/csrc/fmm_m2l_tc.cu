@@ -253,6 +253,14 @@ __global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int
 // The multipoles split into NP bf16 pieces, once per solve: Mbf[node][comp][piece][Lp], each
 // piece the round-to-nearest of the remaining FP32 residual (exact: every piece removes the
 // leading bits of the remainder).
+// Output columns each 16-wide K step of the M2L needs: with the degree cutoff l + lambda <= P, the
+// inputs of a K step (degrees >= lambda_min) only reach outputs of degree <= P - lambda_min,
+// which are the first (P - lambda_min + 1)^2 columns (rounded up to 16). Step 0 is always full.
+struct M2LCols
+{
+   int n[32];
+};
+
 template <int NP>
 __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int Lp, __nv_bfloat16* __restrict__ Mbf)
 {
@@ -276,7 +284,7 @@ template <int NP, int KCW>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int L, int Lp, int nChunks,
        const uint8_t* __restrict__ img, const __nv_bfloat16* __restrict__ Mbf, float* __restrict__ Lc, int drainEvery,
-       int nStages, int drainMode, int nFirst, unsigned long long* counters, int* err)
+       int nStages, int drainMode, const M2LCols cols, unsigned long long* counters, int* err)
 {
    using namespace tc;
    using Lay = Layout<KCW>;
@@ -303,6 +311,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 136); // 10 words: offsets present in the tile
    int* itemOffset = reinterpret_cast<int*>(ctrl + 192);        // compacted present offsets [316] + count
    int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
+   int* colTab = tileNode + 64;                                 // output columns per K step [32]
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
@@ -313,6 +322,11 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
 
    if(tid < 10) present[tid] = 0;
    if(tid < TT) tileNode[tid] = tid < nTile ? targets[first + tid] : -1;
+   if(tid == 0)
+   {
+#pragma unroll
+      for(int g = 0; g < 32; g++) colTab[g] = cols.n[g];
+   }
    if(tid == 0)
    {
       *abortFlag = 0;
@@ -365,37 +379,47 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    {
       if(lane == 0)
       {
-         // the N output columns in one MMA (N <= 256) or two: nFirst + (N - nFirst), both multiples of 16
-         const int nA = nFirst, nB = N - nFirst;
-         const uint32_t idA = instrDescBf16(ROWS, nA);
-         const uint32_t idB = nB > 0 ? instrDescBf16(ROWS, nB) : 0u;
          bool firstMma = true;
          int drains = 0;
          for(int it = 0; it < nItems; it++)
          {
             const int s = it % NS;
+            // this chunk's output widths per K step, read before the wait
+            int nColK[KCH / 16];
+#pragma unroll
+            for(int ks = 0; ks < KCH / 16; ks++) nColK[ks] = colTab[(it % nChunks) * (KCH / 16) + ks];
             if(!mbarWait(fullBar0 + 8 * s, (it / NS) & 1, err, abortFlag)) break;
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
             const uint32_t aSt = st, bSt = st + NP * aBytes;
-            // K steps of 16 that reach a coefficient < L (the last chunk is partly padding)
-            const int cItem = nChunks - 1 - it % nChunks;
+            // K steps of 16 that reach a coefficient < L (the last chunk is partly padding); chunks run
+            // in increasing K, so an accumulation always starts with a full-width MMA
+            const int cItem = it % nChunks;
             const int kSteps = min(KCH / 16, (L - cItem * KCH + 15) / 16);
+            // descriptors of the stage's pieces; an MMA's operand is the piece's descriptor plus its
+            // byte offset / 16 (the start-address field, bits 0-13, holds every address of the stage)
+            const uint64_t dA = smemDescT<KCW>(aSt), dB = smemDescT<KCW>(bSt);
 #pragma unroll
             for(int ks = 0; ks < KCH / 16; ks++)
             {
                if(ks >= kSteps) break;
                const uint32_t koff = ks * 32;
+               // this K step's output columns in one MMA (<= 256) or two (256 + the rest)
+               const int nCol = nColK[ks];
+               if(nCol == 0) break;
+               const int nA = min(nCol, 256), nB = nCol - nA;
+               const uint32_t idA = instrDescBf16(ROWS, nA);
+               const uint32_t idB = instrDescBf16(ROWS, nB > 0 ? nB : 16);
 #pragma unroll
                for(int pass = 0; pass < NPASS; pass++)
                {
                   const int pa = NP == 2 ? PA2[pass] : PA[pass];
                   const int pb = NP == 2 ? PB2[pass] : PB[pass];
-                  const uint32_t a = aSt + pa * aBytes + koff;
-                  const uint32_t b = bSt + pb * bBytes + koff;
+                  const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
+                  const uint64_t db = dB + ((pb * bBytes + koff) >> 4);
                   const uint32_t acc = firstMma ? 0u : 1u;
-                  mmaBf16(tmem, smemDescT<KCW>(a), smemDescT<KCW>(b), idA, acc);
-                  if(nB > 0) mmaBf16(tmem + nA, smemDescT<KCW>(a), smemDescT<KCW>(b + nA * Lay::RB), idB, acc);
+                  mmaBf16(tmem, da, db, idA, acc);
+                  if(nB > 0) mmaBf16(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
                   firstMma = false;
                }
             }
@@ -431,11 +455,14 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          {
             const int s = it % NS;
             if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag)) break;
-            const int o = itemOffset[it / nChunks], c = nChunks - 1 - it % nChunks;
+            const int o = itemOffset[it / nChunks], c = it % nChunks;
             const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
             const uint32_t dst = base + s * stageBytes + NP * aBytes;
-            mbarArriveExpectTx(fullBar0 + 8 * s, NP * bBytes);
-            bulkLoad(dst, src, NP * bBytes, fullBar0 + 8 * s);
+            // only the operator rows (output columns) this chunk's widest K step uses
+            const uint32_t rowBytes = uint32_t(colTab[c * (KCH / 16)]) * Lay::RB;
+            mbarArriveExpectTx(fullBar0 + 8 * s, NP * rowBytes);
+#pragma unroll
+            for(int j = 0; j < NP; j++) bulkLoad(dst + j * bBytes, src + j * bBytes, rowBytes, fullBar0 + 8 * s);
          }
       }
       __syncwarp();
@@ -457,6 +484,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       //                the accumulator leaves free (columns N .. 511); only the rest, and the final
       //                result, travel to global memory.
       const int nS = drainMode == 2 ? (min(N, 512 - N) & ~15) : 0;
+      const int cG = nS;                                         // first column kept in global memory
       const uint32_t tSum = tAcc + uint32_t(N);
       for(int d = 0; d < nDrains; d++)
       {
@@ -493,13 +521,13 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          // step's running sums are loaded before this step's accumulator values are read
          const bool rmw = drainMode != 0 && d > 0 && et >= 0;
          float4 nxt[4];
-         if(rmw && nS < N)
+         if(rmw && cG < N)
          {
-            const float4* o4 = reinterpret_cast<const float4*>(out + nS);
+            const float4* o4 = reinterpret_cast<const float4*>(out + cG);
 #pragma unroll
             for(int i = 0; i < 4; i++) nxt[i] = o4[i];
          }
-         for(int c0 = nS; c0 < N; c0 += 16)
+         for(int c0 = cG; c0 < N; c0 += 16)
          {
             uint32_t u[16];
             float4 old[4];
@@ -548,7 +576,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       for(int it = 0; it < nItems; it++)
       {
          const int s = it % NS;
-         const int oi = it / nChunks, c = nChunks - 1 - it % nChunks;
+         const int oi = it / nChunks, c = it % nChunks;
          if(it % nChunks == 0 && oi + 1 < nOff)
             srcNext = tgt >= 0 ? vtab[int64_t(tgt) * 316 + itemOffset[oi + 1]] : -1;
          if(pending >= 0)
@@ -614,7 +642,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(count <= 0) return FMM_OK;
    const int blocks = (count + tc::TT - 1) / tc::TT;
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 192 + 4 * (320 + 64);
+   const size_t fixed = 1024 + 192 + 4 * (320 + 64 + 32);
    const size_t budget = 232448;
    const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
@@ -626,7 +654,19 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    P.tcTiles = blocks;
    // first MMA's width: all of N up to 256, else 256 or (balanced) the multiple of 16 nearest N / 2;
    // the second starts on an 8-row boundary of the swizzled operator block either way
-   const int nFirst = Lp <= 256 ? Lp : (P.tcBalancedN ? ((Lp / 2 + 15) / 16) * 16 : 256);
+   // the degree cutoff: 0 -> p + 8, negative -> none (l + lambda <= 2p, the full operator)
+   const int cut = P.cfg.m2l_tc_degree_cutoff == 0 ? P.p + 8 : (P.cfg.m2l_tc_degree_cutoff < 0 ? 2 * P.p
+                                                                : std::max(P.cfg.m2l_tc_degree_cutoff, P.p));
+   M2LCols cols{};
+   for(int g = 0; g < nChunks * (Lay::KC / 16) && g < 32; g++)
+   {
+      const int k = 16 * g;
+      int lmin = 0;
+      while((lmin + 1) * (lmin + 1) <= k) lmin++;
+      int n = cut - lmin >= 0 ? std::min(L, (cut - lmin + 1) * (cut - lmin + 1)) : 0;
+      n = std::min(Lp, (n + 15) / 16 * 16);
+      cols.n[g] = k < L ? n : 0;
+   }
    const int64_t rows = P.tree.nNodes * 3;
    FMM_TRY(P.multBf.reserve(sizeof(__nv_bfloat16) * rows * NP * Lp));
    kSplitMultipoles<NP><<<148 * 16, 256, 0, st>>>((const float*)P.mult.ptr, rows, Lp, (__nv_bfloat16*)P.multBf.ptr);
@@ -634,7 +674,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    kM2LTc<NP, KCW><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, L, Lp, nChunks,
                                                       (const uint8_t*)P.opM2Lbf.ptr, (const __nv_bfloat16*)P.multBf.ptr,
                                                       (float*)P.local.ptr, P.tcDrainEvery, nStages, P.tcDrainMode,
-                                                      nFirst, (unsigned long long*)P.tcCounters.ptr, P.err);
+                                                      cols, (unsigned long long*)P.tcCounters.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
    int herr = 0;

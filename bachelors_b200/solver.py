@@ -88,7 +88,7 @@ class Plan:
     """Owns one fmm_plan (one expansion order, leaf capacity, precision and M2L mode)."""
 
     def __init__(self, order=10, leaf_capacity=64, target_leaf_capacity=0, precision="fp32", m2l="simt",
-                 m2l_truncate=False, device=0, root=None):
+                 m2l_truncate=False, device=0, root=None, m2l_degree_cutoff=0):
         self.lib = _lib.load()
         cfg = _lib.FmmConfig()
         self.lib.fmm_default_config(ctypes.byref(cfg))
@@ -99,6 +99,7 @@ class Plan:
         cfg.m2l_mode = _M2L[m2l]
         cfg.m2l_truncate = int(bool(m2l_truncate))
         cfg.device = int(device)
+        cfg.m2l_tc_degree_cutoff = int(m2l_degree_cutoff)
         if root is not None:
             center, H = root
             for d in range(3):

@@ -68,6 +68,11 @@ typedef struct fmm_config {
    int device;         /* CUDA device ordinal */
    double root_center[3];
    double root_half_width; /* <= 0: the cube around the bounding box of sources and targets */
+   int m2l_tc_degree_cutoff; /* tensor-core M2L modes: translation terms with l + lambda above this are
+                                dropped (they decay like (box size / distance)^(l + lambda)); 0: p + 8,
+                                which keeps the FP64 truncation error near that of the full operator
+                                (about 1e-7 relative at p = 16); < 0: the full operator (l + lambda <= 2p);
+                                values below p are raised to p */
 } fmm_config;
 
 typedef struct fmm_plan fmm_plan;
