@@ -538,95 +538,149 @@ __global__ void __launch_bounds__(NT) kP2M(Tree t, const RootBox* __restrict__ r
 // ====================================================================================
 
 // ====================================================================================
-// M2L on the CUDA cores. A block owns TT consecutive target nodes (3 TT rows: node x
-// component) and all output coefficients; for each of the 316 offsets it gathers the source
-// rows named by the dense V table and multiplies by the operator, K-chunk by K-chunk through
-// shared memory. Thread (rg, cg): rows 12 rg .. 12 rg + 11, columns cg + 64 n.
+// M2L on the CUDA cores (FP32 or FP64 FMA). A block owns TT target boxes from the octant-grouped
+// list of boxes with an M2L list (3 TT rows: box x component) and all output coefficients; it
+// walks only the offsets present in its tile and, per offset, the K chunks of the operator. The
+// gathered source rows and the operator slice of an item are brought to shared memory with
+// cp.async, double-buffered so that the next item's copies run under this item's arithmetic.
+// Warp w owns rows RPT w .. RPT w + RPT - 1 (its A reads are broadcasts), lane c the columns
+// c + 32 n. With the degree cutoff l + lambda <= P, a K chunk whose lowest input degree is
+// lambda_min only reaches the first (P - lambda_min + 1)^2 columns; the rest are skipped.
 // ====================================================================================
-constexpr int M2L_TT = 16;
-constexpr int M2L_ROWS = 3 * M2L_TT;   // 48
-constexpr int M2L_CG = 64;
-constexpr int M2L_NC = 5;              // 5 x 64 = 320 >= Lp for p <= 16
+constexpr int SM_NC = 10;              // 10 x 32 = 320 >= Lp for p <= 16
 
-template <class T, int M2L_KC>
-__global__ void __launch_bounds__(256) kM2LSimt(int firstNode, int nNodes, const int* __restrict__ vtab,
-                                                const int* __restrict__ nv, int p, int Lp,
-                                                const T* __restrict__ opw, const T* __restrict__ M,
-                                                T* __restrict__ Lc)
+template <class T> struct SimtShape;
+template <> struct SimtShape<float> { static constexpr int RPT = 12, KC = 32; };
+template <> struct SimtShape<double> { static constexpr int RPT = 6, KC = 16; };
+
+struct SimtCols
 {
-   __shared__ T As[M2L_KC][M2L_ROWS];
-   __shared__ T Bs[M2L_KC][M2L_CG * M2L_NC];
-   __shared__ int srcRow[M2L_TT];
-   __shared__ int anyPresent;
+   int n[32];   // output columns of each K chunk (0: chunk unused)
+};
+
+__device__ __forceinline__ void cpAsync16Simt(void* dst, const void* src, uint32_t srcBytes)
+{
+   const uint32_t d = uint32_t(__cvta_generic_to_shared(dst));
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(srcBytes) : "memory");
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) kM2LSimt(const int* __restrict__ targets, int nTargets,
+                                                const int* __restrict__ vtab, int p, int Lp, int nChunks,
+                                                const SimtCols cols, const T* __restrict__ opw,
+                                                const T* __restrict__ M, T* __restrict__ Lc)
+{
+   constexpr int RPT = SimtShape<T>::RPT, KC = SimtShape<T>::KC;
+   constexpr int ROWS = 8 * RPT, TT = ROWS / 3;
+   constexpr int NCOL = 32 * SM_NC;
+   extern __shared__ __align__(16) unsigned char smraw[];
+   T* As = (T*)smraw;                       // [2][ROWS][KC]
+   T* Bs = As + 2 * ROWS * KC;              // [2][KC][NCOL]
+   __shared__ int tileNode[TT];
+   __shared__ uint32_t present[10];
+   __shared__ int offs[316];
+   __shared__ int nOffS;
+   __shared__ int colTab[32];
+   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
    const int L = nharm(p);
-   const int tid = threadIdx.x;
-   const int rg = tid / M2L_CG;   // 0..3
-   const int cg = tid % M2L_CG;   // 0..63
-   const int tgt0 = firstNode + blockIdx.x * M2L_TT;
-   T acc[12][M2L_NC];
-#pragma unroll
-   for(int r = 0; r < 12; r++)
-#pragma unroll
-      for(int n = 0; n < M2L_NC; n++) acc[r][n] = T(0);
-   for(int o = 0; o < 316; o++)
+   const int first = blockIdx.x * TT;
+   if(tid < TT) tileNode[tid] = first + tid < nTargets ? targets[first + tid] : -1;
+   if(tid < 10) present[tid] = 0;
+   if(tid == 0)
    {
-      __syncthreads();
-      if(tid == 0) anyPresent = 0;
-      __syncthreads();
-      if(tid < M2L_TT)
+#pragma unroll
+      for(int g = 0; g < 32; g++) colTab[g] = cols.n[g];
+   }
+   __syncthreads();
+   for(int e = tid; e < TT * 316; e += 256)
+   {
+      const int t = tileNode[e / 316], o = e % 316;
+      if(t >= 0 && vtab[int64_t(t) * 316 + o] >= 0) atomicOr(&present[o >> 5], 1u << (o & 31));
+   }
+   __syncthreads();
+   if(tid == 0)
+   {
+      int k = 0;
+      for(int o = 0; o < 316; o++)
+         if(present[o >> 5] & (1u << (o & 31))) offs[k++] = o;
+      nOffS = k;
+   }
+   __syncthreads();
+   const int nItems = nOffS * nChunks;
+   // copies of item it into buffer b: source rows (A) and operator rows k0 .. k0 + KC (B)
+   auto issue = [&](int it, int b) {
+      const int o = offs[it / nChunks], c = it % nChunks;
+      const int k0 = c * KC;
+      const int nCol = colTab[c];
+      T* A = As + b * ROWS * KC;
+      T* B = Bs + b * KC * NCOL;
+      constexpr int ACH = KC * int(sizeof(T)) / 16;          // 16-byte chunks per row
+      for(int e = tid; e < ROWS * ACH; e += 256)
       {
-         int node = tgt0 + tid;
-         int s = -1;
-         if(node < firstNode + nNodes && nv[node] > 0) s = vtab[int64_t(node) * 316 + o];
-         srcRow[tid] = s;
-         if(s >= 0) anyPresent = 1;
+         const int r = e / ACH, q = e % ACH;
+         const int t = tileNode[r / 3];
+         const int src = t >= 0 ? vtab[int64_t(t) * 316 + o] : -1;
+         const T* g = M + (int64_t(src >= 0 ? src : 0) * 3 + r % 3) * Lp + k0 + q * (16 / int(sizeof(T)));
+         cpAsync16Simt(A + r * KC + q * (16 / int(sizeof(T))), g, src >= 0 ? 16u : 0u);
       }
-      __syncthreads();
-      if(!anyPresent) continue;
+      constexpr int BCH = NCOL * int(sizeof(T)) / 16;        // 16-byte chunks per operator row
       const T* op = opw + int64_t(o) * L * Lp;
-      for(int k0 = 0; k0 < L; k0 += M2L_KC)
+      for(int e = tid; e < KC * BCH; e += 256)
       {
-         __syncthreads();
-         // gather A: rows = (target, component), columns = input coefficients k0..k0+KC
-         for(int e = tid; e < M2L_KC * M2L_ROWS; e += 256)
-         {
-            int kk = e % M2L_KC, row = e / M2L_KC;
-            int s = srcRow[row / 3];
-            int k = k0 + kk;
-            As[kk][row] = (s >= 0 && k < L) ? M[(int64_t(s) * 3 + row % 3) * Lp + k] : T(0);
-         }
-         for(int e = tid; e < M2L_KC * M2L_CG * M2L_NC; e += 256)
-         {
-            int col = e % (M2L_CG * M2L_NC), kk = e / (M2L_CG * M2L_NC);
-            int k = k0 + kk;
-            Bs[kk][col] = (k < L && col < Lp) ? op[int64_t(k) * Lp + col] : T(0);
-         }
-         __syncthreads();
-#pragma unroll 4
-         for(int kk = 0; kk < M2L_KC; kk++)
-         {
-            T a[12], bv[M2L_NC];
-#pragma unroll
-            for(int r = 0; r < 12; r++) a[r] = As[kk][12 * rg + r];
-#pragma unroll
-            for(int n = 0; n < M2L_NC; n++) bv[n] = Bs[kk][cg + M2L_CG * n];
-#pragma unroll
-            for(int r = 0; r < 12; r++)
-#pragma unroll
-               for(int n = 0; n < M2L_NC; n++) acc[r][n] += a[r] * bv[n];
-         }
+         const int kk = e / BCH, q = e % BCH;
+         const int col = q * (16 / int(sizeof(T)));
+         const int k = k0 + kk;
+         const bool in = k < L && col < nCol;
+         cpAsync16Simt(B + kk * NCOL + col, op + (in ? int64_t(k) * Lp + col : 0), in ? 16u : 0u);
       }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+   };
+   T acc[RPT][SM_NC];
+#pragma unroll
+   for(int r = 0; r < RPT; r++)
+#pragma unroll
+      for(int n = 0; n < SM_NC; n++) acc[r][n] = T(0);
+   if(nItems > 0) issue(0, 0);
+   for(int it = 0; it < nItems; it++)
+   {
+      const int b = it & 1;
+      if(it + 1 < nItems)
+      {
+         issue(it + 1, b ^ 1);
+         asm volatile("cp.async.wait_group 1;" ::: "memory");
+      }
+      else
+         asm volatile("cp.async.wait_group 0;" ::: "memory");
+      __syncthreads();
+      const T* A = As + b * ROWS * KC + warp * RPT * KC;
+      const T* B = Bs + b * KC * NCOL + lane;
+      const int nCol = colTab[it % nChunks];
+#pragma unroll 2
+      for(int kk = 0; kk < KC; kk++)
+      {
+         T a[RPT], bv[SM_NC];
+#pragma unroll
+         for(int r = 0; r < RPT; r++) a[r] = A[r * KC + kk];
+#pragma unroll
+         for(int n = 0; n < SM_NC; n++) bv[n] = 32 * n < nCol ? B[kk * NCOL + 32 * n] : T(0);
+#pragma unroll
+         for(int r = 0; r < RPT; r++)
+#pragma unroll
+            for(int n = 0; n < SM_NC; n++)
+               if(32 * n < nCol) acc[r][n] += a[r] * bv[n];
+      }
+      __syncthreads();
    }
 #pragma unroll
-   for(int r = 0; r < 12; r++)
+   for(int r = 0; r < RPT; r++)
    {
-      int row = 12 * rg + r;
-      int node = tgt0 + row / 3;
-      if(node >= firstNode + nNodes) continue;
+      const int row = RPT * warp + r;
+      const int node = tileNode[row / 3];
+      if(node < 0) continue;
 #pragma unroll
-      for(int n = 0; n < M2L_NC; n++)
+      for(int n = 0; n < SM_NC; n++)
       {
-         int col = cg + M2L_CG * n;
+         const int col = lane + 32 * n;
          if(col < Lp) Lc[(int64_t(node) * 3 + row % 3) * Lp + col] = col < L ? acc[r][n] : T(0);
       }
    }
@@ -952,14 +1006,31 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
 template <class T>
 fmm_status m2lSimt(Plan& P, cudaStream_t st)
 {
-   const int64_t N = P.tree.nNodes;
-   int first = P.tree.levelStart[1];   // roots have no M2L list
-   int count = int(N - first);
+   const int count = P.nM2LTargets;
    if(count <= 0) return FMM_OK;
-   int blocks = (count + M2L_TT - 1) / M2L_TT;
-   constexpr int KC = sizeof(T) == 4 ? 32 : 16;
-   kM2LSimt<T, KC><<<blocks, 256, 0, st>>>(first, count, P.lists.vtab, P.lists.nv, P.p, P.Lp, (const T*)P.opM2Lw.ptr,
-                                       (const T*)P.mult.ptr, (T*)P.local.ptr);
+   constexpr int RPT = SimtShape<T>::RPT, KC = SimtShape<T>::KC;
+   constexpr int TT = 8 * RPT / 3;
+   const int L = P.L, Lp = P.Lp;
+   const int nChunks = (L + KC - 1) / KC;
+   if(Lp > 32 * SM_NC || nChunks > 32) return setError(FMM_E_INVALID, "CUDA-core M2L supports p <= 16");
+   // degree cutoff (see fmm_config.m2l_tc_degree_cutoff): FP32 plans default to p + 8, FP64 plans
+   // to the full operator
+   const int c = P.cfg.m2l_tc_degree_cutoff;
+   const int cut = c < 0 || (c == 0 && P.fp64) ? 2 * P.p : (c == 0 ? P.p + 8 : std::max(c, P.p));
+   SimtCols cols{};
+   for(int g = 0; g < nChunks; g++)
+   {
+      const int k = KC * g;
+      int lmin = 0;
+      while((lmin + 1) * (lmin + 1) <= k) lmin++;
+      const int n = cut - lmin >= 0 ? std::min(L, (cut - lmin + 1) * (cut - lmin + 1)) : 0;
+      cols.n[g] = std::min(Lp, (n + 3) / 4 * 4);
+   }
+   const size_t smem = sizeof(T) * 2 * (size_t(8 * RPT) * KC + size_t(KC) * 32 * SM_NC);
+   FMM_CUDA(cudaFuncSetAttribute(kM2LSimt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   const int blocks = (count + TT - 1) / TT;
+   kM2LSimt<T><<<blocks, 256, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, P.p, Lp, nChunks, cols,
+                                          (const T*)P.opM2Lw.ptr, (const T*)P.mult.ptr, (T*)P.local.ptr);
    FMM_TRY(launched(P, "kM2LSimt", st));
    FMM_CHECK_LAUNCH();
    return FMM_OK;

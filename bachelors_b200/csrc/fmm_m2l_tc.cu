@@ -673,7 +673,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    FMM_TRY(launched(P, "kSplitMultipoles", st));
    kM2LTc<NP, KCW><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, L, Lp, nChunks,
                                                       (const uint8_t*)P.opM2Lbf.ptr, (const __nv_bfloat16*)P.multBf.ptr,
-                                                      (float*)P.local.ptr, P.tcDrainEvery, nStages, P.tcDrainMode,
+                                                      (float*)P.local.ptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)), nStages, P.tcDrainMode,
                                                       cols, (unsigned long long*)P.tcCounters.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
