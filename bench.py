@@ -41,6 +41,9 @@ sys.path.insert(0, ROOT)
 METRIC = "B evals/s (N=2^24, p=16) split-BF16 vs FP32 FMM at rel err<=1e-6; adjoint/forward"
 UNIT = "target-evals/s"
 SEED = 20260002
+# DRAM bytes (read + write) per M2L pair of the tensor-core M2L, from an ncu capture of the
+# 128 x 32 x 64 torus at p = 16 (2.50 GB for 1,271,544 pairs)
+M2L_DRAM_BYTES_PER_PAIR = 2.50e9 / 1271544
 # a bounded CPU sample of the same workload family: 32 x 8 x 8 torus points, targets = sources
 CPU_SAMPLE = (32, 8, 8)
 
@@ -474,9 +477,14 @@ def main():
         "phases_ms": {k: st[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_near", "ms_total")},
         "tree": {k: st[k] for k in ("nodes", "levels", "v_pairs", "p2p_pairs", "m2l_tiles", "m2l_tile_offsets")},
         "roofline": {"kernel": f"M2L ({m2l})", "bound": "tensor", "achieved": achieved, "peak": bf16_peak,
-                     "unit": "TFLOP/s", "frac": achieved / bf16_peak, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / bf16_peak,
+                     "traffic": M2L_DRAM_BYTES_PER_PAIR * st["v_pairs"] if m2l == "bf16x3" else None,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the "
+                                       "kernel on the 128x32x64 torus (1.97 KB per M2L pair), scaled by the pairs "
+                                       "of this launch",
                      "flops_per_launch": flops_m2l,
-                     "note": "algorithmic FLOPs = V pairs x 3 components x 2 (p+1)^4; peak = measured bf16 dense"},
+                     "note": "algorithmic FLOPs = V pairs x 3 components x 2 (p+1)^4; peak = measured bf16 dense "
+                             "(MEASURED_PEAKS.json, burst)"},
         "clocks": clk,
     }
 
