@@ -19,7 +19,8 @@ FMM_M2L_SIMT, FMM_M2L_BF16X3, FMM_M2L_TF32, FMM_M2L_BF16X6 = 0, 1, 2, 3
 EXPORTS = [
     "fmm_default_config", "fmm_plan_create", "fmm_plan_destroy", "fmm_set_sources", "fmm_set_targets",
     "fmm_build_tree", "fmm_upward", "fmm_downward", "fmm_evaluate", "fmm_solve", "fmm_direct",
-    "fmm_direct_fp64_subset", "fmm_adjoint", "fmm_adjoint_direct", "fmm_batch_set_coils", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
+    "fmm_direct_fp64_subset", "fmm_adjoint", "fmm_adjoint_direct", "fmm_autotune", "fmm_get_tuning",
+    "fmm_set_tuning", "fmm_batch_set_coils", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
     "fmm_get_stats", "fmm_get_operator", "fmm_direct_B_noalloc", "fmm_translate_all", "fmm_translate_all_matrix",
     "fmm_translate_all_matrix_complex", "fmm_add_vectors",
     "fmm_last_error_string", "fmm_version",
@@ -47,6 +48,11 @@ class FmmStats(ctypes.Structure):
         for k in ("nodes", "leaves", "levels", "v_pairs", "p2p_pairs", "p2p_interactions", "n_sources", "n_targets")
     ] + [("ms_adjoint", ctypes.c_double), ("coils", ctypes.c_int64), ("m2l_tiles", ctypes.c_int64),
          ("m2l_tile_offsets", ctypes.c_int64)]
+
+
+class FmmTuning(ctypes.Structure):
+    _fields_ = [("m2l_k_chunk", ctypes.c_int), ("near_tile", ctypes.c_int), ("p2m_chunk", ctypes.c_int),
+                ("ms_upward", ctypes.c_double), ("ms_downward", ctypes.c_double), ("ms_near", ctypes.c_double)]
 
 
 class FmmError(RuntimeError):
@@ -85,6 +91,9 @@ def load():
         "fmm_direct_fp64_subset": (ctypes.c_int, [vp, dbl, vp, i64, vp]),
         "fmm_adjoint": (ctypes.c_int, [vp, dbl, vp, vp, vp, ctypes.c_int, vp]),
         "fmm_adjoint_direct": (ctypes.c_int, [vp, dbl, vp, vp, vp, ctypes.c_int, vp]),
+        "fmm_autotune": (ctypes.c_int, [vp, ctypes.POINTER(FmmTuning), vp]),
+        "fmm_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(FmmTuning)]),
+        "fmm_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(FmmTuning)]),
         "fmm_batch_set_coils": (ctypes.c_int, [vp, i64, vp, vp]),
         "fmm_update_sources": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
         "fmm_graph_capture": (ctypes.c_int, [vp, ctypes.c_int, vp]),

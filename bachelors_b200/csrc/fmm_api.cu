@@ -2,6 +2,8 @@
 // phase sequencing, timing and error reporting.
 #include <cstdlib>
 #include <cstring>
+#include <array>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -20,6 +22,15 @@ fmm_status directFp64Subset(Plan& P, double current, const double* tgtDev, int k
 
 namespace {
 thread_local std::string g_lastError;
+
+// autotuned choices per (device, order, leaf capacity, target leaf capacity, precision, M2L mode)
+std::mutex g_tuneMutex;
+std::map<std::array<int, 6>, fmm_tuning> g_tuned;
+
+std::array<int, 6> tuneKey(const fmm_config& c)
+{
+   return {c.device, c.order, c.leaf_capacity, c.target_leaf_capacity, c.precision, c.m2l_mode};
+}
 }
 
 fmm_status setError(fmm_status s, const char* fmt, ...)
@@ -73,11 +84,21 @@ fmm_status Plan::init(const fmm_config& c)
    fp64 = c.precision == FMM_FP64;
    const char* dbg = getenv("FMM_DEBUG_SYNC");
    debugSync = dbg && dbg[0] == '1';
+   {
+      std::lock_guard<std::mutex> lock(g_tuneMutex);
+      auto it = g_tuned.find(tuneKey(c));
+      if(it != g_tuned.end())
+      {
+         tcKChunk = it->second.m2l_k_chunk;
+         nearTile = it->second.near_tile;
+         p2mChunk = it->second.p2m_chunk;
+      }
+   }
    if(const char* e = getenv("FMM_TC_KC")) tcKChunk = atoi(e) == 32 ? 32 : 64;
    if(const char* e = getenv("FMM_TC_DRAIN")) tcDrainEvery = std::max(1, atoi(e));
    if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(2, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
-   if(const char* e = getenv("FMM_TC_BALANCED")) tcBalancedN = atoi(e) != 0;
+
    FMM_TRY(rootb.reserve(sizeof(RootBox)));
    FMM_TRY(errb.reserve(sizeof(int)));
    FMM_TRY(initOffsetTables());
@@ -489,6 +510,122 @@ fmm_status fmm_adjoint_direct(fmm_plan* plan, double current, const void* dL_dB,
       if(dL_dx && P.n) FMM_CUDA(cudaMemcpyAsync(dL_dx, dx, es * 3 * P.n, cudaMemcpyDeviceToHost, st));
       FMM_CUDA(cudaStreamSynchronize(st));
    }
+   return FMM_OK;
+}
+
+fmm_status fmm_get_tuning(const fmm_plan* plan, fmm_tuning* out)
+{
+   if(!plan || !out) return setError(FMM_E_INVALID, "null argument");
+   const Plan& P = plan->P;
+   std::memset(out, 0, sizeof(*out));
+   out->m2l_k_chunk = P.tcKChunk ? P.tcKChunk : (P.cfg.m2l_mode == FMM_M2L_BF16X6 ? 32 : 64);
+   out->near_tile = P.nearTile;
+   out->p2m_chunk = P.p2mChunk;
+   return FMM_OK;
+}
+
+fmm_status fmm_set_tuning(fmm_plan* plan, const fmm_tuning* in)
+{
+   if(!plan || !in) return setError(FMM_E_INVALID, "null argument");
+   if((in->m2l_k_chunk != 32 && in->m2l_k_chunk != 64) || (in->near_tile != 128 && in->near_tile != 256) ||
+      (in->p2m_chunk != 16 && in->p2m_chunk != 32))
+      return setError(FMM_E_INVALID, "fmm_set_tuning: m2l_k_chunk 32|64, near_tile 128|256, p2m_chunk 16|32");
+   Plan& P = plan->P;
+   P.tcKChunk = in->m2l_k_chunk;
+   P.nearTile = in->near_tile;
+   P.p2mChunk = in->p2m_chunk;
+   P.dropGraph();
+   return FMM_OK;
+}
+
+fmm_status fmm_autotune(fmm_plan* plan, fmm_tuning* out, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!P.downReady) return setError(FMM_E_INVALID, "fmm_autotune: run fmm_solve first (the tuner times the plan's data)");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   P.dropGraph();
+   cudaEvent_t e0, e1;
+   FMM_CUDA(cudaEventCreate(&e0));
+   cudaError_t ce = cudaEventCreate(&e1);
+   if(ce != cudaSuccess)
+   {
+      cudaEventDestroy(e0);
+      return setError(FMM_E_CUDA, "fmm_autotune: %s", cudaGetErrorString(ce));
+   }
+   fmm_status s = FMM_OK;
+   // best of two runs of one phase, in milliseconds
+   auto timePhase = [&](auto&& phase, double& ms) -> fmm_status {
+      ms = 1e300;
+      for(int r = 0; r < 2; r++)
+      {
+         cudaEventRecord(e0, st);
+         FMM_TRY(phase());
+         cudaEventRecord(e1, st);
+         FMM_CUDA(cudaEventSynchronize(e1));
+         float t = 0;
+         cudaEventElapsedTime(&t, e0, e1);
+         ms = std::min(ms, double(t));
+      }
+      return FMM_OK;
+   };
+   auto up = [&]() { return P.fp64 ? upwardT<double>(P, st) : upwardT<float>(P, st); };
+   auto down = [&]() { return P.fp64 ? downwardT<double>(P, st) : downwardT<float>(P, st); };
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   auto near = [&]() { return P.fp64 ? evaluateT<double>(P, 1.0, 1, st) : evaluateT<float>(P, 1.0, 1, st); };
+   fmm_tuning best{};
+   do
+   {
+      s = P.outB.reserve(es * 3 * std::max<int64_t>(P.m, 1));
+      if(s != FMM_OK) break;
+      // P2M chunk
+      double bestMs = 1e300;
+      for(int cv : {16, 32})
+      {
+         P.p2mChunk = cv;
+         double ms;
+         if((s = timePhase(up, ms)) != FMM_OK) break;
+         if(ms < bestMs) { bestMs = ms; best.p2m_chunk = cv; best.ms_upward = ms; }
+      }
+      if(s != FMM_OK) break;
+      P.p2mChunk = best.p2m_chunk;
+      // tensor-core M2L K chunk (CUDA-core and FP64 plans have one shape)
+      bestMs = 1e300;
+      const bool tc = !P.fp64 && P.cfg.m2l_mode != FMM_M2L_SIMT;
+      for(int kc : {64, 32})
+      {
+         if(!tc && kc == 32) continue;
+         P.tcKChunk = kc;
+         double ms;
+         if((s = timePhase(down, ms)) != FMM_OK) break;
+         if(ms < bestMs) { bestMs = ms; best.m2l_k_chunk = kc; best.ms_downward = ms; }
+      }
+      if(s != FMM_OK) break;
+      P.tcKChunk = best.m2l_k_chunk;
+      // leave the plan's locals from a run of the chosen variant
+      if((s = down()) != FMM_OK) break;
+      // near-field tile
+      bestMs = 1e300;
+      for(int ts : {256, 128})
+      {
+         P.nearTile = ts;
+         double ms;
+         if((s = timePhase(near, ms)) != FMM_OK) break;
+         if(ms < bestMs) { bestMs = ms; best.near_tile = ts; best.ms_near = ms; }
+      }
+      if(s != FMM_OK) break;
+      P.nearTile = best.near_tile;
+      FMM_CUDA(cudaStreamSynchronize(st));
+   } while(false);
+   cudaEventDestroy(e0);
+   cudaEventDestroy(e1);
+   FMM_TRY(s);
+   {
+      std::lock_guard<std::mutex> lock(g_tuneMutex);
+      g_tuned[tuneKey(P.cfg)] = best;
+   }
+   if(out) *out = best;
    return FMM_OK;
 }
 

@@ -146,7 +146,8 @@ struct Plan
                                          // with twice the accumulations per offset, drains twice as often)
    int tcDrainMode = 2;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1
    int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length
-   int tcBalancedN = 0;                  // split the N output columns into two near-equal MMAs
+   int nearTile = 256;                   // near-field source tile, points (128 or 256)
+   int p2mChunk = 16;                    // P2M recurrence steps reduced per shared tile (16 or 32)
    DevBuf tcCounters;                    // [items, tile-offset pairs] of the last tensor-core M2L
    int64_t tcTiles = 0;
    int opImgOrder = -1;                  // order the tensor-core operator image was built for

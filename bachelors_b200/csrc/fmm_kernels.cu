@@ -984,10 +984,14 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
    FMM_TRY(P.mult.reserve(sizeof(T) * N * 3 * Lp));
    FMM_CUDA(cudaMemsetAsync(P.mult.ptr, 0, sizeof(T) * N * 3 * Lp, st));
    typedef typename Vec4<T>::type V4;
-   constexpr int NT = 64, CV = 16;
+   constexpr int NT = 64;
    const size_t shm = sizeof(T) * 3 * Lp;
-   kP2M<T, NT, CV><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
-                                           (T*)P.mult.ptr);
+   if(P.p2mChunk == 32)
+      kP2M<T, NT, 32><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
+                                              (T*)P.mult.ptr);
+   else
+      kP2M<T, NT, 16><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
+                                              (T*)P.mult.ptr);
    FMM_TRY(launched(P, "kP2M", st));
    FMM_CHECK_LAUNCH();
    const int nCol = (Lp + TG_N - 1) / TG_N;
@@ -1065,7 +1069,8 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
    typedef typename Vec4<T>::type V4;
    const int64_t N = P.tree.nNodes;
    const int L = P.L, Lb = nharm(P.p - 1);
-   constexpr int NT = 64, TS = 256, NE = 128;
+   constexpr int NT = 64, NE = 128;
+   const int TS = P.nearTile == 128 ? 128 : 256;
    size_t shm = ((sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31)) + 2 * sizeof(V4) * TS + sizeof(double) * 6 * NT;
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
    auto run = [&](auto kernel) -> fmm_status {
@@ -1076,8 +1081,16 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
                                       (T*)P.outB.ptr, (T*)P.outA.ptr);
       return FMM_OK;
    };
-   if(want & 2) FMM_TRY(run(kL2PNear<T, NT, TS, NE, true>));
-   else FMM_TRY(run(kL2PNear<T, NT, TS, NE, false>));
+   if(TS == 128)
+   {
+      if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 128, NE, true>));
+      else FMM_TRY(run(kL2PNear<T, NT, 128, NE, false>));
+   }
+   else
+   {
+      if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 256, NE, true>));
+      else FMM_TRY(run(kL2PNear<T, NT, 256, NE, false>));
+   }
    FMM_TRY(launched(P, "kL2PNear", st));
    FMM_CHECK_LAUNCH();
    return FMM_OK;

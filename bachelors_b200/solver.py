@@ -252,6 +252,22 @@ class Plan:
                                                    len(t), ctypes.c_void_p(out.ctypes.data)))
         return out
 
+    def autotune(self):
+        """Times the kernels' tile choices on this plan's data (after a solve) and keeps the fastest;
+        later plans with the same order, leaf sizes, precision and M2L mode start with it."""
+        t = _lib.FmmTuning()
+        _lib.check(self.lib.fmm_autotune(self.handle, ctypes.byref(t), self._stream()))
+        return {k: getattr(t, k) for k, _ in _lib.FmmTuning._fields_}
+
+    def tuning(self):
+        t = _lib.FmmTuning()
+        _lib.check(self.lib.fmm_get_tuning(self.handle, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _lib.FmmTuning._fields_[:3]}
+
+    def set_tuning(self, m2l_k_chunk=64, near_tile=256, p2m_chunk=16):
+        t = _lib.FmmTuning(int(m2l_k_chunk), int(near_tile), int(p2m_chunk), 0.0, 0.0, 0.0)
+        _lib.check(self.lib.fmm_set_tuning(self.handle, ctypes.byref(t)))
+
     def stats(self):
         s = _lib.FmmStats()
         _lib.check(self.lib.fmm_get_stats(self.handle, ctypes.byref(s)))

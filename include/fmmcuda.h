@@ -163,6 +163,24 @@ fmm_status fmm_adjoint_direct(fmm_plan* plan, double current, const void* dL_dB,
 #define FMM_MAX_COILS 65536
 fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* src_offsets, const int64_t* tgt_offsets);
 
+/* Tile choices of the kernels (no counterpart in the reference, whose kernels have fixed shapes).
+ * Every choice computes the same result up to rounding; they differ in speed with the order, the
+ * leaf sizes and the point distribution. */
+typedef struct fmm_tuning {
+   int m2l_k_chunk;  /* tensor-core M2L: K chunk width, 64 (two 108 KB stages at p = 16) or 32 (four) */
+   int near_tile;    /* near field: source points per shared-memory tile, 128 or 256 */
+   int p2m_chunk;    /* P2M: recurrence steps reduced per shared-memory tile, 16 or 32 */
+   double ms_upward, ms_downward, ms_near; /* fmm_autotune: the chosen variants' times */
+} fmm_tuning;
+
+/* The project's autotuner: times every variant of each choice on the plan's current data (call it
+ * after an fmm_solve, which builds the tree), keeps the fastest and records it for plans created
+ * later in this process with the same device, order, leaf capacities, precision and M2L mode (they
+ * start with it). The plan's expansions stay valid; `out` may be NULL. Synchronises `stream`. */
+fmm_status fmm_autotune(fmm_plan* plan, fmm_tuning* out, void* stream);
+fmm_status fmm_get_tuning(const fmm_plan* plan, fmm_tuning* out);
+fmm_status fmm_set_tuning(fmm_plan* plan, const fmm_tuning* tuning);
+
 /* New weights w[n] and currents J[3n] for the same source positions (J must be NULL exactly when
  * the sources were set without J). Keeps the tree; the next solve or graph launch uses them. */
 fmm_status fmm_update_sources(fmm_plan* plan, const void* w, const void* J, int on_device, void* stream);

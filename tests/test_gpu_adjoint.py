@@ -117,3 +117,24 @@ def test_adjoint_direct_matches_oracle(precision, tol, with_J):
     assert np.linalg.norm(dJ - rJ) / np.linalg.norm(rJ) < tol
     assert np.linalg.norm(dx - rx) / np.linalg.norm(rx) < tol
     plan.close()
+
+
+def test_autograd_gradcheck_fp64():
+    """torch.autograd.gradcheck of the wrapper in FP64 on a small problem: the adjoint FMM's
+    Jacobian-vector products against finite differences of the forward FMM (positions and J)."""
+    import torch
+    from bachelors_b200 import Plan
+    from bachelors_b200.autograd import biot_savart
+    xyz, w, J = G.torus(8, 4, 2, 2.0, 0.5)
+    rng = np.random.default_rng(11)
+    tgt = rng.normal(size=(6, 3))
+    tgt = tgt / np.linalg.norm(tgt, axis=1, keepdims=True) * 6.0
+    c, H = G.root_cube(xyz, tgt)
+    plan = Plan(order=16, leaf_capacity=8, precision="fp64", root=(c, H * 1.01))
+    X = torch.tensor(xyz, dtype=torch.float64, device="cuda", requires_grad=True)
+    Jt = torch.tensor(J, dtype=torch.float64, device="cuda", requires_grad=True)
+    Wt = torch.tensor(w, dtype=torch.float64, device="cuda")
+    T = torch.tensor(tgt, dtype=torch.float64, device="cuda")
+    f = lambda x, j: biot_savart(x, Wt, j, T, plan=plan) * 1e7   # scale B (~1e-7 T) to O(1)
+    assert torch.autograd.gradcheck(f, (X, Jt), eps=1e-6, atol=1e-5, rtol=1e-3)
+    plan.close()
