@@ -12,7 +12,8 @@
 // the tile it accumulates  D[128 x N] += A_o[128 x K] * T_o^T[K x N]  where the rows of A_o are
 // the gathered source multipoles. Operands are split into bf16 pieces: x = hi + lo with the three
 // products hi*hi + hi*lo + lo*hi (BF16X3), or x = hi + mid + lo with the six products down to
-// 2^-16 relative (BF16X6); all are accumulated in FP32 in tensor memory.
+// 2^-16 relative (BF16X6), or one TF32 product of operands rounded to 11 significant bits (TF32,
+// kind::tf32, 4-byte elements); all are accumulated in FP32 in tensor memory.
 //
 // Warp roles (448 threads):
 //   warp 0      TMEM allocation; lane 0 issues the tcgen05.mma instructions
@@ -133,6 +134,33 @@ __device__ __forceinline__ void mmaBf16(uint32_t dTmem, uint64_t aDesc, uint64_t
       ::"r"(dTmem), "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate));
 }
 
+// Instruction descriptor: tf32 x tf32 -> f32, A and B K-major, shape M x N.
+__host__ __device__ constexpr uint32_t instrDescTf32(int M, int N)
+{
+   return (1u << 4)                  // D format F32
+          | (2u << 7)                // A format TF32
+          | (2u << 10)               // B format TF32
+          | (uint32_t(N >> 3) << 17) // N
+          | (uint32_t(M >> 4) << 24);  // M
+}
+
+__device__ __forceinline__ void mmaTf32(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc, uint32_t accumulate)
+{
+   asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(dTmem), "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate));
+}
+
+// x rounded to tf32 (10 explicit mantissa bits, round to nearest, ties away), as its fp32 bit pattern
+__device__ __forceinline__ uint32_t toTf32(float x)
+{
+   uint32_t r;
+   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+   return r;
+}
+
 __device__ __forceinline__ void mmaCommit(uint32_t bar)
 {
    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -180,31 +208,42 @@ __device__ __forceinline__ void tmemLd16(uint32_t addr, float* v)
 // (128-byte swizzle) or 32 elements in 64-byte rows (64-byte swizzle). A stage holds one chunk
 // of every piece of A (128 rows) and of T_o (N rows); the number of stages is what fits in
 // shared memory (2 with 64-wide chunks of two pieces at p = 16, 4 with 32-wide ones).
+// ES: element bytes; KSTEP: K elements per MMA instruction (32 bytes for both element types).
 template <int KCW> struct Layout;
 template <> struct Layout<64>
 {
-   static constexpr int KC = 64, RB = 128, SBO = 1024, SWZ = 2;
+   static constexpr int KC = 64, RB = 128, SBO = 1024, SWZ = 2, ES = 2, KSTEP = 16;
+   static constexpr bool TF32 = false;
    __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
    { return row * 128u + ((((k >> 3) ^ (row & 7u)) & 7u) << 4) + ((k & 7u) << 1); }
 };
 template <> struct Layout<32>
 {
-   static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4;
+   static constexpr int KC = 32, RB = 64, SBO = 512, SWZ = 4, ES = 2, KSTEP = 16;
+   static constexpr bool TF32 = false;
    __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
    { return row * 64u + ((((k >> 3) ^ ((row >> 1) & 3u)) & 3u) << 4) + ((k & 7u) << 1); }
+};
+// tf32 operands: 32 elements of 4 bytes per 128-byte row, 128-byte swizzle
+struct LayoutTf32
+{
+   static constexpr int KC = 32, RB = 128, SBO = 1024, SWZ = 2, ES = 4, KSTEP = 8;
+   static constexpr bool TF32 = true;
+   __host__ __device__ static constexpr uint32_t off(uint32_t row, uint32_t k)
+   { return row * 128u + ((((k >> 2) ^ (row & 7u)) & 7u) << 4) + ((k & 3u) << 2); }
 };
 constexpr int MAXSTAGE = 6;
 
 // Shared-memory matrix descriptor: K-major, swizzled rows, 8-row groups SBO bytes apart.
-template <int KCW>
+template <class Lay>
 __device__ __forceinline__ uint64_t smemDescT(uint32_t addr)
 {
    uint64_t d = 0;
    d |= uint64_t((addr >> 4) & 0x3FFF);               // start address
    d |= uint64_t(1) << 16;                             // leading byte offset (unused when swizzled)
-   d |= uint64_t(Layout<KCW>::SBO >> 4) << 32;        // stride byte offset
+   d |= uint64_t(Lay::SBO >> 4) << 32;                // stride byte offset
    d |= uint64_t(1) << 46;                             // descriptor version for sm_100
-   d |= uint64_t(Layout<KCW>::SWZ) << 61;             // swizzle mode
+   d |= uint64_t(Lay::SWZ) << 61;                     // swizzle mode
    return d;
 }
 
@@ -226,10 +265,9 @@ __device__ __forceinline__ void splitBf16(double x, __nv_bfloat16* piece)
 // Operator image for the tensor-core M2L: for every offset slot and K chunk, the NP piece blocks
 // (hi first), each N rows (output coefficients, N = Lp) x KC bf16 (input coefficients) in the
 // swizzled K-major layout, zero outside the (p+1)^2 x (p+1)^2 operator.
-template <int NP, int KCW>
+template <int NP, class Lay>
 __global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int nChunks, uint8_t* img)
 {
-   using Lay = tc::Layout<KCW>;
    const int64_t blockBytes = int64_t(N) * Lay::RB;
    const int64_t total = int64_t(316) * nChunks * int64_t(N) * Lay::KC;
    for(int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
@@ -241,12 +279,17 @@ __global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int
       const int o = int(r / nChunks);
       const int k = c * Lay::KC + kk;
       const double x = (n < L && k < L) ? op64[(int64_t(o) * L + n) * L + k] : 0.0;
-      __nv_bfloat16 piece[NP];
-      tc::splitBf16<NP>(x, piece);
       uint8_t* blk = img + (int64_t(o) * nChunks + c) * NP * blockBytes;
+      if constexpr(Lay::TF32)
+         *reinterpret_cast<uint32_t*>(blk + Lay::off(uint32_t(n), uint32_t(kk))) = tc::toTf32(float(x));
+      else
+      {
+         __nv_bfloat16 piece[NP];
+         tc::splitBf16<NP>(x, piece);
 #pragma unroll
-      for(int i = 0; i < NP; i++)
-         *reinterpret_cast<__nv_bfloat16*>(blk + i * blockBytes + Lay::off(uint32_t(n), uint32_t(kk))) = piece[i];
+         for(int i = 0; i < NP; i++)
+            *reinterpret_cast<__nv_bfloat16*>(blk + i * blockBytes + Lay::off(uint32_t(n), uint32_t(kk))) = piece[i];
+      }
    }
 }
 
@@ -256,40 +299,47 @@ __global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int
 // Output columns each 16-wide K step of the M2L needs: with the degree cutoff l + lambda <= P, the
 // inputs of a K step (degrees >= lambda_min) only reach outputs of degree <= P - lambda_min,
 // which are the first (P - lambda_min + 1)^2 columns (rounded up to 16). Step 0 is always full.
+constexpr int MAXKSTEPS = 64;   // K steps of one row (38 at p = 16 with 8-element TF32 steps)
 struct M2LCols
 {
-   int n[32];
+   int n[MAXKSTEPS];
 };
 
-template <int NP>
-__global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int Lp, __nv_bfloat16* __restrict__ Mbf)
+template <int NP, bool TF32>
+__global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int Lp, uint8_t* __restrict__ Mout)
 {
+   __nv_bfloat16* Mbf = reinterpret_cast<__nv_bfloat16*>(Mout);
    const int64_t total = rows * Lp;
    for(int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
    {
       const int64_t row = e / Lp;
       const int k = int(e % Lp);
       float r = M[e];
-#pragma unroll
-      for(int j = 0; j < NP; j++)
+      if constexpr(TF32)
+         reinterpret_cast<uint32_t*>(Mout)[e] = tc::toTf32(r);   // one piece
+      else
       {
-         const __nv_bfloat16 b = __float2bfloat16_rn(r);
-         Mbf[(row * NP + j) * Lp + k] = b;
-         r -= __bfloat162float(b);
+#pragma unroll
+         for(int j = 0; j < NP; j++)
+         {
+            const __nv_bfloat16 b = __float2bfloat16_rn(r);
+            Mbf[(row * NP + j) * Lp + k] = b;
+            r -= __bfloat162float(b);
+         }
       }
    }
 }
 
-template <int NP, int KCW>
+template <int NP, class Lay>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int L, int Lp, int nChunks,
-       const uint8_t* __restrict__ img, const __nv_bfloat16* __restrict__ Mbf, float* __restrict__ Lc, int drainEvery,
+       const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc, int drainEvery,
        int nStages, int drainMode, const M2LCols cols, unsigned long long* counters, int* err)
 {
    using namespace tc;
-   using Lay = Layout<KCW>;
    constexpr int KCH = Lay::KC;
-   constexpr int NPASS = NP == 2 ? 3 : 6;
+   constexpr int KS = Lay::KSTEP;                      // K elements per MMA
+   constexpr int NPASS = NP == 1 ? 1 : (NP == 2 ? 3 : 6);
    // (A piece, B piece) of every product kept: hi*hi, hi*lo, lo*hi  /  down to 2^-16 with three pieces
    constexpr int PA[6] = {0, 0, 1, 1, 0, 2};
    constexpr int PB[6] = {0, 1, 0, 1, 2, 0};
@@ -311,7 +361,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 136); // 10 words: offsets present in the tile
    int* itemOffset = reinterpret_cast<int*>(ctrl + 192);        // compacted present offsets [316] + count
    int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
-   int* colTab = tileNode + 64;                                 // output columns per K step [32]
+   int* colTab = tileNode + 64;                                 // output columns per K step [MAXKSTEPS]
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
@@ -325,7 +375,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    if(tid == 0)
    {
 #pragma unroll
-      for(int g = 0; g < 32; g++) colTab[g] = cols.n[g];
+      for(int g = 0; g < MAXKSTEPS; g++) colTab[g] = cols.n[g];
    }
    if(tid == 0)
    {
@@ -385,9 +435,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          {
             const int s = it % NS;
             // this chunk's output widths per K step, read before the wait
-            int nColK[KCH / 16];
+            int nColK[KCH / KS];
 #pragma unroll
-            for(int ks = 0; ks < KCH / 16; ks++) nColK[ks] = colTab[(it % nChunks) * (KCH / 16) + ks];
+            for(int ks = 0; ks < KCH / KS; ks++) nColK[ks] = colTab[(it % nChunks) * (KCH / KS) + ks];
             if(!mbarWait(fullBar0 + 8 * s, (it / NS) & 1, err, abortFlag)) break;
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
@@ -395,12 +445,12 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             // K steps of 16 that reach a coefficient < L (the last chunk is partly padding); chunks run
             // in increasing K, so an accumulation always starts with a full-width MMA
             const int cItem = it % nChunks;
-            const int kSteps = min(KCH / 16, (L - cItem * KCH + 15) / 16);
+            const int kSteps = min(KCH / KS, (L - cItem * KCH + KS - 1) / KS);
             // descriptors of the stage's pieces; an MMA's operand is the piece's descriptor plus its
             // byte offset / 16 (the start-address field, bits 0-13, holds every address of the stage)
-            const uint64_t dA = smemDescT<KCW>(aSt), dB = smemDescT<KCW>(bSt);
+            const uint64_t dA = smemDescT<Lay>(aSt), dB = smemDescT<Lay>(bSt);
 #pragma unroll
-            for(int ks = 0; ks < KCH / 16; ks++)
+            for(int ks = 0; ks < KCH / KS; ks++)
             {
                if(ks >= kSteps) break;
                const uint32_t koff = ks * 32;
@@ -408,18 +458,26 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                const int nCol = nColK[ks];
                if(nCol == 0) break;
                const int nA = min(nCol, 256), nB = nCol - nA;
-               const uint32_t idA = instrDescBf16(ROWS, nA);
-               const uint32_t idB = instrDescBf16(ROWS, nB > 0 ? nB : 16);
+               const uint32_t idA = Lay::TF32 ? instrDescTf32(ROWS, nA) : instrDescBf16(ROWS, nA);
+               const uint32_t idB = Lay::TF32 ? instrDescTf32(ROWS, nB > 0 ? nB : 16) : instrDescBf16(ROWS, nB > 0 ? nB : 16);
 #pragma unroll
                for(int pass = 0; pass < NPASS; pass++)
                {
-                  const int pa = NP == 2 ? PA2[pass] : PA[pass];
-                  const int pb = NP == 2 ? PB2[pass] : PB[pass];
+                  const int pa = NP == 1 ? 0 : (NP == 2 ? PA2[pass] : PA[pass]);
+                  const int pb = NP == 1 ? 0 : (NP == 2 ? PB2[pass] : PB[pass]);
                   const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
                   const uint64_t db = dB + ((pb * bBytes + koff) >> 4);
                   const uint32_t acc = firstMma ? 0u : 1u;
-                  mmaBf16(tmem, da, db, idA, acc);
-                  if(nB > 0) mmaBf16(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                  if constexpr(Lay::TF32)
+                  {
+                     mmaTf32(tmem, da, db, idA, acc);
+                     if(nB > 0) mmaTf32(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                  }
+                  else
+                  {
+                     mmaBf16(tmem, da, db, idA, acc);
+                     if(nB > 0) mmaBf16(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                  }
                   firstMma = false;
                }
             }
@@ -459,7 +517,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
             const uint32_t dst = base + s * stageBytes + NP * aBytes;
             // only the operator rows (output columns) this chunk's widest K step uses
-            const uint32_t rowBytes = uint32_t(colTab[c * (KCH / 16)]) * Lay::RB;
+            const uint32_t rowBytes = uint32_t(colTab[c * (KCH / KS)]) * Lay::RB;
             mbarArriveExpectTx(fullBar0 + 8 * s, NP * rowBytes);
 #pragma unroll
             for(int j = 0; j < NP; j++) bulkLoad(dst + j * bBytes, src + j * bBytes, rowBytes, fullBar0 + 8 * s);
@@ -565,7 +623,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       // of every piece each. Item it - 1 is signalled as soon as its copies have landed, then the
       // copies of item it are issued once its stage is free: one item's gather is in flight while
       // the tensor cores work on the previous one, and issuing never delays a signal.
-      constexpr int PER = KCH / 2;
+      constexpr int PER = KCH / 2;                   // K elements per thread and chunk
+      constexpr int EPC = 16 / Lay::ES;              // elements per 16-byte copy
       const int ptid = tid - 64;
       const int row = ptid >> 1, half = ptid & 1;
       const int slot = row / 3, comp = row % 3;
@@ -589,15 +648,16 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag)) break;
          const uint32_t aSt = base + s * stageBytes;
          const int k0 = c * KCH + half * PER;
-         const __nv_bfloat16* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp;
+         const uint8_t* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp * Lay::ES;
 #pragma unroll
-         for(int q = 0; q < PER / 8; q++)
+         for(int q = 0; q < PER / EPC; q++)
          {
-            const int k = k0 + 8 * q;
+            const int k = k0 + EPC * q;
             const uint32_t bytes = (src >= 0 && k < Lp) ? 16u : 0u;
-            const uint32_t off = Lay::off(uint32_t(row), uint32_t(half * PER + 8 * q));
+            const uint32_t off = Lay::off(uint32_t(row), uint32_t(half * PER + EPC * q));
 #pragma unroll
-            for(int j = 0; j < NP; j++) cpAsync16(aSt + j * aBytes + off, rowp + j * Lp + (bytes ? k : 0), bytes);
+            for(int j = 0; j < NP; j++)
+               cpAsync16(aSt + j * aBytes + off, rowp + (int64_t(j) * Lp + (bytes ? k : 0)) * Lay::ES, bytes);
          }
          cpAsyncCommit();
          pending = it;
@@ -622,18 +682,17 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    }
 }
 
-template <int NP, int KCW>
+template <int NP, class Lay>
 static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
 {
-   using Lay = tc::Layout<KCW>;
    const int L = P.L, Lp = P.Lp;
    const int nChunks = (L + Lay::KC - 1) / Lay::KC;
    const size_t imgBytes = size_t(316) * nChunks * NP * size_t(Lp) * Lay::RB;
-   const int tag = (P.p * 8 + NP) * 128 + KCW;
+   const int tag = ((P.p * 8 + NP) * 128 + Lay::KC) * 2 + (Lay::TF32 ? 1 : 0);
    if(P.opImgOrder != tag)
    {
       FMM_TRY(P.opM2Lbf.reserve(imgBytes));
-      kPrepM2LImage<NP, KCW><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, L, Lp, nChunks,
+      kPrepM2LImage<NP, Lay><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, L, Lp, nChunks,
                                                    (uint8_t*)P.opM2Lbf.ptr);
       FMM_TRY(launched(P, "kPrepM2LImage", st));
       P.opImgOrder = tag;
@@ -642,12 +701,12 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(count <= 0) return FMM_OK;
    const int blocks = (count + tc::TT - 1) / tc::TT;
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 192 + 4 * (320 + 64 + 32);
+   const size_t fixed = 1024 + 192 + 4 * (320 + 64 + MAXKSTEPS);
    const size_t budget = 232448;
    const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
    const size_t smem = fixed + nStages * stageBytes;
-   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, KCW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
    FMM_TRY(P.tcCounters.reserve(2 * sizeof(unsigned long long)));
    FMM_CUDA(cudaMemsetAsync(P.tcCounters.ptr, 0, 2 * sizeof(unsigned long long), st));
@@ -658,9 +717,11 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    const int cut = P.cfg.m2l_tc_degree_cutoff == 0 ? P.p + 8 : (P.cfg.m2l_tc_degree_cutoff < 0 ? 2 * P.p
                                                                 : std::max(P.cfg.m2l_tc_degree_cutoff, P.p));
    M2LCols cols{};
-   for(int g = 0; g < nChunks * (Lay::KC / 16) && g < 32; g++)
+   if(nChunks * (Lay::KC / Lay::KSTEP) > MAXKSTEPS)
+      return setError(FMM_E_INVALID, "tensor-core M2L: %d K steps exceed the column table", nChunks * (Lay::KC / Lay::KSTEP));
+   for(int g = 0; g < nChunks * (Lay::KC / Lay::KSTEP); g++)
    {
-      const int k = 16 * g;
+      const int k = Lay::KSTEP * g;
       int lmin = 0;
       while((lmin + 1) * (lmin + 1) <= k) lmin++;
       int n = cut - lmin >= 0 ? std::min(L, (cut - lmin + 1) * (cut - lmin + 1)) : 0;
@@ -668,11 +729,11 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
       cols.n[g] = k < L ? n : 0;
    }
    const int64_t rows = P.tree.nNodes * 3;
-   FMM_TRY(P.multBf.reserve(sizeof(__nv_bfloat16) * rows * NP * Lp));
-   kSplitMultipoles<NP><<<148 * 16, 256, 0, st>>>((const float*)P.mult.ptr, rows, Lp, (__nv_bfloat16*)P.multBf.ptr);
+   FMM_TRY(P.multBf.reserve(size_t(Lay::ES) * rows * NP * Lp));
+   kSplitMultipoles<NP, Lay::TF32><<<148 * 16, 256, 0, st>>>((const float*)P.mult.ptr, rows, Lp, (uint8_t*)P.multBf.ptr);
    FMM_TRY(launched(P, "kSplitMultipoles", st));
-   kM2LTc<NP, KCW><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, L, Lp, nChunks,
-                                                      (const uint8_t*)P.opM2Lbf.ptr, (const __nv_bfloat16*)P.multBf.ptr,
+   kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, L, Lp, nChunks,
+                                                      (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
                                                       (float*)P.local.ptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)), nStages, P.tcDrainMode,
                                                       cols, (unsigned long long*)P.tcCounters.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
@@ -688,11 +749,12 @@ fmm_status m2lTensorCore(Plan& P, cudaStream_t st)
 {
    if(P.Lp > 320) return setError(FMM_E_INVALID, "tensor-core M2L supports p <= 16");
    if(P.Lp % 16) return setError(FMM_E_INVALID, "tensor-core M2L needs 16-aligned coefficient rows");
+   using tc::Layout;
    if(P.cfg.m2l_mode == FMM_M2L_BF16X3)
-      return P.tcKChunk == 32 ? launchM2LTc<2, 32>(P, st) : launchM2LTc<2, 64>(P, st);
+      return P.tcKChunk == 32 ? launchM2LTc<2, Layout<32>>(P, st) : launchM2LTc<2, Layout<64>>(P, st);
    if(P.cfg.m2l_mode == FMM_M2L_BF16X6)
-      return P.tcKChunk == 64 ? launchM2LTc<3, 64>(P, st) : launchM2LTc<3, 32>(P, st);
-   return setError(FMM_E_INVALID, "tensor-core M2L: the TF32 mode is not built");
+      return P.tcKChunk == 64 ? launchM2LTc<3, Layout<64>>(P, st) : launchM2LTc<3, Layout<32>>(P, st);
+   return launchM2LTc<1, tc::LayoutTf32>(P, st);
 }
 
 }  // namespace fmm

@@ -513,7 +513,7 @@ def main():
         del dJ, dx, g
 
     # the other M2L forms on the same workload (one warm-up and one timed solve each): the plain
-    # FP32 FMM (M2L on the CUDA cores) for the split-BF16 ratio, and the cheaper BF16X3 split
+    # FP32 FMM (M2L on the CUDA cores) for the split-BF16 ratio, the six-piece split and one TF32 pass
     def one_mode(mode):
         pplan = Plan(order=args.order, leaf_capacity=args.leaf, precision="fp32", m2l=mode, device=local)
         pplan.set_sources(d_xyz, d_w, d_J)
@@ -536,7 +536,7 @@ def main():
         return res
 
     if not args.no_plain:
-        for mode in ("simt", "bf16x3", "bf16x6"):
+        for mode in ("simt", "bf16x3", "bf16x6", "tf32"):
             if mode == m2l:
                 continue
             key = "plain_fp32" if mode == "simt" else f"m2l_{mode}"
