@@ -121,3 +121,49 @@ def torus_batch(n_coils=256, seed=20260004, count_range=(2 ** 12, 2 ** 18), targ
         so.append(so[-1] + len(w)); to.append(to[-1] + len(t))
     return (np.concatenate(xs), np.concatenate(ws), np.concatenate(Js), np.concatenate(ts),
             np.array(so, dtype=np.int64), np.array(to, dtype=np.int64))
+
+
+def hex_torus_tetrahedra(radius=2.0, section_width=0.2, n_length=20, n_width=4, n_height=4):
+    """The reference's tetrahedral torus (FMM/FMMGPU/torus.cpp:9-117): a torus of square cross-section
+    (side `section_width`, centre line of radius `radius`, axis z) cut into n_length x n_width x
+    n_height hexahedra - n_length steps around the axis (step angle 360 / n_length degrees with the
+    reference's PI literal), n_width radial steps and n_height steps in z - and each hexahedron into
+    five tetrahedra. Returns the vertices [T, 4, 3], hexahedra in (length, width, height) order."""
+    ref_pi = 3.14159265359
+    step = 360.0 / n_length * ref_pi / 180.0
+    r_in = radius - section_width / 2.0
+    bottom = -section_width / 2.0
+    dz = section_width / n_height
+    dw = section_width / n_width
+    tets = []
+    # vertex indices of the five tetrahedra of a hexahedron (torus.cpp:103-117)
+    split = ((0, 1, 3, 5), (0, 3, 5, 6), (0, 2, 3, 6), (0, 4, 5, 6), (3, 5, 6, 7))
+    for i in range(n_length):
+        a0 = np.array([r_in * np.cos(step * i), r_in * np.sin(step * i)])
+        a1 = np.array([r_in * np.cos(step * (i + 1)), r_in * np.sin(step * (i + 1))])
+        u0, u1 = a0 / np.linalg.norm(a0), a1 / np.linalg.norm(a1)
+        for j in range(n_width):
+            right, next_right = a0 + u0 * dw * j, a0 + u0 * dw * (j + 1)
+            left, next_left = a1 + u1 * dw * j, a1 + u1 * dw * (j + 1)
+            for k in range(n_height):
+                zb, zt = bottom + dz * k, bottom + dz * (k + 1)
+                pts = np.array([[*right, zb], [*next_right, zb], [*left, zb], [*next_left, zb],
+                                [*right, zt], [*next_right, zt], [*left, zt], [*next_left, zt]])
+                tets.extend(pts[list(s)] for s in split)
+    return np.array(tets)
+
+
+def tetra_quadratures(tets, rule_x, rule_w):
+    """Quadrature points and weights of tetrahedra [T, 4, 3] for a basis rule on the unit tetrahedron
+    (rule_x [K, 3] local coordinates, rule_w [K] weights summing to 1), as the reference maps them
+    (integration.cpp:34-42,163-187): x = a + (b - a) u + (c - a) v + (d - a) w, weight = volume x w_i.
+    Returns xyz [T K, 3] and w [T K], tetrahedron-major."""
+    tets = np.asarray(tets, dtype=np.float64)
+    rx = np.asarray(rule_x, dtype=np.float64)
+    rw = np.asarray(rule_w, dtype=np.float64)
+    a, b, c, d = tets[:, 0], tets[:, 1], tets[:, 2], tets[:, 3]
+    vol = np.abs(np.einsum("ij,ij->i", a - d, np.cross(b - d, c - d))) / 6.0
+    xyz = a[:, None, :] + (b - a)[:, None, :] * rx[None, :, 0:1] + (c - a)[:, None, :] * rx[None, :, 1:2] \
+        + (d - a)[:, None, :] * rx[None, :, 2:3]
+    w = vol[:, None] * rw[None, :]
+    return xyz.reshape(-1, 3), w.reshape(-1)

@@ -234,6 +234,16 @@ class Reference:
         self.lib.ref_translate_all_matrix(len(a), p, _d(a), _d(_c64(b).reshape(L, L)), _d(out))
         return out
 
+    def torus_quadratures(self, radius, width, nL, nW, nH, rule_x, rule_w):
+        """Quadratures [K, 4] (x, y, z, weight) of the reference's tetrahedral torus and basis rule files."""
+        f = self.lib.ref_torus_quadratures
+        f.restype = ctypes.c_int
+        args = (ctypes.c_double(radius), ctypes.c_double(width), nL, nW, nH, rule_x.encode(), rule_w.encode())
+        k = f(*args, None)
+        out = np.zeros((k, 4))
+        f(*args, _d(out))
+        return out
+
     def eval_local(self, p, local, d):
         out = np.zeros(3)
         self.lib.ref_eval_local(p, _d(_c64(local)), _d(_c64(d)), _d(out))

@@ -14,6 +14,7 @@
 //   mult(local, regular) (A from a local expansion)                       calculation_point_octree.cpp:192-212
 //   math::calcBioSavartLaplace (direct sum)                               integration.cpp:101-120
 //   kernels::translateAllCPU, translateAllCPUMatrixBLAS                   translation_algorithms_cpu.cpp:9-135
+//   Torus (hexahedra -> 5 tetrahedra) + math::tetrahedraToQuadratures     torus.cpp:9-117, integration.cpp:163-187
 //   FastMultipoleSolver full B / A pipeline                               fast_multipole_solver.cpp:12-231
 #include <chrono>
 #include <cstdint>
@@ -27,6 +28,8 @@
 #include "integration.hpp"
 #include "multipole_translator.hpp"
 #include "translation_algorithms.hpp"
+#include "torus.hpp"
+#include "basis_quadratures.hpp"
 
 namespace {
 HarmonicSeries<Vector3> toSeries(int order, const double* in)
@@ -141,6 +144,24 @@ void ref_translate_all_matrix(int count, int order, const double* a, const doubl
    std::vector<real> ar(a, a + L * count), br(b, b + L * L), res(L * count);
    kernels::translateAllCPUMatrixBLAS(res.data(), ar.data(), br.data(), size_t(count), size_t(order));
    for(size_t i = 0; i < L * count; i++) result[i] = res[i];
+}
+
+// The reference's tetrahedral torus quadratures (Torus(radius, width, nL, nW, nH) split into
+// tetrahedra, each carrying the basis rule read from the two text files): xyzw[4 k], k = number of
+// tetrahedra x rule points. Returns k; with out == nullptr only counts.
+int ref_torus_quadratures(double radius, double width, int nL, int nW, int nH, const char* ruleX, const char* ruleW,
+                          double* out)
+{
+   Torus torus(real(radius), real(width), nL, nW, nH);
+   BasisQuadratures bq;
+   bq.initFromTXT(ruleX, ruleW);
+   auto q = math::tetrahedraToQuadratures(torus.tetrahedra, bq);
+   if(out)
+      for(size_t i = 0; i < q.size(); i++)
+      {
+         out[4 * i] = q[i].x; out[4 * i + 1] = q[i].y; out[4 * i + 2] = q[i].z; out[4 * i + 3] = q[i].weight;
+      }
+   return int(q.size());
 }
 
 // A(x) = sum_k local_k * R_k(d), d = x - center (no 1/(4 pi) or current factor).

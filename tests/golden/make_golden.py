@@ -4,7 +4,8 @@ Runs the patched reference build (oracle/_ref/libref_fmm_*.so, made by oracle/re
 from the reference sources) on seeded inputs and stores inputs and outputs as .npz. The
 reference is not needed afterwards: the tests read only the .npz files.
 
-Usage: python tests/golden/make_golden.py [main] [seam]   (default: all)
+Usage: python tests/golden/make_golden.py [main] [seam] [telma]   (default: all)
+The reference sources are read from REFERENCE_ROOT (default /root/reference).
 """
 import os
 import sys
@@ -12,6 +13,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
 sys.path.insert(0, os.path.join(HERE, "..", ".."))
 from oracle.oracle import Reference  # noqa: E402
 from bachelors_b200 import geometry  # noqa: E402
@@ -89,8 +91,44 @@ def seam():
     print("wrote", path, len(out), "arrays")
 
 
+def read_telma(path):
+    """FMM/FMMGPU/results/telma_results.txt: a header line, the point count, then per point an
+    index, x, y, z and the external H field computed by the Telma program (read as in
+    FMM/FMMGPU/main.cpp:28-48)."""
+    with open(path) as f:
+        tok = f.read().split()
+    n = int(float(tok[3]))
+    vals = np.array([float(v) for v in tok[4:4 + 7 * n]]).reshape(n, 7)
+    return vals[:, 1:4], vals[:, 4:7]
+
+
+def telma():
+    """The reference's known-answer case (FMM/FMMGPU/main.cpp:50-134): the field of createTorus()
+    (R 2, section 0.2, 20 x 4 x 4 hexahedra, 5 tetrahedra each, the 24-point Keast rule of
+    basis_quadratures/keast 7 *.txt) at the 100 points of results/telma_results.txt, where Telma's
+    H (times MU0) is the comparison value, with current 5."""
+    ref_dir = os.path.join(REF_ROOT, "FMM", "FMMGPU")
+    rule_x = os.path.join(ref_dir, "basis_quadratures", "keast 7 x.txt")
+    rule_w = os.path.join(ref_dir, "basis_quadratures", "keast 7 w.txt")
+    pts, H = read_telma(os.path.join(ref_dir, "results", "telma_results.txt"))
+    ref = Reference("f64", 10)
+    q = ref.torus_quadratures(2.0, 0.2, 20, 4, 4, rule_x, rule_w)
+    out = {
+        "rule_x": np.loadtxt(rule_x), "rule_w": np.loadtxt(rule_w),
+        "telma_points": pts, "telma_H": H,
+        "quad_sample_index": np.arange(0, len(q), 37), "quad_sample": q[::37],
+        "quad_count": np.array(len(q)), "quad_sums": q.sum(axis=0),
+        "direct_B_current5": ref.direct_B(q, pts, 5.0),
+    }
+    path = os.path.join(HERE, "reference_telma.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, len(out), "arrays")
+
+
 if __name__ == "__main__":
-    what = sys.argv[1:] or ["main", "seam"]
+    what = sys.argv[1:] or ["main", "seam", "telma"]
+    if "telma" in what:
+        telma()
     if "main" in what:
         main()
     if "seam" in what:
