@@ -73,13 +73,21 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The maximum of x over the ranks (device times are reported as the slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(units_per_rank, ms_per_rank, world):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    ms = max_over_ranks(ms_per_rank, world)
+    return world * units_per_rank / (ms / 1000.0), ms
 
 
 class ClockSampler:
@@ -447,8 +455,7 @@ def main():
     barrier(world)
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1) / args.steps
-    ms_max = max_over_ranks(ms, world)
-    value = world * n / (ms_max / 1000.0)
+    value, ms_max = aggregate(n, ms, world)
 
     st = phase[-1]
     L = (args.order + 1) ** 2
