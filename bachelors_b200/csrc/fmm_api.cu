@@ -96,7 +96,7 @@ fmm_status Plan::init(const fmm_config& c)
    }
    if(const char* e = getenv("FMM_TC_KC")) tcKChunk = atoi(e) == 32 ? 32 : 64;
    if(const char* e = getenv("FMM_TC_DRAIN")) tcDrainEvery = std::max(1, atoi(e));
-   if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(2, std::max(0, atoi(e)));
+   if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(3, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
 
    FMM_TRY(rootb.reserve(sizeof(RootBox)));

@@ -144,7 +144,8 @@ struct Plan
    int tcKChunk = 0;                     // K chunk width 32 or 64 (0: 64 for BF16X3, 32 for BF16X6)
    int tcDrainEvery = 8;                 // offsets accumulated in tensor memory between drains (BF16X6,
                                          // with twice the accumulations per offset, drains twice as often)
-   int tcDrainMode = 2;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1
+   int tcDrainMode = 3;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1,
+                                         // 3: as 2 with 32 more columns in the drain threads' registers
    int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length
    int nearTile = 256;                   // near-field source tile, points (128 or 256)
    int p2mChunk = 16;                    // P2M recurrence steps reduced per shared tile (16 or 32)

@@ -15,16 +15,18 @@
 // 2^-16 relative (BF16X6), or one TF32 product of operands rounded to 11 significant bits (TF32,
 // kind::tf32, 4-byte elements); all are accumulated in FP32 in tensor memory.
 //
-// Warp roles (448 threads):
+// Warp roles (576 threads):
 //   warp 0      TMEM allocation; lane 0 issues the tcgen05.mma instructions
 //   warp 1      lane 0 streams the pre-swizzled operator image with cp.async.bulk (no multicast)
 //   warps 2..9  gather the source rows, already split into bf16 pieces once per solve
 //               (kSplitMultipoles), with 16-byte cp.async copies into the swizzled K-major layout
-//   warps 10-13 drain: every few offsets tcgen05.ld the accumulator and add it to FP32 running
+//   warps 10-17 drain: every few offsets tcgen05.ld the accumulator and add it to FP32 running
 //               sums (the tensor-core accumulation truncates; long chains into one TMEM value lose
 //               accuracy), then release the accumulator for a fresh accumulation. The running sums
 //               live in the tensor-memory columns the accumulator leaves free (208 of 512 at
-//               p = 16, all of them at p <= 12), the rest in the local expansions in global memory
+//               p = 16, all of them at p <= 12), then (drainMode 3) 32 more in the drain threads'
+//               registers, the rest in the local expansions in global memory. Each TMEM lane
+//               quadrant has two drain warps, one per half of the columns
 // Stages hold one K chunk of every piece of A and of T_o; two stages rotate through mbarriers
 // (full: producers + bulk-copy bytes, empty: tcgen05.commit). Every wait is bounded by
 // a 2 s global-timer limit; on expiry the CTA records FMM timeout in the error word and stops.
@@ -42,7 +44,7 @@ constexpr int TT = 42;               // target boxes per tile
 constexpr int ROWS = 128;            // MMA M
 // (the K chunk width depends on the number of bf16 pieces, see Layout)
 constexpr int NPROD = 256;           // producer threads
-constexpr int NTHREADS = 448;
+constexpr int NTHREADS = 576;
 constexpr uint64_t TIMEOUT_NS = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
@@ -330,8 +332,9 @@ __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int 
    }
 }
 
+// 18 warps: five of them share one SM sub-partition's 16K registers, so 96 per thread at most.
 template <int NP, class Lay>
-__global__ void __launch_bounds__(tc::NTHREADS, 1)
+__global__ void __maxnreg__(96)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int L, int Lp, int nChunks,
        const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc, int drainEvery,
        int nStages, int drainMode, const M2LCols cols, unsigned long long* counters, int* err)
@@ -387,7 +390,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       }
       mbarInit(doneBar, 1);
       mbarInit(drainFull, 1);
-      mbarInit(drainEmpty, 128);
+      mbarInit(drainEmpty, 256);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
    if(warp == 0)
@@ -527,31 +530,47 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    }
    else if(warp >= 10)
    {
-      // drain warps 10..13: TMEM lanes 32 (warp % 4) .. + 31, one accumulator row per thread
+      // drain warps 10..17: warp w reads TMEM lanes 32 (w % 4) .. + 31 (one accumulator row per
+      // thread) and half of the columns of every part below (warps 10-13 the first half)
       const int lanes = 32 * (warp & 3);
+      const int half = (warp - 10) >> 2;
       const int r = lanes + lane;
       const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
       float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
       const uint32_t tAcc = tmem + (uint32_t(lanes) << 16);
       const int nDrains = (nOff + drainEvery - 1) / drainEvery;
-      // The running sum is FP32, rounded to nearest, and has one writer per row (this thread); the
-      // locals start at zero and no other CTA touches these rows, so the result is deterministic.
-      //   drainMode 0: every drain adds into the locals with fire-and-forget vector atomics.
-      //   drainMode 1: the first drain stores, later ones load, add and store (prefetched).
-      //   drainMode 2: as 1, but the running sums of the first nS columns stay in the tensor memory
-      //                the accumulator leaves free (columns N .. 511); only the rest, and the final
-      //                result, travel to global memory.
-      const int nS = drainMode == 2 ? (min(N, 512 - N) & ~15) : 0;
-      const int cG = nS;                                         // first column kept in global memory
+      // The running sum is FP32, rounded to nearest, and has one writer per row and column (this
+      // thread); the locals start at zero and no other CTA touches these rows, so the result is
+      // deterministic. Its columns live in three parts:
+      //   [0, nS)    in the tensor memory the accumulator leaves free (columns N .. 511), drainMode >= 2
+      //   [nS, nR)   in this thread's registers (RHALF columns per half), drainMode 3
+      //   [nR, N)    in the local expansions: fire-and-forget vector atomics (drainMode 0) or
+      //              load-add-store, the first drain storing (drainMode >= 1)
+      constexpr int RHALF = 16;
+      const int nS = drainMode >= 2 ? (min(N, 512 - N) & ~15) : 0;
+      const int nR = drainMode == 3 ? min(N, nS + 2 * RHALF) : nS;
+      // [a, b) split at a multiple of 16 columns; this warp's half
+      auto split = [&](int a, int b, int& lo, int& hi) {
+         const int mid = min(b, a + ((((b - a) >> 1) + 15) & ~15));
+         lo = half ? mid : a;
+         hi = half ? b : mid;
+      };
+      int sLo, sHi, gLo, gHi;
+      split(0, nS, sLo, sHi);
+      const int rLo = nS + half * RHALF;
+      const int rHi = min(nR, rLo + RHALF);
+      split(nR, N, gLo, gHi);
       const uint32_t tSum = tAcc + uint32_t(N);
+      float rsum[RHALF];
+#pragma unroll
+      for(int i = 0; i < RHALF; i++) rsum[i] = 0.f;
       for(int d = 0; d < nDrains; d++)
       {
          if(!mbarWait(drainFull, d & 1, err, abortFlag)) break;
          fenceAfterSync();
          const bool last = d == nDrains - 1;
-         // running sums kept in tensor memory: S += acc (d > 0) or S = acc; the last drain writes
-         // S + acc to the locals instead
-         for(int c0 = 0; c0 < nS; c0 += 16)
+         // tensor-memory part: S += acc (d > 0) or S = acc; the last drain writes S + acc to the locals
+         for(int c0 = sLo; c0 < sHi; c0 += 16)
          {
             uint32_t a[16], sv[16];
             tmemLd16NoWait(tAcc + uint32_t(c0), a);
@@ -574,33 +593,40 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             else
                tmemSt16(tSum + uint32_t(c0), sv);
          }
-         if(nS > 0 && !last) tmemWaitSt();
-         // the remaining columns through global memory, 16 per step; with load-add-store the next
-         // step's running sums are loaded before this step's accumulator values are read
-         const bool rmw = drainMode != 0 && d > 0 && et >= 0;
-         float4 nxt[4];
-         if(rmw && cG < N)
-         {
-            const float4* o4 = reinterpret_cast<const float4*>(out + cG);
+         if(sHi > sLo && !last) tmemWaitSt();
+         // register part
 #pragma unroll
-            for(int i = 0; i < 4; i++) nxt[i] = o4[i];
+         for(int j = 0; j < RHALF / 16; j++)
+         {
+            const int c0 = rLo + 16 * j;
+            if(c0 >= rHi) break;
+            uint32_t a[16];
+            tmemLd16NoWait(tAcc + uint32_t(c0), a);
+            tmemWaitLd();
+#pragma unroll
+            for(int i = 0; i < 16; i++) rsum[16 * j + i] = (d > 0 ? rsum[16 * j + i] : 0.f) + __uint_as_float(a[i]);
+            if(last && et >= 0)
+            {
+               float4* o4 = reinterpret_cast<float4*>(out + c0);
+#pragma unroll
+               for(int i = 0; i < 4; i++)
+                  o4[i] = make_float4(rsum[16 * j + 4 * i], rsum[16 * j + 4 * i + 1], rsum[16 * j + 4 * i + 2],
+                                      rsum[16 * j + 4 * i + 3]);
+            }
          }
-         for(int c0 = cG; c0 < N; c0 += 16)
+         // global part, 16 columns per step; the running sums load while the accumulator does
+         const bool rmw = drainMode != 0 && d > 0 && et >= 0;
+         for(int c0 = gLo; c0 < gHi; c0 += 16)
          {
             uint32_t u[16];
             float4 old[4];
             float4* o4 = reinterpret_cast<float4*>(out + c0);
+            tmemLd16NoWait(tAcc + uint32_t(c0), u);
             if(rmw)
             {
 #pragma unroll
-               for(int i = 0; i < 4; i++) old[i] = nxt[i];
-               if(c0 + 16 < N)
-               {
-#pragma unroll
-                  for(int i = 0; i < 4; i++) nxt[i] = o4[4 + i];
-               }
+               for(int i = 0; i < 4; i++) old[i] = o4[i];
             }
-            tmemLd16NoWait(tAcc + uint32_t(c0), u);
             tmemWaitLd();
             if(et < 0) continue;
 #pragma unroll
