@@ -528,8 +528,8 @@ fmm_status fmm_set_tuning(fmm_plan* plan, const fmm_tuning* in)
 {
    if(!plan || !in) return setError(FMM_E_INVALID, "null argument");
    if((in->m2l_k_chunk != 32 && in->m2l_k_chunk != 64) || (in->near_tile != 128 && in->near_tile != 256) ||
-      (in->p2m_chunk != 16 && in->p2m_chunk != 32))
-      return setError(FMM_E_INVALID, "fmm_set_tuning: m2l_k_chunk 32|64, near_tile 128|256, p2m_chunk 16|32");
+      (in->p2m_chunk != 0 && in->p2m_chunk != 16 && in->p2m_chunk != 32))
+      return setError(FMM_E_INVALID, "fmm_set_tuning: m2l_k_chunk 32|64, near_tile 128|256, p2m_chunk 0|16|32");
    Plan& P = plan->P;
    P.tcKChunk = in->m2l_k_chunk;
    P.nearTile = in->near_tile;
@@ -579,9 +579,9 @@ fmm_status fmm_autotune(fmm_plan* plan, fmm_tuning* out, void* stream)
    {
       s = P.outB.reserve(es * 3 * std::max<int64_t>(P.m, 1));
       if(s != FMM_OK) break;
-      // P2M chunk
+      // P2M variant
       double bestMs = 1e300;
-      for(int cv : {16, 32})
+      for(int cv : {0, 16, 32})
       {
          P.p2mChunk = cv;
          double ms;

@@ -148,7 +148,8 @@ struct Plan
                                          // 3: as 2 with 32 more columns in the drain threads' registers
    int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length
    int nearTile = 256;                   // near-field source tile, points (128 or 256)
-   int p2mChunk = 16;                    // P2M recurrence steps reduced per shared tile (16 or 32)
+   int p2mChunk = 0;                     // P2M: 0 one warp per leaf; 16 or 32: one block per leaf, that many
+                                         // recurrence steps reduced per shared tile
    DevBuf tcCounters;                    // [items, tile-offset pairs] of the last tensor-core M2L
    int64_t tcTiles = 0;
    int opImgOrder = -1;                  // order the tensor-core operator image was built for

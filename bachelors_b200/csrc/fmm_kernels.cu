@@ -527,6 +527,156 @@ __global__ void __launch_bounds__(NT) kP2M(Tree t, const RootBox* __restrict__ r
 }
 
 // ====================================================================================
+// P2M, one warp per leaf. Lane (u, c), u < U = p / 2 + 1, c < 3, owns component c of the
+// complex coefficients S_l^m of the two orders m_a = u and m_b = p - u (p + 2 values; p / 2 + 1
+// when m_a = m_b), so the U units cover every order once and the 3 U <= 27 lanes have equal
+// work. The leaf's points go 32 at a time: lane j scales point j to the box and writes its
+// diagonal values S_m^m (m = 0..p, the recurrence's first step) to shared memory; then every lane
+// walks the points in order, running the l-recurrence of m_a and then of m_b and adding
+// q_c S_l^m into registers. Step j of a lane uses the coefficients (a, b, e) of its table row:
+//   S_j = a z S_{j-1} - b r^2 S_{j-2} + e S_{m_b}^{m_b}
+// with e = 1, a = b = 0 at the step that starts the m_b chain and b = 0 at the first step of
+// each chain, so no lane branches. At the end the real coefficients (-1)^l sqrt2 (Re, Im) S_l^m
+// (m > 0) and (-1)^l S_l^0 go through shared memory to one coalesced store of the leaf's
+// multipole.
+// ====================================================================================
+constexpr int P2MW_WARPS = 4;
+constexpr int P2MW_STEPS = MAXORDER + 2;
+
+template <class T>
+inline size_t p2mWarpSmem(int p, int Lp)
+{
+   const size_t perWarp = 32 * 8 + std::max<size_t>(size_t(32) * 2 * (p + 1), size_t(3) * Lp);
+   return sizeof(T) * (size_t(P2MW_STEPS) * 32 * 4 + P2MW_WARPS * perWarp);
+}
+
+template <class T>
+__global__ void __launch_bounds__(32 * P2MW_WARPS) kP2MWarp(Tree t, const RootBox* __restrict__ rootp,
+                                                          const typename Vec4<T>::type* __restrict__ pos,
+                                                          const typename Vec4<T>::type* __restrict__ q, int p,
+                                                          int Lp, T* __restrict__ M)
+{
+   typedef typename Vec4<T>::type V4;
+   extern __shared__ __align__(16) unsigned char smraw[];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int U = p / 2 + 1;
+   // the step table, [step][lane] (a, b, e, 0)
+   V4* AB = (V4*)smraw;
+   const size_t perWarp = 32 * 8 + max(32 * 2 * (p + 1), 3 * Lp);
+   T* Pt = (T*)(AB + P2MW_STEPS * 32) + warp * perWarp;   // [32][8] point: u, r^2, q
+   T* Ds = Pt + 32 * 8;                                  // [32][p + 1] (re, im) of S_m^m; later [3][Lp]
+   const int u = lane % U, c = min(lane / U, 2);
+   const int ma = u, mb = p - u;
+   const int na = p + 1 - ma;                            // terms of the m_a chain
+   for(int e = threadIdx.x; e < P2MW_STEPS * 32; e += 32 * P2MW_WARPS)
+   {
+      const int j = e / 32, ln = e % 32;
+      const int uu = ln % U;
+      const int a0 = uu, b0 = p - uu, n0 = p + 1 - a0;
+      const int n = n0 + (b0 != a0 ? p + 1 - b0 : 0);
+      T a = T(0), b = T(0), ee = T(0);
+      if(j == n0 && j < n) ee = T(1);
+      else if(j > 0 && j < n)
+      {
+         const int m = j < n0 ? a0 : b0;
+         const int l = j < n0 ? a0 + j - 1 : b0 + (j - n0) - 1;
+         const T inv = T(1) / T((l - m + 1) * (l + m + 1));
+         a = T(2 * l + 1) * inv;
+         b = l == m ? T(0) : inv;
+      }
+      AB[e] = V4{a, b, ee, T(0)};
+   }
+   __syncthreads();
+   const int node = blockIdx.x * P2MW_WARPS + warp;
+   if(node >= t.nNodes || t.nchild[node] != 0) return;
+   const int s0 = t.s0[node], s1 = t.s1[node];
+   if(s1 == s0) return;
+   const RootBox rb = rootp[rootOf(t, node)];
+   double cen[3], h;
+   nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], cen, h);
+   const double ih = 1.0 / h;
+   T accR[P2MW_STEPS], accI[P2MW_STEPS];
+#pragma unroll
+   for(int j = 0; j < P2MW_STEPS; j++) { accR[j] = T(0); accI[j] = T(0); }
+   for(int base = s0; base < s1; base += 32)
+   {
+      const int cnt = min(32, s1 - base);
+      if(lane < cnt)
+      {
+         const V4 xp = pos[base + lane], w = q[base + lane];
+         const T x = T((double(xp.x) - cen[0]) * ih), y = T((double(xp.y) - cen[1]) * ih),
+                 z = T((double(xp.z) - cen[2]) * ih);
+         T* pt = Pt + lane * 8;
+         pt[0] = x; pt[1] = y; pt[2] = z; pt[3] = x * x + y * y + z * z;
+         pt[4] = w.x; pt[5] = w.y; pt[6] = w.z;
+         T dre = T(1), dim = T(0);
+         T* d = Ds + lane * 2 * (p + 1);
+         d[0] = dre; d[1] = dim;
+         for(int m = 1; m <= p; m++)
+         {
+            const T sc = T(1) / T(2 * m);
+            const T nre = (dre * x - dim * y) * sc;
+            const T nim = (dre * y + dim * x) * sc;
+            dre = nre; dim = nim;
+            d[2 * m] = dre; d[2 * m + 1] = dim;
+         }
+      }
+      __syncwarp();
+      for(int i = 0; i < cnt; i++)
+      {
+         const T* pt = Pt + i * 8;
+         const T z = pt[2], r2 = pt[3], qc = pt[4 + c];
+         const T* d = Ds + i * 2 * (p + 1);
+         T are = d[2 * ma], aim = d[2 * ma + 1];
+         const T bdr = d[2 * mb], bdi = d[2 * mb + 1];
+         T bre = T(0), bim = T(0);
+         accR[0] += qc * are;
+         accI[0] += qc * aim;
+#pragma unroll
+         for(int j = 1; j < P2MW_STEPS; j++)
+         {
+            if(j > p + 1) break;
+            const V4 k = AB[j * 32 + lane];
+            const T az = k.x * z, br = k.y * r2;
+            const T cre = k.z * bdr + (az * are - br * bre);
+            const T cim = k.z * bdi + (az * aim - br * bim);
+            bre = are; bim = aim; are = cre; aim = cim;
+            accR[j] += qc * are;
+            accI[j] += qc * aim;
+         }
+      }
+      __syncwarp();
+   }
+   // real coefficients through shared memory, then one coalesced store
+   T* Mst = Ds;
+   for(int e = lane; e < 3 * Lp; e += 32)
+      if(e % Lp >= (p + 1) * (p + 1)) Mst[e] = T(0);
+   if(lane < 3 * U)
+   {
+      const int nb = mb != ma ? p + 1 - mb : 0;
+      const T sq2 = T(1.4142135623730950488);
+#pragma unroll
+      for(int j = 0; j < P2MW_STEPS; j++)
+      {
+         if(j >= na + nb) break;
+         const int m = j < na ? ma : mb;
+         const int l = j < na ? ma + j : mb + (j - na);
+         const T sg = (l & 1) ? T(-1) : T(1);
+         T* mc = Mst + c * Lp;
+         if(m == 0) mc[hidx(l, 0)] = sg * accR[j];
+         else
+         {
+            mc[hidx(l, m)] = sg * sq2 * accR[j];
+            mc[hidx(l, -m)] = sg * sq2 * accI[j];
+         }
+      }
+   }
+   __syncwarp();
+   T* out = M + int64_t(node) * 3 * Lp;
+   for(int e = lane; e < 3 * Lp; e += 32) out[e] = Mst[e];
+}
+
+// ====================================================================================
 // M2M, one level: one block per node of the level with children; the parent sums the
 // translated multipoles of its children. Output coefficient k of degree l only needs input
 // coefficients j < (l+1)^2.
@@ -620,8 +770,11 @@ __global__ void __launch_bounds__(256) kM2LSimt(const int* __restrict__ targets,
          const int r = e / ACH, q = e % ACH;
          const int t = tileNode[r / 3];
          const int src = t >= 0 ? vtab[int64_t(t) * 316 + o] : -1;
-         const T* g = M + (int64_t(src >= 0 ? src : 0) * 3 + r % 3) * Lp + k0 + q * (16 / int(sizeof(T)));
-         cpAsync16Simt(A + r * KC + q * (16 / int(sizeof(T))), g, src >= 0 ? 16u : 0u);
+         // K positions past the row (k0 + KC can exceed Lp) are zero-filled, never read
+         const int k = k0 + q * (16 / int(sizeof(T)));
+         const bool in = src >= 0 && k < Lp;
+         const T* g = M + (int64_t(in ? src : 0) * 3 + r % 3) * Lp + (in ? k : 0);
+         cpAsync16Simt(A + r * KC + q * (16 / int(sizeof(T))), g, in ? 16u : 0u);
       }
       constexpr int BCH = NCOL * int(sizeof(T)) / 16;        // 16-byte chunks per operator row
       const T* op = opw + int64_t(o) * L * Lp;
@@ -986,7 +1139,15 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
    typedef typename Vec4<T>::type V4;
    constexpr int NT = 64;
    const size_t shm = sizeof(T) * 3 * Lp;
-   if(P.p2mChunk == 32)
+   if(P.p2mChunk == 0)
+   {
+      const size_t shw = p2mWarpSmem<T>(P.p, Lp);
+      if(shw > 48 * 1024)
+         FMM_CUDA(cudaFuncSetAttribute(kP2MWarp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shw)));
+      kP2MWarp<T><<<int((N + P2MW_WARPS - 1) / P2MW_WARPS), 32 * P2MW_WARPS, shw, st>>>(
+         P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp, (T*)P.mult.ptr);
+   }
+   else if(P.p2mChunk == 32)
       kP2M<T, NT, 32><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
                                               (T*)P.mult.ptr);
    else

@@ -264,7 +264,7 @@ class Plan:
         _lib.check(self.lib.fmm_get_tuning(self.handle, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in _lib.FmmTuning._fields_[:3]}
 
-    def set_tuning(self, m2l_k_chunk=64, near_tile=256, p2m_chunk=16):
+    def set_tuning(self, m2l_k_chunk=64, near_tile=256, p2m_chunk=0):
         t = _lib.FmmTuning(int(m2l_k_chunk), int(near_tile), int(p2m_chunk), 0.0, 0.0, 0.0)
         _lib.check(self.lib.fmm_set_tuning(self.handle, ctypes.byref(t)))
 

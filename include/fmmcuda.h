@@ -169,7 +169,8 @@ fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* sr
 typedef struct fmm_tuning {
    int m2l_k_chunk;  /* tensor-core M2L: K chunk width, 64 (two 108 KB stages at p = 16) or 32 (four) */
    int near_tile;    /* near field: source points per shared-memory tile, 128 or 256 */
-   int p2m_chunk;    /* P2M: recurrence steps reduced per shared-memory tile, 16 or 32 */
+   int p2m_chunk;    /* P2M: 0 = one warp per leaf (lanes own harmonic orders); 16 or 32 = one block
+                        per leaf, that many recurrence steps reduced per shared-memory tile */
    double ms_upward, ms_downward, ms_near; /* fmm_autotune: the chosen variants' times */
 } fmm_tuning;
 
