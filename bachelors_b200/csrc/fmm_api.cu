@@ -98,6 +98,7 @@ fmm_status Plan::init(const fmm_config& c)
    if(const char* e = getenv("FMM_TC_DRAIN")) tcDrainEvery = std::max(1, atoi(e));
    if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(3, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
+   if(const char* e = getenv("FMM_L2P_SPLIT")) l2pSplit = atoi(e) != 0;
 
    FMM_TRY(rootb.reserve(sizeof(RootBox)));
    FMM_TRY(errb.reserve(sizeof(int)));
@@ -121,7 +122,7 @@ void Plan::release()
    DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
                      &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &parList, &m2lTargets, &m2lKeys, &errb,
                      &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf, &multBf, &tcCounters,
-                     &adjG, &adjOut};
+                     &adjG, &adjOut, &nearCounts};
    for(DevBuf* b : bufs) b->release();
    for(auto& b : nodeBufs) b.release();
    for(auto& b : listBufs) b.release();
@@ -792,6 +793,15 @@ fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats)
    s.levels = P.tree.nLevels;
    s.p2p_pairs = P.nP2P;
    s.v_pairs = P.nV;
+   if(P.treeReady && P.nearCounts.ptr)
+   {
+      unsigned long long c[2] = {0, 0};
+      if(cudaMemcpy(c, P.nearCounts.ptr, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess)
+      {
+         s.leaves = int64_t(c[0]);
+         s.p2p_interactions = int64_t(c[1]);
+      }
+   }
    s.n_sources = P.n;
    s.n_targets = P.m;
    s.coils = P.nCoils;

@@ -876,13 +876,177 @@ __device__ inline T gradCoeff(const T* Lv, int j, int lp, int mu)
    return h * coefAt(Lv, l, 1 - mu) + h * coefAt(Lv, l, -mu - 1);
 }
 
+// L2P alone, one warp per target leaf, one target per lane (32 at a time). The leaf's curl
+// expansion (and, for A, its local expansion) is stored as [k] (x, y, z, 0) with the real-basis
+// factors (-1)^l sqrt2 folded in, so each visited harmonic costs one broadcast 16-byte shared
+// load and three FMAs per coefficient. The recurrence's coefficients come from a table shared by
+// the block (visit order: m outer, l inner): 1/(2m) at l = m, else the (a, b) of
+// S_l^m = a z S_{l-1}^m - b r^2 S_{l-2}^m, so no lane divides. The far field is written to the
+// outputs unscaled; kL2PNear<..., FAR = false> adds the near field and applies the scale.
+constexpr int L2PW_WARPS = 4;
+
+template <class T, bool WANTA>
+inline size_t l2pWarpSmem(int p)
+{
+   const int L = nharm(p), Lb = nharm(p - 1), nV = (p + 1) * (p + 2) / 2;
+   const size_t perWarp = size_t(4) * Lb + (WANTA ? size_t(4) * L : 0) + ((size_t(3) * L + 3) & ~size_t(3));
+   return sizeof(T) * (size_t(4) * nV + L2PW_WARPS * perWarp);
+}
+
+template <class T, bool WANTA>
+__global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBox* __restrict__ rootp, int p,
+                                                          int Lp, const T* __restrict__ Lc,
+                                                          const typename Vec4<T>::type* __restrict__ tpos,
+                                                          const int* __restrict__ tOrder, int want,
+                                                          T* __restrict__ outB, T* __restrict__ outA)
+{
+   typedef typename Vec4<T>::type V4;
+   extern __shared__ __align__(16) unsigned char smraw[];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int L = nharm(p), Lb = nharm(p - 1);
+   const int q = WANTA ? p : p - 1;                     // highest degree visited
+   const int nV = (p + 1) * (p + 2) / 2;                // table: degrees 0..p
+   V4* tab = (V4*)smraw;
+   const int perWarp = 4 * Lb + (WANTA ? 4 * L : 0) + ((3 * L + 3) & ~3);
+   T* wbase = (T*)(tab + nV) + warp * perWarp;
+   V4* Cs = (V4*)wbase;                                 // [Lb] curl expansion
+   V4* As = Cs + Lb;                                    // [L] local expansion (WANTA)
+   T* Ls = wbase + 4 * Lb + (WANTA ? 4 * L : 0);        // [3][L] local expansion as stored
+   for(int v = threadIdx.x; v < nV; v += 32 * L2PW_WARPS)
+   {
+      int m = 0, r = v;
+      while(r >= p + 1 - m) { r -= p + 1 - m; m++; }
+      const int l = m + r;
+      T a = T(0), b = T(0);
+      if(l == m) a = m > 0 ? T(1) / T(2 * m) : T(1);
+      else
+      {
+         const int lp = l - 1;
+         const T inv = T(1) / T((lp - m + 1) * (lp + m + 1));
+         a = T(2 * lp + 1) * inv;
+         b = lp == m ? T(0) : inv;
+      }
+      tab[v] = V4{a, b, T(0), T(0)};
+   }
+   __syncthreads();
+   const int node = blockIdx.x * L2PW_WARPS + warp;
+   if(node >= t.nNodes || t.nchild[node] != 0) return;
+   const int t0 = t.t0[node], t1 = t.t1[node];
+   if(t1 == t0) return;
+   const T* lc = Lc + int64_t(node) * 3 * Lp;
+   for(int e = lane; e < 3 * L; e += 32) Ls[e] = lc[(e / L) * Lp + e % L];
+   __syncwarp();
+   const T sq2 = T(1.4142135623730950488);
+   auto degreeOf = [](int k) {
+      int l = int(sqrtf(float(k)));
+      while(l * l > k) l--;
+      while((l + 1) * (l + 1) <= k) l++;
+      return l;
+   };
+   for(int e = lane; e < 3 * Lb; e += 32)
+   {
+      const int c = e / Lb, k = e % Lb;
+      const int lp = degreeOf(k), mu = k - lp * lp - lp;
+      const T f = ((lp & 1) ? T(-1) : T(1)) * (mu != 0 ? sq2 : T(1));
+      // B_x = dAz/dy - dAy/dz, B_y = dAx/dz - dAz/dx, B_z = dAy/dx - dAx/dy
+      const int cp = (c + 2) % 3, cm = (c + 1) % 3;
+      const int jp = (c + 1) % 3, jm = (c + 2) % 3;
+      T* cs = (T*)(Cs + k);
+      cs[c] = f * (gradCoeff(Ls + cp * L, jp, lp, mu) - gradCoeff(Ls + cm * L, jm, lp, mu));
+      if(c == 0) cs[3] = T(0);
+   }
+   if(WANTA)
+      for(int e = lane; e < 3 * L; e += 32)
+      {
+         const int c = e / L, k = e % L;
+         const int l = degreeOf(k), mu = k - l * l - l;
+         const T f = ((l & 1) ? T(-1) : T(1)) * (mu != 0 ? sq2 : T(1));
+         T* as = (T*)(As + k);
+         as[c] = f * Ls[e];
+         if(c == 0) as[3] = T(0);
+      }
+   __syncwarp();
+   const RootBox rb = rootp[rootOf(t, node)];
+   double cen[3], h;
+   nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], cen, h);
+   const T ih = T(1.0 / h), ih2 = T(1.0 / (h * h));
+   for(int base = t0; base < t1; base += 32)
+   {
+      const int ti = base + lane;
+      const bool act = ti < t1;
+      const V4 x = act ? tpos[ti] : V4{T(0), T(0), T(0), T(0)};
+      const T ux = T((double(x.x) - cen[0]) / h), uy = T((double(x.y) - cen[1]) / h),
+              uz = T((double(x.z) - cen[2]) / h);
+      const T r2 = ux * ux + uy * uy + uz * uz;
+      T B0 = T(0), B1 = T(0), B2 = T(0), A0 = T(0), A1 = T(0), A2 = T(0);
+      T dre = T(1), dim = T(0);   // S_m^m
+      int v = 0;
+      for(int m = 0; m <= q; m++)
+      {
+         if(m > 0)
+         {
+            const T sc = tab[v].x;
+            const T nre = (dre * ux - dim * uy) * sc;
+            const T nim = (dre * uy + dim * ux) * sc;
+            dre = nre; dim = nim;
+         }
+         T are = dre, aim = dim, bre = T(0), bim = T(0);
+         int k0 = m * m + 2 * m, k1 = m * m;   // hidx(l, m), hidx(l, -m) at l = m
+         for(int l = m; l <= q; l++, v++)
+         {
+            if(l > m)
+            {
+               const V4 ab = tab[v];
+               const T cre = ab.x * uz * are - ab.y * r2 * bre;
+               const T cim = ab.x * uz * aim - ab.y * r2 * bim;
+               bre = are; bim = aim; are = cre; aim = cim;
+               k0 += 2 * l; k1 += 2 * l;
+            }
+            if(!WANTA || l < p)
+            {
+               const V4 c0 = Cs[k0];
+               B0 += c0.x * are; B1 += c0.y * are; B2 += c0.z * are;
+               if(m > 0)
+               {
+                  const V4 c1 = Cs[k1];
+                  B0 += c1.x * aim; B1 += c1.y * aim; B2 += c1.z * aim;
+               }
+            }
+            if(WANTA)
+            {
+               const V4 a0 = As[k0];
+               A0 += a0.x * are; A1 += a0.y * are; A2 += a0.z * are;
+               if(m > 0)
+               {
+                  const V4 a1 = As[k1];
+                  A0 += a1.x * aim; A1 += a1.y * aim; A2 += a1.z * aim;
+               }
+            }
+         }
+         v += p - q;   // table entries of the degrees above q
+      }
+      if(act)
+      {
+         const int o = tOrder[ti];
+         if(want & 1)
+         {
+            outB[3 * int64_t(o)] = B0 * ih2; outB[3 * int64_t(o) + 1] = B1 * ih2; outB[3 * int64_t(o) + 2] = B2 * ih2;
+         }
+         if(WANTA)
+         {
+            outA[3 * int64_t(o)] = A0 * ih; outA[3 * int64_t(o) + 1] = A1 * ih; outA[3 * int64_t(o) + 2] = A2 * ih;
+         }
+      }
+   }
+}
+
 // L2P and the direct near field: one block of NT threads per target leaf. The far field comes from
 // the leaf's local expansion (analytic curl, one target per thread). The near field packs the
 // points of the leaf's direct-interaction source nodes into shared tiles of TS points; when the
 // leaf has fewer targets than threads, the G = NT / targets thread groups each take every G-th
 // source of a tile and their partial sums are added in a fixed order at the end. Each thread
 // sums one tile in T and the tile sums in FP64, so no single-precision chain is longer than a tile.
-template <class T, int NT, int TS, int NE, bool WANTA>
+template <class T, int NT, int TS, int NE, bool WANTA, bool FAR>
 __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict__ rootp, int p, int Lp,
                                                const T* __restrict__ Lc,
                                                const typename Vec4<T>::type* __restrict__ tpos,
@@ -901,8 +1065,8 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
    const int Lb = nharm(p - 1);
    T* Ls = (T*)smraw;          // [3][L] local
    T* Cs = Ls + 3 * L;         // [3][Lb] curl expansion
-   // source tiles start on a 32-byte boundary after the two coefficient arrays
-   const size_t coefBytes = (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31);
+   // source tiles start on a 32-byte boundary after the two coefficient arrays (none without FAR)
+   const size_t coefBytes = FAR ? (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31) : 0;
    V4* Sp = (V4*)(smraw + coefBytes);  // [TS] source positions
    V4* Sq = Sp + TS;                   // [TS] source strengths w J
    double* red = (double*)(Sq + TS);   // [6][NT] group partial sums
@@ -910,6 +1074,8 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
    __shared__ typename ScanT::TempStorage scanTmp;
    __shared__ int ePre[NE + 1];        // prefix sums of the batch's source counts
    __shared__ int eSrc[NE];            // first sorted source of each batch entry
+   if(FAR)
+   {
    for(int e = tid; e < 3 * L; e += NT) Ls[e] = Lc[int64_t(node) * 3 * Lp + (e / L) * Lp + e % L];
    __syncthreads();
    for(int e = tid; e < 3 * Lb; e += NT)
@@ -925,6 +1091,7 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
       Cs[e] = gradCoeff(Ls + cp * L, jp, lp, mu) - gradCoeff(Ls + cm * L, jm, lp, mu);
    }
    __syncthreads();
+   }
    const RootBox rb = rootp[rootOf(t, node)];
    double c[3], h;
    nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], c, h);
@@ -941,7 +1108,14 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
       const int ti = base + tt;
       V4 x = inGroup ? tpos[ti] : V4{T(0), T(0), T(0), T(0)};
       double Bd[3] = {0, 0, 0}, Ad[3] = {0, 0, 0};
-      if(inGroup && g == 0)
+      if(!FAR && inGroup && g == 0)
+      {
+         // the far field, already evaluated by kL2PWarp into the outputs (unscaled)
+         const int o = tOrder[ti];
+         if(want & 1) for(int d = 0; d < 3; d++) Bd[d] = double(outB[3 * int64_t(o) + d]);
+         if(WANTA) for(int d = 0; d < 3; d++) Ad[d] = double(outA[3 * int64_t(o) + d]);
+      }
+      if(FAR && inGroup && g == 0)
       {
          T B[3] = {T(0), T(0), T(0)}, A[3] = {T(0), T(0), T(0)};
          const T ux = T((double(x.x) - c[0]) / h), uy = T((double(x.y) - c[1]) / h), uz = T((double(x.z) - c[2]) / h);
@@ -1232,8 +1406,23 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
    const int L = P.L, Lb = nharm(P.p - 1);
    constexpr int NT = 64, NE = 128;
    const int TS = P.nearTile == 128 ? 128 : 256;
-   size_t shm = ((sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31)) + 2 * sizeof(V4) * TS + sizeof(double) * 6 * NT;
+   const bool split = P.l2pSplit != 0;
+   const size_t coef = split ? 0 : (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31);
+   size_t shm = coef + 2 * sizeof(V4) * TS + sizeof(double) * 6 * NT;
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
+   if(split)
+   {
+      auto runL2P = [&](auto kernel, size_t sh) -> fmm_status {
+         if(sh > 48 * 1024) FMM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh)));
+         kernel<<<int((N + L2PW_WARPS - 1) / L2PW_WARPS), 32 * L2PW_WARPS, sh, st>>>(
+            P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr, (const int*)P.tIdx.ptr, want,
+            (T*)P.outB.ptr, (T*)P.outA.ptr);
+         return FMM_OK;
+      };
+      if(want & 2) FMM_TRY(runL2P(kL2PWarp<T, true>, l2pWarpSmem<T, true>(P.p)));
+      else FMM_TRY(runL2P(kL2PWarp<T, false>, l2pWarpSmem<T, false>(P.p)));
+      FMM_TRY(launched(P, "kL2PWarp", st));
+   }
    auto run = [&](auto kernel) -> fmm_status {
       FMM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
       kernel<<<int(N), NT, shm, st>>>(P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr,
@@ -1242,15 +1431,28 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
                                       (T*)P.outB.ptr, (T*)P.outA.ptr);
       return FMM_OK;
    };
-   if(TS == 128)
+   if(split)
    {
-      if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 128, NE, true>));
-      else FMM_TRY(run(kL2PNear<T, NT, 128, NE, false>));
+      if(TS == 128)
+      {
+         if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 128, NE, true, false>));
+         else FMM_TRY(run(kL2PNear<T, NT, 128, NE, false, false>));
+      }
+      else
+      {
+         if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 256, NE, true, false>));
+         else FMM_TRY(run(kL2PNear<T, NT, 256, NE, false, false>));
+      }
+   }
+   else if(TS == 128)
+   {
+      if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 128, NE, true, true>));
+      else FMM_TRY(run(kL2PNear<T, NT, 128, NE, false, true>));
    }
    else
    {
-      if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 256, NE, true>));
-      else FMM_TRY(run(kL2PNear<T, NT, 256, NE, false>));
+      if(want & 2) FMM_TRY(run(kL2PNear<T, NT, 256, NE, true, true>));
+      else FMM_TRY(run(kL2PNear<T, NT, 256, NE, false, true>));
    }
    FMM_TRY(launched(P, "kL2PNear", st));
    FMM_CHECK_LAUNCH();

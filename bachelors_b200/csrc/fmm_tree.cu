@@ -365,6 +365,38 @@ __global__ void kListsLevel(Tree t, Lists L, int a, int b, int* err)
 }
 
 // Direct-interaction source nodes of every target leaf (count pass when out == nullptr).
+// Statistics of the finished tree: out[0] += leaves, out[1] += direct (target, source) pairs the near
+// field evaluates (targets of a leaf x points of its direct-list nodes, the self pairs included).
+__global__ void kNearCounts(Tree t, int nNodes, const int* __restrict__ off, const int* __restrict__ list,
+                            unsigned long long* out)
+{
+   unsigned long long leaves = 0, pairs = 0;
+   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < nNodes; n += gridDim.x * blockDim.x)
+   {
+      if(t.nchild[n] != 0) continue;
+      leaves++;
+      const int nt = t.t1[n] - t.t0[n];
+      if(nt == 0) continue;
+      long long ns = 0;
+      for(int e = off[n]; e < off[n + 1]; e++)
+      {
+         const int S = list[e];
+         ns += t.s1[S] - t.s0[S];
+      }
+      pairs += (unsigned long long)nt * (unsigned long long)ns;
+   }
+   for(int d = 16; d > 0; d >>= 1)
+   {
+      leaves += __shfl_down_sync(0xffffffffu, leaves, d);
+      pairs += __shfl_down_sync(0xffffffffu, pairs, d);
+   }
+   if((threadIdx.x & 31) == 0)
+   {
+      atomicAdd(out, leaves);
+      atomicAdd(out + 1, pairs);
+   }
+}
+
 __global__ void kP2PLists(Tree t, Lists L, int nNodes, const int* __restrict__ off, int* cnt, int* out, int* err)
 {
    int T = blockIdx.x * blockDim.x + threadIdx.x;
@@ -655,6 +687,11 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    FMM_CHECK_LAUNCH();
    P.nP2P = nP2P;
    P.nV = nV;
+   FMM_TRY(P.nearCounts.reserve(2 * sizeof(unsigned long long)));
+   FMM_CUDA(cudaMemsetAsync(P.nearCounts.ptr, 0, 2 * sizeof(unsigned long long), st));
+   kNearCounts<<<148 * 4, 256, 0, st>>>(t, nn, po, (const int*)P.p2pList.ptr, (unsigned long long*)P.nearCounts.ptr);
+   FMM_TRY(launched(P, "kNearCounts", st));
+   FMM_CHECK_LAUNCH();
    // parents per level for the M2M / L2L GEMMs
    {
       int* flags = (int*)P.lvlCnt.ptr;   // nn + 1 ints, free again once the direct lists are counted
