@@ -876,6 +876,59 @@ __device__ inline T gradCoeff(const T* Lv, int j, int lp, int mu)
    return h * coefAt(Lv, l, 1 - mu) + h * coefAt(Lv, l, -mu - 1);
 }
 
+// 1/sqrt(x) by the PTX approximate reciprocal square root (flushes subnormal inputs to zero).
+__device__ __forceinline__ float rsqrtApprox(float x)
+{
+   float y;
+   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+   return y;
+}
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two floats in one 64-bit register, low half first.
+typedef unsigned long long f2p;
+__device__ __forceinline__ f2p pk2(float a, float b)
+{
+   f2p r;
+   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+   return r;
+}
+__device__ __forceinline__ void upk2(f2p v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ f2p sub2(f2p a, f2p b)
+{
+   f2p d;
+   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+   return d;
+}
+__device__ __forceinline__ f2p mul2(f2p a, f2p b)
+{
+   f2p d;
+   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+   return d;
+}
+__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c)
+{
+   f2p d;
+   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+   return d;
+}
+__device__ __forceinline__ void cpAsync4(void* dst, const void* src, uint32_t srcBytes)
+{
+   const uint32_t d = uint32_t(__cvta_generic_to_shared(dst));
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(srcBytes) : "memory");
+}
+// Bytes of one near-field source tile of TS points: FP32 tiles hold source pairs
+// [x0 x1 y0 y1 z0 z1 wx0 wx1 wy0 wy1 wz0 wz1] (24 bytes a point), FP64 tiles two [TS] arrays of
+// (x, y, z, -) and (wx, wy, wz, -).
+template <class T>
+__host__ __device__ constexpr int nearTileBytes(int TS)
+{
+   return sizeof(T) == 4 ? 24 * TS : 2 * 4 * int(sizeof(T)) * TS;
+}
+
+// Largest 1/r whose cube is finite in T, for the coincident-pair cap of the near field.
+template <class T> __device__ __forceinline__ T riCap();
+template <> __device__ __forceinline__ float riCap<float>() { return 6.0e12f; }
+template <> __device__ __forceinline__ double riCap<double>() { return 1.0e100; }
+
 // L2P alone, one warp per target leaf, one target per lane (32 at a time). The leaf's curl
 // expansion (and, for A, its local expansion) is stored as [k] (x, y, z, 0) with the real-basis
 // factors (-1)^l sqrt2 folded in, so each visited harmonic costs one broadcast 16-byte shared
@@ -1047,7 +1100,7 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
 // source of a tile and their partial sums are added in a fixed order at the end. Each thread
 // sums one tile in T and the tile sums in FP64, so no single-precision chain is longer than a tile.
 template <class T, int NT, int TS, int NE, bool WANTA, bool FAR>
-__global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict__ rootp, int p, int Lp,
+__global__ void __launch_bounds__(NT, FAR ? 1 : (sizeof(T) == 4 ? (WANTA ? 12 : 16) : 8)) kL2PNear(Tree t, const RootBox* __restrict__ rootp, int p, int Lp,
                                                const T* __restrict__ Lc,
                                                const typename Vec4<T>::type* __restrict__ tpos,
                                                const typename Vec4<T>::type* __restrict__ spos,
@@ -1067,9 +1120,8 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
    T* Cs = Ls + 3 * L;         // [3][Lb] curl expansion
    // source tiles start on a 32-byte boundary after the two coefficient arrays (none without FAR)
    const size_t coefBytes = FAR ? (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31) : 0;
-   V4* Sp = (V4*)(smraw + coefBytes);  // [TS] source positions
-   V4* Sq = Sp + TS;                   // [TS] source strengths w J
-   double* red = (double*)(Sq + TS);   // [6][NT] group partial sums
+   unsigned char* tiles = smraw + coefBytes;                          // two source tiles
+   double* red = (double*)(tiles + 2 * nearTileBytes<T>(TS));        // [6][NT] group partial sums
    typedef cub::BlockScan<int, NT> ScanT;
    __shared__ typename ScanT::TempStorage scanTmp;
    __shared__ int ePre[NE + 1];        // prefix sums of the batch's source counts
@@ -1147,24 +1199,82 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
          for(int d = 0; d < 3; d++) { Bd[d] = double(B[d] * ih2); Ad[d] = double(A[d] * ih); }
       }
       // near field over packed tiles of the direct-list source nodes
-      auto tileSum = [&](int n) {
+      auto tileSum = [&](int n, int b) {
          if(!inGroup) return;
          T pb[3] = {T(0), T(0), T(0)}, pa[3] = {T(0), T(0), T(0)};
-#pragma unroll 4
-         for(int i = g; i < n; i += G)
+         if constexpr(sizeof(T) == 4)
          {
-            const V4 y = Sp[i], w = Sq[i];
-            const T dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
-            const T r2 = dx * dx + dy * dy + dz * dz;
-            T ri;
-            if constexpr(sizeof(T) == 4) ri = rsqrtf(r2);
-            else ri = rsqrt(r2);
-            ri = r2 > T(0) ? ri : T(0);   // coincident pair (the target itself): no contribution
-            const T ri3 = ri * ri * ri;
-            pb[0] += (w.y * dz - w.z * dy) * ri3;
-            pb[1] += (w.z * dx - w.x * dz) * ri3;
-            pb[2] += (w.x * dy - w.y * dx) * ri3;
-            if(wantA) { pa[0] += w.x * ri; pa[1] += w.y * ri; pa[2] += w.z * ri; }
+            // two sources per step in packed f32x2 arithmetic; the cross product's two products are
+            // accumulated in separate sums (no negation in the packed FMA)
+            const ulonglong2* tq = (const ulonglong2*)(tiles + b * nearTileBytes<T>(TS));
+            const int nPairs = (n + 1) >> 1;
+            const f2p X = pk2(x.x, x.x), Y = pk2(x.y, x.y), Z = pk2(x.z, x.z);
+            f2p sxp = 0, sxn = 0, syp = 0, syn = 0, szp = 0, szn = 0, ax = 0, ay = 0, az = 0;
+#pragma unroll 2
+            for(int P = g; P < nPairs; P += G)
+            {
+               const ulonglong2 q0 = tq[3 * P], q1 = tq[3 * P + 1], q2 = tq[3 * P + 2];
+               const f2p DX = sub2(X, q0.x), DY = sub2(Y, q0.y), DZ = sub2(Z, q1.x);
+               f2p R2 = mul2(DX, DX);
+               R2 = fma2(DY, DY, R2);
+               R2 = fma2(DZ, DZ, R2);
+               float r2a, r2b;
+               upk2(R2, r2a, r2b);
+               float ria = rsqrtApprox(r2a), rib = rsqrtApprox(r2b);
+               // coincident pair (the target itself) and the empty slot of an odd tile: no
+               // contribution. For B the capped 1/r (whose cube still fits a float) meets a zero
+               // difference vector or a zero weight; A needs the explicit test.
+               if constexpr(WANTA)
+               {
+                  ria = r2a > 0.f ? ria : 0.f;
+                  rib = r2b > 0.f ? rib : 0.f;
+               }
+               else
+               {
+                  ria = fminf(ria, riCap<float>());
+                  rib = fminf(rib, riCap<float>());
+               }
+               const f2p RI = pk2(ria, rib);
+               const f2p RI3 = mul2(mul2(RI, RI), RI);
+               const f2p UX = mul2(q1.y, RI3), UY = mul2(q2.x, RI3), UZ = mul2(q2.y, RI3);
+               sxp = fma2(UY, DZ, sxp); sxn = fma2(UZ, DY, sxn);
+               syp = fma2(UZ, DX, syp); syn = fma2(UX, DZ, syn);
+               szp = fma2(UX, DY, szp); szn = fma2(UY, DX, szn);
+               if constexpr(WANTA)
+               {
+                  ax = fma2(q1.y, RI, ax); ay = fma2(q2.x, RI, ay); az = fma2(q2.y, RI, az);
+               }
+            }
+            float u0, u1, v0, v1;
+            upk2(sxp, u0, u1); upk2(sxn, v0, v1); pb[0] = (u0 + u1) - (v0 + v1);
+            upk2(syp, u0, u1); upk2(syn, v0, v1); pb[1] = (u0 + u1) - (v0 + v1);
+            upk2(szp, u0, u1); upk2(szn, v0, v1); pb[2] = (u0 + u1) - (v0 + v1);
+            if constexpr(WANTA)
+            {
+               upk2(ax, u0, u1); pa[0] = u0 + u1;
+               upk2(ay, u0, u1); pa[1] = u0 + u1;
+               upk2(az, u0, u1); pa[2] = u0 + u1;
+            }
+         }
+         else
+         {
+            const V4* tp = (const V4*)(tiles + b * nearTileBytes<T>(TS));
+            const V4* tq = tp + TS;
+#pragma unroll 4
+            for(int i = g; i < n; i += G)
+            {
+               const V4 y = tp[i], w = tq[i];
+               const T dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+               const T r2 = dx * dx + dy * dy + dz * dz;
+               T ri = rsqrt(r2);
+               if constexpr(WANTA) ri = r2 > T(0) ? ri : T(0);
+               else ri = min(ri, riCap<T>());
+               const T ri3 = ri * ri * ri;
+               pb[0] += (w.y * dz - w.z * dy) * ri3;
+               pb[1] += (w.z * dx - w.x * dz) * ri3;
+               pb[2] += (w.x * dy - w.y * dx) * ri3;
+               if(wantA) { pa[0] += w.x * ri; pa[1] += w.y * ri; pa[2] += w.z * ri; }
+            }
          }
          for(int d = 0; d < 3; d++) { Bd[d] += double(pb[d]); Ad[d] += double(pa[d]); }
       };
@@ -1195,25 +1305,62 @@ __global__ void __launch_bounds__(NT) kL2PNear(Tree t, const RootBox* __restrict
          for(int r = 0; r < NE / NT; r++) ePre[tid * (NE / NT) + r] = sz[r];
          if(tid == 0) ePre[NE] = total;
          __syncthreads();
-         for(int pos = 0; pos < total; pos += TS)
-         {
+         // tiles double-buffered: tile k + 1's copies (cp.async) are in flight while tile k is summed
+         auto issueTile = [&](int pos, int b) {
             const int n = min(TS, total - pos);
-            for(int j = tid; j < n; j += NT)
+            const int nf = sizeof(T) == 4 ? (n + 1) & ~1 : n;   // FP32: the odd tile's last pair slot zero-filled
+            unsigned char* tb = tiles + b * nearTileBytes<T>(TS);
+            for(int j = tid; j < nf; j += NT)
             {
-               const int qpos = pos + j;
-               int lo = 0, hi = ne;  // last entry with ePre <= qpos
-               while(hi - lo > 1)
+               const bool in = j < n;
+               int src = 0;
+               if(in)
                {
-                  const int mid = (lo + hi) >> 1;
-                  if(ePre[mid] <= qpos) lo = mid;
-                  else hi = mid;
+                  const int qpos = pos + j;
+                  int lo = 0, hi = ne;  // last entry with ePre <= qpos
+                  while(hi - lo > 1)
+                  {
+                     const int mid = (lo + hi) >> 1;
+                     if(ePre[mid] <= qpos) lo = mid;
+                     else hi = mid;
+                  }
+                  src = eSrc[lo] + (qpos - ePre[lo]);
                }
-               const int src = eSrc[lo] + (qpos - ePre[lo]);
-               Sp[j] = spos[src];
-               Sq[j] = sq[src];
+               if constexpr(sizeof(T) == 4)
+               {
+                  float* d = (float*)tb + 12 * (j >> 1) + (j & 1);
+                  const float* ps = (const float*)(spos + src);
+                  const float* qs = (const float*)(sq + src);
+                  const uint32_t by = in ? 4u : 0u;
+                  cpAsync4(d, ps, by); cpAsync4(d + 2, ps + 1, by); cpAsync4(d + 4, ps + 2, by);
+                  cpAsync4(d + 6, qs, by); cpAsync4(d + 8, qs + 1, by); cpAsync4(d + 10, qs + 2, by);
+               }
+               else
+               {
+                  V4* tp = (V4*)tb;
+#pragma unroll
+                  for(int h = 0; h < int(sizeof(V4)) / 16; h++)
+                  {
+                     cpAsync16Simt((char*)(tp + j) + 16 * h, (const char*)(spos + src) + 16 * h, 16u);
+                     cpAsync16Simt((char*)(tp + TS + j) + 16 * h, (const char*)(sq + src) + 16 * h, 16u);
+                  }
+               }
             }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+         };
+         const int nTiles = (total + TS - 1) / TS;
+         if(nTiles > 0) issueTile(0, 0);
+         for(int k = 0; k < nTiles; k++)
+         {
+            if(k + 1 < nTiles)
+            {
+               issueTile((k + 1) * TS, (k + 1) & 1);
+               asm volatile("cp.async.wait_group 1;" ::: "memory");
+            }
+            else
+               asm volatile("cp.async.wait_group 0;" ::: "memory");
             __syncthreads();
-            tileSum(n);
+            tileSum(min(TS, total - k * TS), k & 1);
             __syncthreads();
          }
       }
@@ -1408,7 +1555,7 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
    const int TS = P.nearTile == 128 ? 128 : 256;
    const bool split = P.l2pSplit != 0;
    const size_t coef = split ? 0 : (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31);
-   size_t shm = coef + 2 * sizeof(V4) * TS + sizeof(double) * 6 * NT;
+   size_t shm = coef + 2 * size_t(nearTileBytes<T>(TS)) + sizeof(double) * 6 * NT;
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
    if(split)
    {
