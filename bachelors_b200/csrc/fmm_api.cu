@@ -99,6 +99,11 @@ fmm_status Plan::init(const fmm_config& c)
    if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(3, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
    if(const char* e = getenv("FMM_L2P_SPLIT")) l2pSplit = atoi(e) != 0;
+   if(const char* e = getenv("FMM_TC_TRANSLATE")) tcTranslate = atoi(e) & 3;
+   if(const char* e = getenv("FMM_TC_TRDRAIN")) tcTrDrainItems = std::max(0, atoi(e));
+   if(const char* e = getenv("FMM_L2L_CHILD")) l2lChildMajor = atoi(e) != 0;
+   if(const char* e = getenv("FMM_TC_TRNP_UP")) tcTrPiecesUp = std::min(3, std::max(0, atoi(e)));
+   if(const char* e = getenv("FMM_TC_TRNP_DN")) tcTrPiecesDn = std::min(3, std::max(0, atoi(e)));
 
    FMM_TRY(rootb.reserve(sizeof(RootBox)));
    FMM_TRY(errb.reserve(sizeof(int)));
@@ -122,7 +127,7 @@ void Plan::release()
    DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
                      &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &parList, &m2lTargets, &m2lKeys, &errb,
                      &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf, &multBf, &tcCounters,
-                     &adjG, &adjOut, &nearCounts};
+                     &adjG, &adjOut, &nearCounts, &vtabUp, &vtabDn, &l2lTargets, &l2lKeys, &opM2Mbf, &opL2Lbf};
    for(DevBuf* b : bufs) b->release();
    for(auto& b : nodeBufs) b.release();
    for(auto& b : listBufs) b.release();

@@ -131,6 +131,23 @@ struct Plan
    std::vector<int> parStart;           // parList index where each level's parents start [nLevels + 1]
    DevBuf m2lTargets, m2lKeys;          // boxes with an M2L list, grouped by octant
    int nM2LTargets = 0;
+   // tensor-core M2M / L2L: per node and child octant, the child with sources (vtabUp, indexed by the
+   // parent) and the parent of a child with targets (vtabDn, indexed by the child); the nodes with
+   // targets below the roots sorted by (level, octant), and where each level starts in that list
+   DevBuf vtabUp, vtabDn, l2lTargets, l2lKeys;
+   std::vector<int> l2lStart;            // [8 level + octant], up to [8 nLevels]
+   DevBuf opM2Mbf, opL2Lbf;              // their operator images
+   int opTrImgTag = -1;
+   int multBfTag = -1;                   // pieces/format multBf holds the multipoles of every node in
+                                         // (levels >= 1), -1 when it holds anything else
+   int tcTranslate = 1;                  // M2M (1) / L2L (2) on the tensor cores in tensor-core M2L plans
+   int tcTrDrainItems = 0;               // their drains: every this many pipeline items (0: per drainEvery offsets)
+   int tcTrPiecesUp = 0, tcTrPiecesDn = 3;   // their bf16 pieces (0: as the M2L mode)
+   int l2lChildMajor = 1;                // CUDA-core L2L over the sorted child lists (kL2LChild)
+   bool tcTranslations(int which = 3) const
+   {
+      return !fp64 && cfg.m2l_mode != FMM_M2L_SIMT && (tcTranslate & which) != 0;
+   }
    int* err = nullptr;
    DevBuf errb;
    // expansions [node][3][Lp] and outputs
@@ -210,6 +227,8 @@ template <class T> fmm_status directT(Plan& P, double current, int want, cudaStr
 fmm_status buildOperators(Plan& P, cudaStream_t st);
 fmm_status initOffsetTables();
 fmm_status m2lTensorCore(Plan& P, cudaStream_t st);
+fmm_status m2mTensorCore(Plan& P, cudaStream_t st);
+fmm_status l2lTensorCore(Plan& P, cudaStream_t st);
 template <class T> fmm_status regatherStrengthsT(Plan& P, cudaStream_t st);
 template <class T> fmm_status scaleCopyT(Plan& P, const void* src, void* dst, int64_t count, double scale, cudaStream_t st);
 template <class T> fmm_status adjointT(Plan& P, Plan& A, double current, const void* g, void* dJ, void* dx, cudaStream_t st);

@@ -688,6 +688,108 @@ __global__ void __launch_bounds__(32 * P2MW_WARPS) kP2MWarp(Tree t, const RootBo
 // ====================================================================================
 
 // ====================================================================================
+// L2L, one level, child-major: the level's children with targets come sorted by octant, and a
+// block takes 32 children of one octant (blockIdx.z), so every row of its tile uses the same
+// operator T_o and none is computed for a child that does not exist. Rows are the parents' locals
+// (parent x component), gathered; the K range per 64-column group is the L2L triangle (inputs of
+// degree >= the output's); the result is added to the children's locals (one writer per child).
+// ====================================================================================
+struct L2LSeg
+{
+   int start[9];   // the octants' ranges in the sorted child list
+};
+
+template <class T>
+__global__ void __launch_bounds__(256, 2) kL2LChild(Tree t, const int* __restrict__ list, L2LSeg seg, int p, int Lp,
+                                                    const T* __restrict__ opw, T* __restrict__ X)
+{
+   const int o = blockIdx.z;
+   const int s0 = seg.start[o] + blockIdx.x * TG_P, s1 = seg.start[o + 1];
+   if(s0 >= s1) return;
+   __shared__ __align__(16) T As[TG_K][TG_ROWS + 1];
+   __shared__ __align__(16) T Bs[TG_K][TG_N];
+   __shared__ int childOf[TG_P], parentOf[TG_P];
+   const int tid = threadIdx.x;
+   const int L = nharm(p);
+   const int n0 = blockIdx.y * TG_N;
+   if(tid < TG_P)
+   {
+      const int ch = s0 + tid < s1 ? list[s0 + tid] : -1;
+      childOf[tid] = ch;
+      parentOf[tid] = ch >= 0 ? t.parent[ch] : -1;
+   }
+   __syncthreads();
+   const int lLo = degreeOf(min(n0, L - 1));
+   const int kLo = lLo * lLo, kHi = L;
+   const int tr = tid >> 4, tc = tid & 15;
+   T acc[6][4];
+#pragma unroll
+   for(int i = 0; i < 6; i++)
+#pragma unroll
+      for(int j = 0; j < 4; j++) acc[i][j] = T(0);
+   const int nK = (kHi - kLo + TG_K - 1) / TG_K;
+   constexpr int QA = TG_K * TG_ROWS / 256, QB = TG_K * TG_N / 256;
+   T ra[QA], rb[QB];
+   const int aK = tid & 31, aR = tid >> 5;
+   const int bN = tid & 63, bK = tid >> 6;
+   const T* op = opw + int64_t(o) * L * Lp + n0 + bN;
+   const bool bIn = n0 + bN < Lp;
+   auto load = [&](int step) {
+      const int k0 = kLo + step * TG_K;
+      const bool aIn = k0 + aK < kHi;
+#pragma unroll
+      for(int q = 0; q < QA; q++)
+      {
+         const int r = aR + 8 * q;
+         const int i = r / 3, c = r - 3 * i;
+         const int src = parentOf[i];
+         ra[q] = (src >= 0 && aIn) ? X[(int64_t(src) * 3 + c) * Lp + k0 + aK] : T(0);
+      }
+#pragma unroll
+      for(int q = 0; q < QB; q++)
+      {
+         const int k = k0 + bK + 4 * q;
+         rb[q] = (k < kHi && bIn) ? op[int64_t(k) * Lp] : T(0);
+      }
+   };
+   if(nK > 0) load(0);
+   for(int step = 0; step < nK; step++)
+   {
+      __syncthreads();
+#pragma unroll
+      for(int q = 0; q < QA; q++) As[aK][aR + 8 * q] = ra[q];
+#pragma unroll
+      for(int q = 0; q < QB; q++) Bs[bK + 4 * q][bN] = rb[q];
+      __syncthreads();
+      if(step + 1 < nK) load(step + 1);
+#pragma unroll 8
+      for(int kk = 0; kk < TG_K; kk++)
+      {
+         T a[6], b[4];
+#pragma unroll
+         for(int i = 0; i < 6; i++) a[i] = As[kk][tr * 6 + i];
+         load4(&Bs[kk][tc * 4], b);
+#pragma unroll
+         for(int i = 0; i < 6; i++)
+#pragma unroll
+            for(int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
+      }
+   }
+#pragma unroll
+   for(int i = 0; i < 6; i++)
+   {
+      const int r = tr * 6 + i, ci = r / 3, c = r % 3;
+      const int ch = childOf[ci];
+      if(ch < 0) continue;
+      for(int j = 0; j < 4; j++)
+      {
+         const int n = n0 + tc * 4 + j;
+         if(n < Lp) X[(int64_t(ch) * 3 + c) * Lp + n] += acc[i][j];
+      }
+   }
+}
+
+// ====================================================================================
 // M2L on the CUDA cores (FP32 or FP64 FMA). A block owns TT target boxes from the octant-grouped
 // list of boxes with an M2L list (3 TT rows: box x component) and all output coefficients; it
 // walks only the offsets present in its tile and, per offset, the K chunks of the operator. The
@@ -1476,6 +1578,7 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
                                               (T*)P.mult.ptr);
    FMM_TRY(launched(P, "kP2M", st));
    FMM_CHECK_LAUNCH();
+   if(P.tcTranslations(1)) return m2mTensorCore(P, st);
    const int nCol = (Lp + TG_N - 1) / TG_N;
    for(int level = P.tree.nLevels - 2; level >= 0; level--)
    {
@@ -1532,7 +1635,24 @@ fmm_status downwardT(Plan& P, cudaStream_t st)
    if(sizeof(T) == 4 && P.cfg.m2l_mode != FMM_M2L_SIMT) FMM_TRY(m2lTensorCore(P, st));
    else FMM_TRY(m2lSimt<T>(P, st));
    if(P.eventsMade && !P.capturing) cudaEventRecord(P.ev[3], st);
+   if(P.tcTranslations(2)) return l2lTensorCore(P, st);
    const int nCol = (Lp + TG_N - 1) / TG_N;
+   if(P.l2lChildMajor)
+   {
+      for(int level = 0; level + 1 < P.tree.nLevels; level++)
+      {
+         L2LSeg seg;
+         int maxTiles = 0;
+         for(int o = 0; o <= 8; o++) seg.start[o] = P.l2lStart[8 * (level + 1) + o];
+         for(int o = 0; o < 8; o++) maxTiles = std::max(maxTiles, (seg.start[o + 1] - seg.start[o] + TG_P - 1) / TG_P);
+         if(maxTiles == 0) continue;
+         kL2LChild<T><<<dim3(maxTiles, nCol, 8), 256, 0, st>>>(P.tree, (const int*)P.l2lTargets.ptr, seg, P.p, Lp,
+                                                                (const T*)P.opL2Lw.ptr, (T*)P.local.ptr);
+         FMM_TRY(launched(P, "kL2LChild", st));
+      }
+      FMM_CHECK_LAUNCH();
+      return FMM_OK;
+   }
    for(int level = 0; level + 1 < P.tree.nLevels; level++)
    {
       const int a = P.parStart[level], b = P.parStart[level + 1];

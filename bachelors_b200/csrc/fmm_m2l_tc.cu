@@ -268,10 +268,10 @@ __device__ __forceinline__ void splitBf16(double x, __nv_bfloat16* piece)
 // (hi first), each N rows (output coefficients, N = Lp) x KC bf16 (input coefficients) in the
 // swizzled K-major layout, zero outside the (p+1)^2 x (p+1)^2 operator.
 template <int NP, class Lay>
-__global__ void kPrepM2LImage(const double* __restrict__ op64, int L, int N, int nChunks, uint8_t* img)
+__global__ void kPrepM2LImage(const double* __restrict__ op64, int nOps, int L, int N, int nChunks, uint8_t* img)
 {
    const int64_t blockBytes = int64_t(N) * Lay::RB;
-   const int64_t total = int64_t(316) * nChunks * int64_t(N) * Lay::KC;
+   const int64_t total = int64_t(nOps) * nChunks * int64_t(N) * Lay::KC;
    for(int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
    {
       int64_t r = e;
@@ -335,9 +335,10 @@ __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int 
 // 18 warps: five of them share one SM sub-partition's 16K registers, so 96 per thread at most.
 template <int NP, class Lay>
 __global__ void __maxnreg__(96)
-kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int L, int Lp, int nChunks,
-       const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc, int drainEvery,
-       int nStages, int drainMode, const M2LCols cols, unsigned long long* counters, int* err)
+kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int nOps, int L, int Lp,
+       int nChunks, const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc,
+       int addOut, int drainEvery, int drainItems, int nStages, int drainMode, const M2LCols cols,
+       unsigned long long* counters, int* err)
 {
    using namespace tc;
    constexpr int KCH = Lay::KC;
@@ -401,27 +402,31 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    }
    __syncthreads();
    // which offsets have a source for some box of the tile
-   for(int e = tid; e < TT * 316; e += NTHREADS)
+   for(int e = tid; e < TT * nOps; e += NTHREADS)
    {
-      const int t = tileNode[e / 316], o = e % 316;
-      if(t >= 0 && vtab[int64_t(t) * 316 + o] >= 0) atomicOr(&present[o >> 5], 1u << (o & 31));
+      const int t = tileNode[e / nOps], o = e % nOps;
+      if(t >= 0 && vtab[int64_t(t) * nOps + o] >= 0) atomicOr(&present[o >> 5], 1u << (o & 31));
    }
    fenceBeforeSync();
    __syncthreads();
    fenceAfterSync();
    if(tid == 0)
    {
-      // far offsets first: the smaller contributions enter the accumulator before the large ones
+      // M2L: far offsets first, so the smaller contributions enter the accumulator before the large
+      // ones; the 8 child octants of M2M / L2L in order
       int k = 0;
-      for(int i = 0; i < 316; i++)
+      for(int i = 0; i < nOps; i++)
       {
-         const int o = d_m2lFarFirst[i];
+         const int o = nOps == 316 ? d_m2lFarFirst[i] : i;
          if(present[o >> 5] & (1u << (o & 31))) itemOffset[k++] = o;
       }
       itemOffset[316] = k;
       // work accounting: pipeline items (offset x K chunk) and tile-offset pairs
-      atomicAdd(counters, (unsigned long long)(k * nChunks));
-      atomicAdd(counters + 1, (unsigned long long)k);
+      if(counters)
+      {
+         atomicAdd(counters, (unsigned long long)(k * nChunks));
+         atomicAdd(counters + 1, (unsigned long long)k);
+      }
    }
    __syncthreads();
    const int nOff = itemOffset[316];
@@ -488,13 +493,16 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             // every drainEvery offsets (and after the last) hand the accumulator to the drain warps
             // and start a fresh one: the tensor cores' FP32 accumulation truncates, so long chains
             // of accumulations into one TMEM value drift; the running sum is kept in FP32 instead
-            if(it % nChunks == nChunks - 1)
+            // (drainItems > 0: every drainItems pipeline items instead, for full-width operators only:
+            // a fresh accumulation must start with an MMA that writes every column)
+            const bool drainNow = drainItems > 0 ? ((it + 1) % drainItems == 0 || it == nItems - 1)
+                                                 : (it % nChunks == nChunks - 1 &&
+                                                    ((it / nChunks + 1) % drainEvery == 0 || it == nItems - 1));
             {
-               const int oi = it / nChunks;
-               if((oi + 1) % drainEvery == 0 || oi == nOff - 1)
+               if(drainNow)
                {
                   mmaCommit(drainFull);
-                  if(oi != nOff - 1)
+                  if(it != nItems - 1)
                   {
                      if(!mbarWait(drainEmpty, drains & 1, err, abortFlag)) break;
                      fenceAfterSync();
@@ -538,7 +546,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
       float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
       const uint32_t tAcc = tmem + (uint32_t(lanes) << 16);
-      const int nDrains = (nOff + drainEvery - 1) / drainEvery;
+      const int nDrains = drainItems > 0 ? (nItems + drainItems - 1) / drainItems : (nOff + drainEvery - 1) / drainEvery;
       // The running sum is FP32, rounded to nearest, and has one writer per row and column (this
       // thread); the locals start at zero and no other CTA touches these rows, so the result is
       // deterministic. Its columns live in three parts:
@@ -586,8 +594,16 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                   float4* o4 = reinterpret_cast<float4*>(out + c0);
 #pragma unroll
                   for(int i = 0; i < 4; i++)
-                     o4[i] = make_float4(__uint_as_float(sv[4 * i]), __uint_as_float(sv[4 * i + 1]),
-                                         __uint_as_float(sv[4 * i + 2]), __uint_as_float(sv[4 * i + 3]));
+                  {
+                     float4 v = make_float4(__uint_as_float(sv[4 * i]), __uint_as_float(sv[4 * i + 1]),
+                                            __uint_as_float(sv[4 * i + 2]), __uint_as_float(sv[4 * i + 3]));
+                     if(addOut)
+                     {
+                        const float4 w = o4[i];
+                        v = make_float4(w.x + v.x, w.y + v.y, w.z + v.z, w.w + v.w);
+                     }
+                     o4[i] = v;
+                  }
                }
             }
             else
@@ -610,12 +626,21 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                float4* o4 = reinterpret_cast<float4*>(out + c0);
 #pragma unroll
                for(int i = 0; i < 4; i++)
-                  o4[i] = make_float4(rsum[16 * j + 4 * i], rsum[16 * j + 4 * i + 1], rsum[16 * j + 4 * i + 2],
-                                      rsum[16 * j + 4 * i + 3]);
+               {
+                  float4 v = make_float4(rsum[16 * j + 4 * i], rsum[16 * j + 4 * i + 1], rsum[16 * j + 4 * i + 2],
+                                         rsum[16 * j + 4 * i + 3]);
+                  if(addOut)
+                  {
+                     const float4 w = o4[i];
+                     v = make_float4(w.x + v.x, w.y + v.y, w.z + v.z, w.w + v.w);
+                  }
+                  o4[i] = v;
+               }
             }
          }
          // global part, 16 columns per step; the running sums load while the accumulator does
-         const bool rmw = drainMode != 0 && d > 0 && et >= 0;
+         // with addOut the first drain adds to the values already there as well
+         const bool rmw = drainMode != 0 && (d > 0 || addOut) && et >= 0;
          for(int c0 = gLo; c0 < gHi; c0 += 16)
          {
             uint32_t u[16];
@@ -635,7 +660,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                const float4 v = make_float4(__uint_as_float(u[4 * i]), __uint_as_float(u[4 * i + 1]),
                                             __uint_as_float(u[4 * i + 2]), __uint_as_float(u[4 * i + 3]));
                if(drainMode == 0) atomicAdd(o4 + i, v);
-               else if(d == 0) o4[i] = v;
+               else if(!rmw) o4[i] = v;
                else o4[i] = make_float4(old[i].x + v.x, old[i].y + v.y, old[i].z + v.z, old[i].w + v.w);
             }
          }
@@ -655,7 +680,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       const int row = ptid >> 1, half = ptid & 1;
       const int slot = row / 3, comp = row % 3;
       const int tgt = row < 3 * TT ? tileNode[slot] : -1;
-      int src = (tgt >= 0 && nItems > 0) ? vtab[int64_t(tgt) * 316 + itemOffset[0]] : -1;
+      int src = (tgt >= 0 && nItems > 0) ? vtab[int64_t(tgt) * nOps + itemOffset[0]] : -1;
       int srcNext = -1;
       int pending = -1;
       for(int it = 0; it < nItems; it++)
@@ -663,7 +688,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          const int s = it % NS;
          const int oi = it / nChunks, c = it % nChunks;
          if(it % nChunks == 0 && oi + 1 < nOff)
-            srcNext = tgt >= 0 ? vtab[int64_t(tgt) * 316 + itemOffset[oi + 1]] : -1;
+            srcNext = tgt >= 0 ? vtab[int64_t(tgt) * nOps + itemOffset[oi + 1]] : -1;
          if(pending >= 0)
          {
             cpAsyncWaitAll();
@@ -718,7 +743,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(P.opImgOrder != tag)
    {
       FMM_TRY(P.opM2Lbf.reserve(imgBytes));
-      kPrepM2LImage<NP, Lay><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, L, Lp, nChunks,
+      kPrepM2LImage<NP, Lay><<<4096, 256, 0, st>>>((const double*)P.opM2L64.ptr, 316, L, Lp, nChunks,
                                                    (uint8_t*)P.opM2Lbf.ptr);
       FMM_TRY(launched(P, "kPrepM2LImage", st));
       P.opImgOrder = tag;
@@ -755,13 +780,17 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
       cols.n[g] = k < L ? n : 0;
    }
    const int64_t rows = P.tree.nNodes * 3;
-   FMM_TRY(P.multBf.reserve(size_t(Lay::ES) * rows * NP * Lp));
-   kSplitMultipoles<NP, Lay::TF32><<<148 * 16, 256, 0, st>>>((const float*)P.mult.ptr, rows, Lp, (uint8_t*)P.multBf.ptr);
-   FMM_TRY(launched(P, "kSplitMultipoles", st));
-   kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, L, Lp, nChunks,
-                                                      (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
-                                                      (float*)P.local.ptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)), nStages, P.tcDrainMode,
-                                                      cols, (unsigned long long*)P.tcCounters.ptr, P.err);
+   // the tensor-core M2M leaves every source level's multipoles split in this format
+   if(P.multBfTag != NP * 2 + (Lay::TF32 ? 1 : 0))
+   {
+      FMM_TRY(P.multBf.reserve(size_t(Lay::ES) * rows * NP * Lp));
+      kSplitMultipoles<NP, Lay::TF32><<<148 * 16, 256, 0, st>>>((const float*)P.mult.ptr, rows, Lp, (uint8_t*)P.multBf.ptr);
+      FMM_TRY(launched(P, "kSplitMultipoles", st));
+   }
+   kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
+                                                      nChunks, (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
+                                                      (float*)P.local.ptr, 0, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
+                                                      0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
    int herr = 0;
@@ -770,6 +799,114 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "tensor-core M2L: a pipeline wait timed out");
    return FMM_OK;
 }
+
+// M2M and L2L on the same kernel, one launch per level, with the 8 child-octant operators in place
+// of the 316 offsets. M2M: the targets are the level's parents, vtabUp gives each parent's child
+// with sources per octant, the children's multipoles are split into pieces first (so after the
+// upward pass every level >= 1 is split and the M2L reuses it), and the parents' multipoles are
+// stored. L2L: the targets are the next level's nodes with targets sorted by octant (one operator
+// per tile), vtabDn gives each one's parent, the parents' locals are split first, and the result
+// is added to the children's locals (addOut). Full output width: the triangular structure (M2M
+// outputs of degree l take inputs of degree <= l, L2L the reverse) is not a prefix of the columns.
+template <int NP, class Lay>
+static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
+{
+   const int L = P.L, Lp = P.Lp;
+   const int nChunks = (L + Lay::KC - 1) / Lay::KC;
+   const int tag = ((P.p * 8 + NP) * 128 + Lay::KC) * 2 + (Lay::TF32 ? 1 : 0);
+   const size_t imgBytes = size_t(8) * nChunks * NP * size_t(Lp) * Lay::RB;
+   if(P.opTrImgTag != tag)
+   {
+      FMM_TRY(P.opM2Mbf.reserve(imgBytes));
+      FMM_TRY(P.opL2Lbf.reserve(imgBytes));
+      kPrepM2LImage<NP, Lay><<<1024, 256, 0, st>>>((const double*)P.opM2M64.ptr, 8, L, Lp, nChunks,
+                                                   (uint8_t*)P.opM2Mbf.ptr);
+      FMM_TRY(launched(P, "kPrepM2LImage", st));
+      kPrepM2LImage<NP, Lay><<<1024, 256, 0, st>>>((const double*)P.opL2L64.ptr, 8, L, Lp, nChunks,
+                                                   (uint8_t*)P.opL2Lbf.ptr);
+      FMM_TRY(launched(P, "kPrepM2LImage", st));
+      P.opTrImgTag = tag;
+   }
+   const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
+   const size_t fixed = 1024 + 192 + 4 * (320 + 64 + MAXKSTEPS);
+   const size_t budget = 232448;
+   const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
+   if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core translation: %zu-byte stages do not fit twice", stageBytes);
+   const size_t smem = fixed + nStages * stageBytes;
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   M2LCols cols{};
+   const int nSteps = nChunks * (Lay::KC / Lay::KSTEP);
+   if(nSteps > MAXKSTEPS) return setError(FMM_E_INVALID, "tensor-core translation: %d K steps exceed the column table", nSteps);
+   for(int g = 0; g < nSteps; g++) cols.n[g] = Lay::KSTEP * g < L ? Lp : 0;
+   const int64_t rows = P.tree.nNodes * 3;
+   FMM_TRY(P.multBf.reserve(size_t(Lay::ES) * rows * NP * Lp));
+   FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   const int drainEvery = NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2);
+   const size_t pieceRow = size_t(Lay::ES) * NP * Lp;   // bytes of one split row
+   const Tree& t = P.tree;
+   auto split = [&](const float* src, int lvl) -> fmm_status {
+      const int64_t r0 = int64_t(t.levelStart[lvl]) * 3, r1 = int64_t(t.levelStart[lvl + 1]) * 3;
+      if(r1 <= r0) return FMM_OK;
+      kSplitMultipoles<NP, Lay::TF32><<<std::min<int64_t>(148 * 16, (r1 - r0) * Lp / 256 + 1), 256, 0, st>>>(
+         src + r0 * Lp, r1 - r0, Lp, (uint8_t*)P.multBf.ptr + r0 * pieceRow);
+      return launched(P, "kSplitMultipoles", st);
+   };
+   if(up)
+   {
+      for(int level = t.nLevels - 2; level >= 0; level--)
+      {
+         const int a = P.parStart[level], b = P.parStart[level + 1];
+         if(b <= a) continue;
+         FMM_TRY(split((const float*)P.mult.ptr, level + 1));
+         kM2LTc<NP, Lay><<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
+            (const int*)P.parList.ptr + a, b - a, (const int*)P.vtabUp.ptr, 8, L, Lp, nChunks,
+            (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0, drainEvery, P.tcTrDrainItems, nStages,
+            P.tcDrainMode, cols, nullptr, P.err);
+         FMM_TRY(launched(P, "kM2LTc<M2M>", st));
+      }
+      P.multBfTag = NP * 2 + (Lay::TF32 ? 1 : 0);
+   }
+   else
+   {
+      for(int level = 0; level + 1 < t.nLevels; level++)
+      {
+         const int a = P.l2lStart[8 * (level + 1)], b = P.l2lStart[8 * (level + 2)];
+         if(b <= a) continue;
+         FMM_TRY(split((const float*)P.local.ptr, level));
+         kM2LTc<NP, Lay><<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
+            (const int*)P.l2lTargets.ptr + a, b - a, (const int*)P.vtabDn.ptr, 8, L, Lp, nChunks,
+            (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, drainEvery, P.tcTrDrainItems, nStages,
+            P.tcDrainMode, cols, nullptr, P.err);
+         FMM_TRY(launched(P, "kM2LTc<L2L>", st));
+      }
+      P.multBfTag = -1;
+   }
+   FMM_CHECK_LAUNCH();
+   if(P.capturing) return FMM_OK;
+   int herr = 0;
+   FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+   FMM_CUDA(cudaStreamSynchronize(st));
+   if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "tensor-core translation: a pipeline wait timed out");
+   return FMM_OK;
+}
+
+static fmm_status translateTensorCore(Plan& P, cudaStream_t st, bool up)
+{
+   if(P.Lp > 320 || P.Lp % 16) return setError(FMM_E_INVALID, "tensor-core translation supports p <= 16");
+   using tc::Layout;
+   // pieces: 0 follows the M2L mode; 3 is BF16X6, whose products carry the full FP32 significand
+   const int np = up ? P.tcTrPiecesUp : P.tcTrPiecesDn;
+   if(np == 3) return P.tcKChunk == 64 ? translateTc<3, Layout<64>>(P, st, up) : translateTc<3, Layout<32>>(P, st, up);
+   if(np == 2) return P.tcKChunk == 32 ? translateTc<2, Layout<32>>(P, st, up) : translateTc<2, Layout<64>>(P, st, up);
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X3)
+      return P.tcKChunk == 32 ? translateTc<2, Layout<32>>(P, st, up) : translateTc<2, Layout<64>>(P, st, up);
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X6)
+      return P.tcKChunk == 64 ? translateTc<3, Layout<64>>(P, st, up) : translateTc<3, Layout<32>>(P, st, up);
+   return translateTc<1, tc::LayoutTf32>(P, st, up);
+}
+
+fmm_status m2mTensorCore(Plan& P, cudaStream_t st) { return translateTensorCore(P, st, true); }
+fmm_status l2lTensorCore(Plan& P, cudaStream_t st) { return translateTensorCore(P, st, false); }
 
 fmm_status m2lTensorCore(Plan& P, cudaStream_t st)
 {

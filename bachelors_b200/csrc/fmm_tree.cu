@@ -486,6 +486,42 @@ __global__ void kParentLevelStarts(Tree t, const int* __restrict__ pos, int* out
    if(l <= t.nLevels) out[l] = pos[t.levelStart[l]];
 }
 
+// Tensor-core M2M / L2L tables (both preset to -1): up[parent][octant] = the child with sources,
+// dn[child][octant of the child] = its parent, for children with targets.
+__global__ void kTranslateTables(Tree t, int nNodes, int* __restrict__ up, int* __restrict__ dn)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if(i >= nNodes) return;
+   const int par = t.parent[i];
+   if(par < 0) return;
+   const int o = int(t.key[i] & 7);
+   if(t.s1[i] > t.s0[i]) up[int64_t(par) * 8 + o] = i;
+   if(t.t1[i] > t.t0[i]) dn[int64_t(i) * 8 + o] = par;
+}
+// Keys (level, octant) of the nodes with targets below the roots; the rest sort last.
+__global__ void kL2LTargetKeys(Tree t, int nNodes, unsigned* keys, int* vals)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if(i >= nNodes) return;
+   const bool has = t.parent[i] >= 0 && t.t1[i] > t.t0[i];
+   keys[i] = has ? (unsigned(t.level[i]) << 3) | unsigned(t.key[i] & 7) : unsigned(MAXLEVEL + 2) << 3;
+   vals[i] = i;
+}
+// out[8 l + o] = the first sorted position whose (level, octant) is >= (l, o), up to (nLevels, 0).
+__global__ void kL2LLevelStarts(const unsigned* __restrict__ keys, int n, int nLevels, int* out)
+{
+   const int lo8 = threadIdx.x;
+   if(lo8 > 8 * nLevels) return;
+   int lo = 0, hi = n;
+   while(lo < hi)
+   {
+      const int mid = (lo + hi) >> 1;
+      if(keys[mid] < unsigned(lo8)) lo = mid + 1;
+      else hi = mid;
+   }
+   out[lo8] = lo;
+}
+
 // ------------------------------------------------------------------------------ host driver
 template <class T>
 fmm_status buildTreeT(Plan& P, cudaStream_t st)
@@ -735,6 +771,38 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       FMM_CUDA(cudaStreamSynchronize(st));
       P.nM2LTargets = cntT;
       FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   }
+   P.multBfTag = -1;
+   // M2M / L2L tables: the L2L child lists always (both L2L forms use them), the octant tables
+   // for the tensor-core forms
+   {
+      if(P.tcTranslations())
+      {
+         FMM_TRY(P.vtabUp.reserve(sizeof(int) * 8 * size_t(nn)));
+         FMM_TRY(P.vtabDn.reserve(sizeof(int) * 8 * size_t(nn)));
+         FMM_CUDA(cudaMemsetAsync(P.vtabUp.ptr, 0xff, sizeof(int) * 8 * size_t(nn), st));
+         FMM_CUDA(cudaMemsetAsync(P.vtabDn.ptr, 0xff, sizeof(int) * 8 * size_t(nn), st));
+         kTranslateTables<<<(nn + 255) / 256, 256, 0, st>>>(t, nn, (int*)P.vtabUp.ptr, (int*)P.vtabDn.ptr);
+         FMM_TRY(launched(P, "kTranslateTables", st));
+      }
+      FMM_TRY(P.l2lTargets.reserve(2 * sizeof(int) * nn));
+      FMM_TRY(P.l2lKeys.reserve(2 * sizeof(unsigned) * nn));
+      unsigned* kk = (unsigned*)P.l2lKeys.ptr;
+      int* vv = (int*)P.l2lTargets.ptr;
+      kL2LTargetKeys<<<(nn + 255) / 256, 256, 0, st>>>(t, nn, kk + nn, vv + nn);
+      FMM_TRY(launched(P, "kL2LTargetKeys", st));
+      tmp = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, tmp, kk + nn, kk, vv + nn, vv, nn, 0, 8, st);
+      FMM_TRY(P.cubTmp.reserve(tmp));
+      tmp = P.cubTmp.bytes;
+      FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, kk + nn, kk, vv + nn, vv, nn, 0, 8, st));
+      FMM_TRY(P.scratch.reserve(sizeof(int) * 8 * (MAXLEVEL + 2)));
+      kL2LLevelStarts<<<1, 8 * (MAXLEVEL + 2), 0, st>>>(kk, nn, nLevels, (int*)P.scratch.ptr);
+      FMM_TRY(launched(P, "kL2LLevelStarts", st));
+      P.l2lStart.assign(8 * nLevels + 1, 0);
+      FMM_CUDA(cudaMemcpyAsync(P.l2lStart.data(), P.scratch.ptr, sizeof(int) * (8 * nLevels + 1), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+      FMM_CHECK_LAUNCH();
    }
    return FMM_OK;
 }
