@@ -50,3 +50,18 @@ def test_split_bf16_repeatable(mode):
     B1, _ = solve(x, ww, JJ, x, 10, 32, mode)
     B2, _ = solve(x, ww, JJ, x, 10, 32, mode)
     np.testing.assert_array_equal(B1, B2)
+
+
+@pytest.mark.parametrize("translate", ["0", "1", "3"])
+@pytest.mark.parametrize("mode", ["bf16x3", "bf16x6", "tf32"])
+def test_translation_forms_match_oracle(monkeypatch, translate, mode):
+    """M2M / L2L forms (read when a plan is created): 0 both on the CUDA cores, 1 M2M on the tensor
+    cores (the default), 3 both on the tensor cores."""
+    monkeypatch.setenv("FMM_TC_TRANSLATE", translate)
+    xyz, w, J = G.torus(64, 16, 16, 2.0, 0.5)
+    tgt = G.uniform_points(2000, -3, 3, 23)
+    x, ww, JJ, t = (a.astype(np.float32) for a in (xyz, w, J, tgt))
+    B, A = solve(x, ww, JJ, t, 12, 32, mode)
+    c, H = G.root_cube(x.astype(np.float64), t.astype(np.float64))
+    Bo, Ao, _ = O.fmm(12, 32, x, ww, JJ, t, c, H, want_A=True)
+    assert rel(B, Bo) < TC_TOL[mode] and rel(A, Ao) < TC_TOL[mode]
