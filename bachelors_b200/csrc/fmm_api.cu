@@ -127,7 +127,7 @@ void Plan::release()
    DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
                      &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &parList, &m2lTargets, &m2lKeys, &errb,
                      &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf, &multBf, &tcCounters,
-                     &adjG, &adjOut, &nearCounts, &vtabUp, &vtabDn, &l2lTargets, &l2lKeys, &opM2Mbf, &opL2Lbf};
+                     &adjG, &adjOut, &nearCounts, &curlTab, &vtabUp, &vtabDn, &l2lTargets, &l2lKeys, &opM2Mbf, &opL2Lbf};
    for(DevBuf* b : bufs) b->release();
    for(auto& b : nodeBufs) b.release();
    for(auto& b : listBufs) b.release();

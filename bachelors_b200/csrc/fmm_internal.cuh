@@ -155,6 +155,8 @@ struct Plan
    // operator tables (scaled basis): FP64 masters and the working-precision copies
    DevBuf opM2M64, opL2L64, opM2L64;     // [8][L][L], [8][L][L], [316][L][L] FP64 row-major
    DevBuf opM2Mw, opL2Lw, opM2Lw;        // transposed working copies, see fmm_kernels.cu
+   DevBuf curlTab;                       // L2P: the curl expansion as <= 4 terms of the local, see kL2PWarp
+   std::vector<unsigned char> curlHost;  // its host copy (kept alive for the asynchronous upload)
    DevBuf opM2Lbf;                       // bf16 hi/lo split for the tensor-core M2L
    DevBuf multBf;                        // multipoles split into bf16 pieces for the tensor-core M2L
    int opOrder = -1;

@@ -15,6 +15,8 @@
 //         (B from analytic gradients here, finite differences there)
 //   near  bioSavartLaplaceFunction                           integration.cpp:113-120
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 
 #include <cuda_bf16.h>
 
@@ -185,6 +187,51 @@ __global__ void kTransposeOps(const double* __restrict__ src, int nops, int L, i
    }
 }
 
+// The gradient coefficients of kL2PNear's gradCoeff as terms: its value is sum_i c[i] Lv[idx[i]]
+// (the same case analysis, for tables).
+struct GradTerms
+{
+   int n;
+   int idx[2];
+   double c[2];
+};
+inline GradTerms gradTerms(int j, int lp, int mu)
+{
+   const int l = lp + 1;
+   const double h = 0.5, r2 = 0.70710678118654752440;
+   GradTerms g{0, {0, 0}, {0.0, 0.0}};
+   auto add = [&](double c, int m) {
+      if(std::abs(m) <= l) { g.idx[g.n] = hidx(l, m); g.c[g.n] = c; g.n++; }
+   };
+   if(j == 2) add(-1.0, mu);
+   else if(j == 0)
+   {
+      if(mu == 0) add(-r2, 1);
+      else if(mu == 1) { add(-h, 2); add(r2, 0); }
+      else if(mu >= 2) { add(-h, mu + 1); add(h, mu - 1); }
+      else if(mu == -1) add(-h, -2);
+      else { add(-h, mu - 1); add(h, mu + 1); }
+   }
+   else
+   {
+      if(mu == 0) add(-r2, -1);
+      else if(mu == 1) add(-h, -2);
+      else if(mu >= 2) { add(-h, -(mu + 1)); add(-h, -(mu - 1)); }
+      else if(mu == -1) { add(h, 2); add(r2, 0); }
+      else { add(h, 1 - mu); add(h, -mu - 1); }
+   }
+   return g;
+}
+// One entry of the L2P curl table: curl-expansion coefficient k' (degree <= p - 1), component c,
+// with the real-basis factor (-1)^l' (sqrt2 for m != 0) folded in, as <= 4 terms of the local
+// expansion row [3][Lp] of a box. Entries are [k'][4]; the fourth of each k' is empty.
+template <class T>
+struct CurlEntry
+{
+   int idx[4];
+   T c[4];
+};
+
 fmm_status buildOperators(Plan& P, cudaStream_t st)
 {
    if(P.opOrder == P.p) return FMM_OK;
@@ -222,6 +269,45 @@ fmm_status buildOperators(Plan& P, cudaStream_t st)
       FMM_TRY(launched(P, "kTransposeOps", st));
    }
    FMM_CHECK_LAUNCH();
+   // the L2P curl table in the plan's precision
+   {
+      const int Lb = nharm(p - 1);
+      const size_t esz = P.fp64 ? sizeof(CurlEntry<double>) : sizeof(CurlEntry<float>);
+      P.curlHost.assign(esz * 4 * Lb, 0);
+      for(int k = 0; k < Lb; k++)
+      {
+         int lp = 0;
+         while((lp + 1) * (lp + 1) <= k) lp++;
+         const int mu = k - lp * lp - lp;
+         const double f = ((lp & 1) ? -1.0 : 1.0) * (mu != 0 ? 1.4142135623730950488 : 1.0);
+         for(int c = 0; c < 3; c++)
+         {
+            // B_x = dAz/dy - dAy/dz, B_y = dAx/dz - dAz/dx, B_z = dAy/dx - dAx/dy
+            const int cp = (c + 2) % 3, cm = (c + 1) % 3, jp = (c + 1) % 3, jm = (c + 2) % 3;
+            const GradTerms gp = gradTerms(jp, lp, mu), gm = gradTerms(jm, lp, mu);
+            int idx[4] = {0, 0, 0, 0};
+            double cf[4] = {0, 0, 0, 0};
+            int n = 0;
+            for(int i = 0; i < gp.n; i++) { idx[n] = cp * Lp + gp.idx[i]; cf[n] = f * gp.c[i]; n++; }
+            for(int i = 0; i < gm.n; i++) { idx[n] = cm * Lp + gm.idx[i]; cf[n] = -f * gm.c[i]; n++; }
+            unsigned char* dst = P.curlHost.data() + esz * (4 * k + c);
+            if(P.fp64)
+            {
+               CurlEntry<double> e;
+               for(int i = 0; i < 4; i++) { e.idx[i] = idx[i]; e.c[i] = cf[i]; }
+               memcpy(dst, &e, sizeof(e));
+            }
+            else
+            {
+               CurlEntry<float> e;
+               for(int i = 0; i < 4; i++) { e.idx[i] = idx[i]; e.c[i] = float(cf[i]); }
+               memcpy(dst, &e, sizeof(e));
+            }
+         }
+      }
+      FMM_TRY(P.curlTab.reserve(P.curlHost.size()));
+      FMM_CUDA(cudaMemcpyAsync(P.curlTab.ptr, P.curlHost.data(), P.curlHost.size(), cudaMemcpyHostToDevice, st));
+   }
    P.opOrder = p;
    P.opImgOrder = -1;
    return FMM_OK;
@@ -1044,7 +1130,7 @@ template <class T, bool WANTA>
 inline size_t l2pWarpSmem(int p)
 {
    const int L = nharm(p), Lb = nharm(p - 1), nV = (p + 1) * (p + 2) / 2;
-   const size_t perWarp = size_t(4) * Lb + (WANTA ? size_t(4) * L : 0) + ((size_t(3) * L + 3) & ~size_t(3));
+   const size_t perWarp = size_t(4) * Lb + (WANTA ? size_t(4) * L : 0);
    return sizeof(T) * (size_t(4) * nV + L2PW_WARPS * perWarp);
 }
 
@@ -1052,7 +1138,8 @@ template <class T, bool WANTA>
 __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBox* __restrict__ rootp, int p,
                                                           int Lp, const T* __restrict__ Lc,
                                                           const typename Vec4<T>::type* __restrict__ tpos,
-                                                          const int* __restrict__ tOrder, int want,
+                                                          const int* __restrict__ tOrder,
+                                                          const CurlEntry<T>* __restrict__ curl, int want,
                                                           T* __restrict__ outB, T* __restrict__ outA)
 {
    typedef typename Vec4<T>::type V4;
@@ -1062,11 +1149,10 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
    const int q = WANTA ? p : p - 1;                     // highest degree visited
    const int nV = (p + 1) * (p + 2) / 2;                // table: degrees 0..p
    V4* tab = (V4*)smraw;
-   const int perWarp = 4 * Lb + (WANTA ? 4 * L : 0) + ((3 * L + 3) & ~3);
+   const int perWarp = 4 * Lb + (WANTA ? 4 * L : 0);
    T* wbase = (T*)(tab + nV) + warp * perWarp;
    V4* Cs = (V4*)wbase;                                 // [Lb] curl expansion
    V4* As = Cs + Lb;                                    // [L] local expansion (WANTA)
-   T* Ls = wbase + 4 * Lb + (WANTA ? 4 * L : 0);        // [3][L] local expansion as stored
    for(int v = threadIdx.x; v < nV; v += 32 * L2PW_WARPS)
    {
       int m = 0, r = v;
@@ -1089,37 +1175,27 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
    const int t0 = t.t0[node], t1 = t.t1[node];
    if(t1 == t0) return;
    const T* lc = Lc + int64_t(node) * 3 * Lp;
-   for(int e = lane; e < 3 * L; e += 32) Ls[e] = lc[(e / L) * Lp + e % L];
-   __syncwarp();
-   const T sq2 = T(1.4142135623730950488);
-   auto degreeOf = [](int k) {
-      int l = int(sqrtf(float(k)));
-      while(l * l > k) l--;
-      while((l + 1) * (l + 1) <= k) l++;
-      return l;
-   };
-   for(int e = lane; e < 3 * Lb; e += 32)
+   // the curl expansion from the table: each entry <= 4 terms of the box's local row
+   for(int e = lane; e < 4 * Lb; e += 32)
    {
-      const int c = e / Lb, k = e % Lb;
-      const int lp = degreeOf(k), mu = k - lp * lp - lp;
-      const T f = ((lp & 1) ? T(-1) : T(1)) * (mu != 0 ? sq2 : T(1));
-      // B_x = dAz/dy - dAy/dz, B_y = dAx/dz - dAz/dx, B_z = dAy/dx - dAx/dy
-      const int cp = (c + 2) % 3, cm = (c + 1) % 3;
-      const int jp = (c + 1) % 3, jm = (c + 2) % 3;
-      T* cs = (T*)(Cs + k);
-      cs[c] = f * (gradCoeff(Ls + cp * L, jp, lp, mu) - gradCoeff(Ls + cm * L, jm, lp, mu));
-      if(c == 0) cs[3] = T(0);
+      const CurlEntry<T> ce = curl[e];
+      ((T*)Cs)[e] = ce.c[0] * lc[ce.idx[0]] + ce.c[1] * lc[ce.idx[1]] + ce.c[2] * lc[ce.idx[2]] +
+                    ce.c[3] * lc[ce.idx[3]];
    }
    if(WANTA)
-      for(int e = lane; e < 3 * L; e += 32)
+   {
+      const T sq2 = T(1.4142135623730950488);
+      for(int e = lane; e < 4 * L; e += 32)
       {
-         const int c = e / L, k = e % L;
-         const int l = degreeOf(k), mu = k - l * l - l;
+         const int k = e >> 2, c = e & 3;
+         int l = int(sqrtf(float(k)));
+         while(l * l > k) l--;
+         while((l + 1) * (l + 1) <= k) l++;
+         const int mu = k - l * l - l;
          const T f = ((l & 1) ? T(-1) : T(1)) * (mu != 0 ? sq2 : T(1));
-         T* as = (T*)(As + k);
-         as[c] = f * Ls[e];
-         if(c == 0) as[3] = T(0);
+         ((T*)As)[e] = c < 3 ? f * lc[c * Lp + k] : T(0);
       }
+   }
    __syncwarp();
    const RootBox rb = rootp[rootOf(t, node)];
    double cen[3], h;
@@ -1136,9 +1212,34 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
       T B0 = T(0), B1 = T(0), B2 = T(0), A0 = T(0), A1 = T(0), A2 = T(0);
       T dre = T(1), dim = T(0);   // S_m^m
       int v = 0;
-      for(int m = 0; m <= q; m++)
+      // m = 0: real values only
       {
-         if(m > 0)
+         T are = T(1), bre = T(0);
+         int k0 = 0;
+         for(int l = 0; l <= q; l++, v++)
+         {
+            if(l > 0)
+            {
+               const V4 ab = tab[v];
+               const T cre = ab.x * uz * are - ab.y * r2 * bre;
+               bre = are; are = cre;
+               k0 += 2 * l;
+            }
+            if(!WANTA || l < p)
+            {
+               const V4 c0 = Cs[k0];
+               B0 += c0.x * are; B1 += c0.y * are; B2 += c0.z * are;
+            }
+            if(WANTA)
+            {
+               const V4 a0 = As[k0];
+               A0 += a0.x * are; A1 += a0.y * are; A2 += a0.z * are;
+            }
+         }
+         v += p - q;
+      }
+      for(int m = 1; m <= q; m++)
+      {
          {
             const T sc = tab[v].x;
             const T nre = (dre * ux - dim * uy) * sc;
@@ -1152,30 +1253,21 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
             if(l > m)
             {
                const V4 ab = tab[v];
-               const T cre = ab.x * uz * are - ab.y * r2 * bre;
-               const T cim = ab.x * uz * aim - ab.y * r2 * bim;
+               const T az = ab.x * uz, br = ab.y * r2;
+               const T cre = az * are - br * bre;
+               const T cim = az * aim - br * bim;
                bre = are; bim = aim; are = cre; aim = cim;
                k0 += 2 * l; k1 += 2 * l;
             }
             if(!WANTA || l < p)
             {
-               const V4 c0 = Cs[k0];
-               B0 += c0.x * are; B1 += c0.y * are; B2 += c0.z * are;
-               if(m > 0)
-               {
-                  const V4 c1 = Cs[k1];
-                  B0 += c1.x * aim; B1 += c1.y * aim; B2 += c1.z * aim;
-               }
+               const V4 c0 = Cs[k0], c1 = Cs[k1];
+               B0 += c0.x * are + c1.x * aim; B1 += c0.y * are + c1.y * aim; B2 += c0.z * are + c1.z * aim;
             }
             if(WANTA)
             {
-               const V4 a0 = As[k0];
-               A0 += a0.x * are; A1 += a0.y * are; A2 += a0.z * are;
-               if(m > 0)
-               {
-                  const V4 a1 = As[k1];
-                  A0 += a1.x * aim; A1 += a1.y * aim; A2 += a1.z * aim;
-               }
+               const V4 a0 = As[k0], a1 = As[k1];
+               A0 += a0.x * are + a1.x * aim; A1 += a0.y * are + a1.y * aim; A2 += a0.z * are + a1.z * aim;
             }
          }
          v += p - q;   // table entries of the degrees above q
@@ -1682,8 +1774,8 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
       auto runL2P = [&](auto kernel, size_t sh) -> fmm_status {
          if(sh > 48 * 1024) FMM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh)));
          kernel<<<int((N + L2PW_WARPS - 1) / L2PW_WARPS), 32 * L2PW_WARPS, sh, st>>>(
-            P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr, (const int*)P.tIdx.ptr, want,
-            (T*)P.outB.ptr, (T*)P.outA.ptr);
+            P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr, (const int*)P.tIdx.ptr,
+            (const CurlEntry<T>*)P.curlTab.ptr, want, (T*)P.outB.ptr, (T*)P.outA.ptr);
          return FMM_OK;
       };
       if(want & 2) FMM_TRY(runL2P(kL2PWarp<T, true>, l2pWarpSmem<T, true>(P.p)));
