@@ -708,27 +708,38 @@ __global__ void __launch_bounds__(32 * P2MW_WARPS) kP2MWarp(Tree t, const RootBo
          }
       }
       __syncwarp();
-      for(int i = 0; i < cnt; i++)
+      // two points per pass (independent recurrences sharing the table loads); an odd count's
+      // partner is a zero-strength point at the box centre
+      for(int i = 0; i < cnt; i += 2)
       {
+         const bool two = i + 1 < cnt;
          const T* pt = Pt + i * 8;
-         const T z = pt[2], r2 = pt[3], qc = pt[4 + c];
          const T* d = Ds + i * 2 * (p + 1);
+         const T z = pt[2], r2 = pt[3], qc = pt[4 + c];
+         const T z2 = two ? pt[8 + 2] : T(0), r22 = two ? pt[8 + 3] : T(0), qc2 = two ? pt[8 + 4 + c] : T(0);
+         const T* d2 = d + 2 * (p + 1);
          T are = d[2 * ma], aim = d[2 * ma + 1];
          const T bdr = d[2 * mb], bdi = d[2 * mb + 1];
-         T bre = T(0), bim = T(0);
-         accR[0] += qc * are;
-         accI[0] += qc * aim;
+         T are2 = two ? d2[2 * ma] : T(0), aim2 = two ? d2[2 * ma + 1] : T(0);
+         const T bdr2 = two ? d2[2 * mb] : T(0), bdi2 = two ? d2[2 * mb + 1] : T(0);
+         T bre = T(0), bim = T(0), bre2 = T(0), bim2 = T(0);
+         accR[0] += qc * are + qc2 * are2;
+         accI[0] += qc * aim + qc2 * aim2;
 #pragma unroll
          for(int j = 1; j < P2MW_STEPS; j++)
          {
             if(j > p + 1) break;
             const V4 k = AB[j * 32 + lane];
             const T az = k.x * z, br = k.y * r2;
+            const T az2 = k.x * z2, br2 = k.y * r22;
             const T cre = k.z * bdr + (az * are - br * bre);
             const T cim = k.z * bdi + (az * aim - br * bim);
+            const T cre2 = k.z * bdr2 + (az2 * are2 - br2 * bre2);
+            const T cim2 = k.z * bdi2 + (az2 * aim2 - br2 * bim2);
             bre = are; bim = aim; are = cre; aim = cim;
-            accR[j] += qc * are;
-            accI[j] += qc * aim;
+            bre2 = are2; bim2 = aim2; are2 = cre2; aim2 = cim2;
+            accR[j] += qc * are + qc2 * are2;
+            accI[j] += qc * aim + qc2 * aim2;
          }
       }
       __syncwarp();
@@ -1130,7 +1141,7 @@ template <class T, bool WANTA>
 inline size_t l2pWarpSmem(int p)
 {
    const int L = nharm(p), Lb = nharm(p - 1), nV = (p + 1) * (p + 2) / 2;
-   const size_t perWarp = size_t(4) * Lb + (WANTA ? size_t(4) * L : 0);
+   const size_t perWarp = size_t(4) * Lb + (WANTA ? size_t(4) * L : 0) + size_t(3) * padded(L);
    return sizeof(T) * (size_t(4) * nV + L2PW_WARPS * perWarp);
 }
 
@@ -1149,10 +1160,11 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
    const int q = WANTA ? p : p - 1;                     // highest degree visited
    const int nV = (p + 1) * (p + 2) / 2;                // table: degrees 0..p
    V4* tab = (V4*)smraw;
-   const int perWarp = 4 * Lb + (WANTA ? 4 * L : 0);
+   const int perWarp = 4 * Lb + (WANTA ? 4 * L : 0) + 3 * Lp;
    T* wbase = (T*)(tab + nV) + warp * perWarp;
    V4* Cs = (V4*)wbase;                                 // [Lb] curl expansion
    V4* As = Cs + Lb;                                    // [L] local expansion (WANTA)
+   T* Ls = wbase + 4 * Lb + (WANTA ? 4 * L : 0);        // [3][Lp] the box's local row
    for(int v = threadIdx.x; v < nV; v += 32 * L2PW_WARPS)
    {
       int m = 0, r = v;
@@ -1174,8 +1186,18 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
    if(node >= t.nNodes || t.nchild[node] != 0) return;
    const int t0 = t.t0[node], t1 = t.t1[node];
    if(t1 == t0) return;
-   const T* lc = Lc + int64_t(node) * 3 * Lp;
+   // the box's local row staged with 16-byte loads (Lp is a multiple of 16), all issued at once
+   {
+      typedef typename Vec4<T>::type V4g;
+      const V4g* src = reinterpret_cast<const V4g*>(Lc + int64_t(node) * 3 * Lp);
+      V4g* dst = reinterpret_cast<V4g*>(Ls);
+#pragma unroll 4
+      for(int e = lane; e < 3 * Lp / 4; e += 32) dst[e] = src[e];
+   }
+   __syncwarp();
+   const T* lc = Ls;
    // the curl expansion from the table: each entry <= 4 terms of the box's local row
+#pragma unroll 4
    for(int e = lane; e < 4 * Lb; e += 32)
    {
       const CurlEntry<T> ce = curl[e];
@@ -1201,64 +1223,58 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
    double cen[3], h;
    nodeCenter(rb, t.level[node], t.ix[node], t.iy[node], t.iz[node], cen, h);
    const T ih = T(1.0 / h), ih2 = T(1.0 / (h * h));
-   for(int base = t0; base < t1; base += 32)
+   // G lanes per target when the leaf is small (G = 4 up to 8 targets, 2 up to 16): group g of the
+   // W = 32 / G lanes visits the orders m = g, g + G, ..., and the groups' sums meet by shuffles
+   const int nt = t1 - t0;
+   const int G = nt <= 8 ? 4 : (nt <= 16 ? 2 : 1), W = 32 / G;
+   const int g = lane / W, jl = lane % W;
+   auto vStart = [&](int m) { return m * (p + 1) - m * (m - 1) / 2; };   // first visit of order m
+   for(int base = t0; base < t1; base += W)
    {
-      const int ti = base + lane;
+      const int ti = base + jl;
       const bool act = ti < t1;
       const V4 x = act ? tpos[ti] : V4{T(0), T(0), T(0), T(0)};
       const T ux = T((double(x.x) - cen[0]) / h), uy = T((double(x.y) - cen[1]) / h),
               uz = T((double(x.z) - cen[2]) / h);
       const T r2 = ux * ux + uy * uy + uz * uz;
       T B0 = T(0), B1 = T(0), B2 = T(0), A0 = T(0), A1 = T(0), A2 = T(0);
-      T dre = T(1), dim = T(0);   // S_m^m
-      int v = 0;
-      // m = 0: real values only
+      T dre = T(1), dim = T(0);   // S_m^m, advanced to this group's first order
+      for(int j = 1; j <= g; j++)
       {
-         T are = T(1), bre = T(0);
-         int k0 = 0;
-         for(int l = 0; l <= q; l++, v++)
-         {
-            if(l > 0)
-            {
-               const V4 ab = tab[v];
-               const T cre = ab.x * uz * are - ab.y * r2 * bre;
-               bre = are; are = cre;
-               k0 += 2 * l;
-            }
-            if(!WANTA || l < p)
-            {
-               const V4 c0 = Cs[k0];
-               B0 += c0.x * are; B1 += c0.y * are; B2 += c0.z * are;
-            }
-            if(WANTA)
-            {
-               const V4 a0 = As[k0];
-               A0 += a0.x * are; A1 += a0.y * are; A2 += a0.z * are;
-            }
-         }
-         v += p - q;
+         const T sc = tab[vStart(j)].x;
+         const T nre = (dre * ux - dim * uy) * sc;
+         const T nim = (dre * uy + dim * ux) * sc;
+         dre = nre; dim = nim;
       }
-      for(int m = 1; m <= q; m++)
+      // S_l^0 stays real (the imaginary parts are zero), so order 0 needs no case of its own: its
+      // k1 = k0 term adds zero
+      for(int m = g; m <= q; m += G)
       {
-         {
-            const T sc = tab[v].x;
-            const T nre = (dre * ux - dim * uy) * sc;
-            const T nim = (dre * uy + dim * ux) * sc;
-            dre = nre; dim = nim;
-         }
+         int v = vStart(m);
          T are = dre, aim = dim, bre = T(0), bim = T(0);
          int k0 = m * m + 2 * m, k1 = m * m;   // hidx(l, m), hidx(l, -m) at l = m
-         for(int l = m; l <= q; l++, v++)
+         if(!WANTA || m < p)
          {
-            if(l > m)
-            {
-               const V4 ab = tab[v];
-               const T az = ab.x * uz, br = ab.y * r2;
-               const T cre = az * are - br * bre;
-               const T cim = az * aim - br * bim;
-               bre = are; bim = aim; are = cre; aim = cim;
-               k0 += 2 * l; k1 += 2 * l;
-            }
+            const V4 c0 = Cs[k0], c1 = Cs[k1];
+            B0 += c0.x * are + c1.x * aim; B1 += c0.y * are + c1.y * aim; B2 += c0.z * are + c1.z * aim;
+         }
+         if(WANTA)
+         {
+            const V4 a0 = As[k0], a1 = As[k1];
+            A0 += a0.x * are + a1.x * aim; A1 += a0.y * are + a1.y * aim; A2 += a0.z * are + a1.z * aim;
+         }
+         v++;
+         // l = m + 1 .. q without branches; unrolled so that the table and coefficient loads, whose
+         // addresses do not depend on the recurrence, issue ahead of it
+#pragma unroll 4
+         for(int l = m + 1; l <= q; l++, v++)
+         {
+            const V4 ab = tab[v];
+            k0 += 2 * l; k1 += 2 * l;
+            const T az = ab.x * uz, br = ab.y * r2;
+            const T cre = az * are - br * bre;
+            const T cim = az * aim - br * bim;
+            bre = are; bim = aim; are = cre; aim = cim;
             if(!WANTA || l < p)
             {
                const V4 c0 = Cs[k0], c1 = Cs[k1];
@@ -1270,9 +1286,28 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
                A0 += a0.x * are + a1.x * aim; A1 += a0.y * are + a1.y * aim; A2 += a0.z * are + a1.z * aim;
             }
          }
-         v += p - q;   // table entries of the degrees above q
+         // S_m^m -> S_{m+G}^{m+G}
+         for(int j = m + 1; j <= m + G && j <= q; j++)
+         {
+            const T sc = tab[vStart(j)].x;
+            const T nre = (dre * ux - dim * uy) * sc;
+            const T nim = (dre * uy + dim * ux) * sc;
+            dre = nre; dim = nim;
+         }
       }
-      if(act)
+      for(int off = 16; off >= W; off >>= 1)
+      {
+         B0 += __shfl_down_sync(0xffffffffu, B0, off);
+         B1 += __shfl_down_sync(0xffffffffu, B1, off);
+         B2 += __shfl_down_sync(0xffffffffu, B2, off);
+         if(WANTA)
+         {
+            A0 += __shfl_down_sync(0xffffffffu, A0, off);
+            A1 += __shfl_down_sync(0xffffffffu, A1, off);
+            A2 += __shfl_down_sync(0xffffffffu, A2, off);
+         }
+      }
+      if(act && g == 0)
       {
          const int o = tOrder[ti];
          if(want & 1)
