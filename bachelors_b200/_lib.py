@@ -18,6 +18,7 @@ FMM_M2L_SIMT, FMM_M2L_BF16X3, FMM_M2L_TF32, FMM_M2L_BF16X6 = 0, 1, 2, 3
 # Every extern "C" symbol include/fmmcuda.h declares.
 EXPORTS = [
     "fmm_default_config", "fmm_plan_create", "fmm_plan_destroy", "fmm_set_sources", "fmm_set_targets",
+    "fmm_set_targets_to_sources",
     "fmm_build_tree", "fmm_upward", "fmm_downward", "fmm_evaluate", "fmm_solve", "fmm_direct",
     "fmm_direct_fp64_subset", "fmm_adjoint", "fmm_adjoint_direct", "fmm_autotune", "fmm_get_tuning",
     "fmm_set_tuning", "fmm_batch_set_coils", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
@@ -82,6 +83,7 @@ def load():
         "fmm_plan_destroy": (ctypes.c_int, [vp]),
         "fmm_set_sources": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.c_int, vp]),
         "fmm_set_targets": (ctypes.c_int, [vp, vp, i64, ctypes.c_int, vp]),
+        "fmm_set_targets_to_sources": (ctypes.c_int, [vp, vp]),
         "fmm_build_tree": (ctypes.c_int, [vp, vp]),
         "fmm_upward": (ctypes.c_int, [vp, vp]),
         "fmm_downward": (ctypes.c_int, [vp, vp]),

@@ -298,6 +298,24 @@ fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_de
    return FMM_OK;
 }
 
+fmm_status fmm_set_targets_to_sources(fmm_plan* plan, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(P.n > 0 && !P.srcXYZ) return setError(FMM_E_INVALID, "fmm_set_targets_to_sources: no sources set");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   const size_t bytes = es * 3 * size_t(P.n);
+   FMM_TRY(P.tgtXYZb.reserve(std::max<size_t>(bytes, 16)));
+   if(bytes) FMM_CUDA(cudaMemcpyAsync(P.tgtXYZb.ptr, P.srcXYZ, bytes, cudaMemcpyDeviceToDevice, st));
+   P.tgtXYZ = P.tgtXYZb.ptr;
+   P.m = P.n;
+   P.treeReady = P.upReady = P.downReady = false;
+   P.dropGraph();
+   return FMM_OK;
+}
+
 fmm_status fmm_build_tree(fmm_plan* plan, void* stream)
 {
    if(!plan) return setError(FMM_E_INVALID, "null plan");

@@ -150,10 +150,19 @@ class Plan:
         self.m = t.n
         self._keep.append(t)
 
+    def set_targets_to_sources(self):
+        """Targets = the source points just set (fmm_set_targets_to_sources): a device-side copy."""
+        _lib.check(self.lib.fmm_set_targets_to_sources(self.handle, self._stream()))
+        self.m = self.n
+
     def _out(self, rows=None):
         rows = self.m if rows is None else rows
         if self.device_mode:
             return torch.empty((rows, 3), dtype=self.torch_dtype, device=f"cuda:{self.cfg.device}")
+        if torch is not None and torch.cuda.is_available():
+            # page-locked host memory from torch's caching host allocator: the device-to-host copy
+            # runs at full DMA speed, and a result's block is reused once the array is released
+            return torch.empty((rows, 3), dtype=self.torch_dtype, pin_memory=True).numpy()
         return np.empty((rows, 3), dtype=self.np_dtype)
 
     @staticmethod
@@ -316,7 +325,10 @@ class FastMultipoleSolver(MultipoleSolver):
                          m2l_truncate=m2l_truncate, device=device, root=root)
         xyz, w, J = (tuple(quadratures) + (None,))[:3]
         self.plan.set_sources(xyz, w, J)
-        self.plan.set_targets(points)
+        if points is xyz:
+            self.plan.set_targets_to_sources()   # B at the quadrature points themselves
+        else:
+            self.plan.set_targets(points)
         self._multipoles = False
         self._locals = False
         self.harmonicOrder = int(order)

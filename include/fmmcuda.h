@@ -105,6 +105,10 @@ fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const
                            int on_device, void* stream);
 /* Targets xyz[3m] (FastMultipoleSolver's `points`, fast_multipole_solver.hpp:16). */
 fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_device, void* stream);
+/* Targets = the current source points, in source input order (no counterpart in the reference, whose
+ * FastMultipoleSolver always takes its own `points`): a device-side copy on `stream`, so a caller
+ * evaluating B at its own quadrature points moves them to the GPU once. */
+fmm_status fmm_set_targets_to_sources(fmm_plan* plan, void* stream);
 
 /* The reference's phases, for drop-in use of its call sequence
  * (FMM/FMMGPU/main.cpp:568-572):
