@@ -1248,12 +1248,9 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
       }
       // S_l^0 stays real (the imaginary parts are zero), so order 0 needs no case of its own: its
       // k1 = k0 term adds zero
-      for(int m = g; m <= q; m += G)
-      {
-         int v = vStart(m);
-         T are = dre, aim = dim, bre = T(0), bim = T(0);
-         int k0 = m * m + 2 * m, k1 = m * m;   // hidx(l, m), hidx(l, -m) at l = m
-         if(!WANTA || m < p)
+      // the contribution of one visited harmonic (l, m): coefficients k0 = hidx(l, m), k1 = hidx(l, -m)
+      auto visit = [&](int l, int k0, int k1, T are, T aim) {
+         if(!WANTA || l < p)
          {
             const V4 c0 = Cs[k0], c1 = Cs[k1];
             B0 += c0.x * are + c1.x * aim; B1 += c0.y * are + c1.y * aim; B2 += c0.z * are + c1.z * aim;
@@ -1263,37 +1260,61 @@ __global__ void __launch_bounds__(32 * L2PW_WARPS) kL2PWarp(Tree t, const RootBo
             const V4 a0 = As[k0], a1 = As[k1];
             A0 += a0.x * are + a1.x * aim; A1 += a0.y * are + a1.y * aim; A2 += a0.z * are + a1.z * aim;
          }
+      };
+      // S_{j-1}^{j-1} -> S_j^j
+      auto diag = [&](T& re, T& im, int j) {
+         const T sc = tab[vStart(j)].x;
+         const T nre = (re * ux - im * uy) * sc;
+         const T nim = (re * uy + im * ux) * sc;
+         re = nre; im = nim;
+      };
+      // orders m and m2 = m + G walked together: two independent recurrences in flight per lane
+      for(int m = g; m <= q; m += 2 * G)
+      {
+         const int m2 = m + G;
+         const bool two = m2 <= q;
+         T e2re = dre, e2im = dim;   // S_{m2}^{m2}
+         for(int j = m + 1; j <= m2 && j <= q; j++) diag(e2re, e2im, j);
+         int v = vStart(m), v2 = two ? vStart(m2) : 0;
+         T are = dre, aim = dim, bre = T(0), bim = T(0);
+         T are2 = e2re, aim2 = e2im, bre2 = T(0), bim2 = T(0);
+         int k0 = m * m + 2 * m, k1 = m * m, k02 = m2 * m2 + 2 * m2, k12 = m2 * m2;
+         visit(m, k0, k1, are, aim);
          v++;
-         // l = m + 1 .. q without branches; unrolled so that the table and coefficient loads, whose
-         // addresses do not depend on the recurrence, issue ahead of it
+         if(two)
+         {
+            visit(m2, k02, k12, are2, aim2);
+            v2++;
+         }
+         const int n2 = two ? q - m2 : 0;   // steps both orders take
+#pragma unroll 2
+         for(int st = 1; st <= n2; st++, v++, v2++)
+         {
+            const int l = m + st, l2 = m2 + st;
+            const V4 ab = tab[v], ab2 = tab[v2];
+            k0 += 2 * l; k1 += 2 * l; k02 += 2 * l2; k12 += 2 * l2;
+            const T az = ab.x * uz, br = ab.y * r2, az2 = ab2.x * uz, br2 = ab2.y * r2;
+            const T cre = az * are - br * bre, cim = az * aim - br * bim;
+            const T cre2 = az2 * are2 - br2 * bre2, cim2 = az2 * aim2 - br2 * bim2;
+            bre = are; bim = aim; are = cre; aim = cim;
+            bre2 = are2; bim2 = aim2; are2 = cre2; aim2 = cim2;
+            visit(l, k0, k1, are, aim);
+            visit(l2, k02, k12, are2, aim2);
+         }
+         // the rest of order m (all of it when m2 > q)
 #pragma unroll 4
-         for(int l = m + 1; l <= q; l++, v++)
+         for(int l = m + n2 + 1; l <= q; l++, v++)
          {
             const V4 ab = tab[v];
             k0 += 2 * l; k1 += 2 * l;
             const T az = ab.x * uz, br = ab.y * r2;
-            const T cre = az * are - br * bre;
-            const T cim = az * aim - br * bim;
+            const T cre = az * are - br * bre, cim = az * aim - br * bim;
             bre = are; bim = aim; are = cre; aim = cim;
-            if(!WANTA || l < p)
-            {
-               const V4 c0 = Cs[k0], c1 = Cs[k1];
-               B0 += c0.x * are + c1.x * aim; B1 += c0.y * are + c1.y * aim; B2 += c0.z * are + c1.z * aim;
-            }
-            if(WANTA)
-            {
-               const V4 a0 = As[k0], a1 = As[k1];
-               A0 += a0.x * are + a1.x * aim; A1 += a0.y * are + a1.y * aim; A2 += a0.z * are + a1.z * aim;
-            }
+            visit(l, k0, k1, are, aim);
          }
-         // S_m^m -> S_{m+G}^{m+G}
-         for(int j = m + 1; j <= m + G && j <= q; j++)
-         {
-            const T sc = tab[vStart(j)].x;
-            const T nre = (dre * ux - dim * uy) * sc;
-            const T nim = (dre * uy + dim * ux) * sc;
-            dre = nre; dim = nim;
-         }
+         // S_m^m -> S_{m+2G}^{m+2G}
+         dre = e2re; dim = e2im;
+         for(int j = m2 + 1; j <= m2 + G && j <= q; j++) diag(dre, dim, j);
       }
       for(int off = 16; off >= W; off >>= 1)
       {

@@ -316,8 +316,7 @@ __global__ void kListsLevel(Tree t, Lists L, int a, int b, int* err)
    if(D >= b) return;
    int P = t.parent[D];
    int ncol = 0, na = 0, nx = 0, nv = 0;
-   int* vt = L.vtab + int64_t(D) * 316;
-   for(int k = 0; k < 316; k++) vt[k] = -1;
+   int* vt = L.vtab + int64_t(D) * 316;   // preset to -1 for the whole tree before the levels
    const bool hasT = t.t1[D] > t.t0[D];
    auto coarse = [&](int S) {
       if(adjacentNodes(t, S, D))
@@ -364,7 +363,6 @@ __global__ void kListsLevel(Tree t, Lists L, int a, int b, int* err)
    L.nv[D] = nv;
 }
 
-// Direct-interaction source nodes of every target leaf (count pass when out == nullptr).
 // Statistics of the finished tree: out[0] += leaves, out[1] += direct (target, source) pairs the near
 // field evaluates (targets of a leaf x points of its direct-list nodes, the self pairs included).
 __global__ void kNearCounts(Tree t, int nNodes, const int* __restrict__ off, const int* __restrict__ list,
@@ -397,6 +395,7 @@ __global__ void kNearCounts(Tree t, int nNodes, const int* __restrict__ off, con
    }
 }
 
+// Direct-interaction source nodes of every target leaf (count pass when out == nullptr).
 __global__ void kP2PLists(Tree t, Lists L, int nNodes, const int* __restrict__ off, int* cnt, int* out, int* err)
 {
    int T = blockIdx.x * blockDim.x + threadIdx.x;
@@ -680,6 +679,8 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    FMM_TRY(P.ensureLists(total));
    Lists& Ls = P.lists;
    FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   // every node's M2L table starts empty: one fill here instead of 316 strided stores per node
+   FMM_CUDA(cudaMemsetAsync(Ls.vtab, 0xff, sizeof(int) * 316 * size_t(total), st));
    kInitRootLists<<<(K + 255) / 256, 256, 0, st>>>(Ls, K);
    FMM_TRY(launched(P, "kInitRootLists", st));
    for(int level = 1; level < nLevels; level++)
