@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <vector>
 
@@ -11,6 +12,38 @@
 #include "fmm_common.cuh"
 
 namespace fmm {
+
+// Four consecutive coefficients (columns col .. col + 3 of multipole row `row`) stored as the tensor-core
+// operand pieces: np = 1 one tf32 word each (round to nearest, ties away), np = 2 or 3 bf16 pieces, each the
+// round-to-nearest of the FP32 residual left by the previous ones (the residuals are exact in FP32).
+// Layout: [row][piece][Lp], 4 bytes an element for tf32 and 2 for bf16 (the tensor-core M2L's Mbf).
+__device__ __forceinline__ void storePieces4(uint8_t* out, int64_t row, int col, int Lp, int np, float4 v)
+{
+   if(np == 1)
+   {
+      uint32_t w[4];
+      const float x[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for(int i = 0; i < 4; i++) asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(w[i]) : "f"(x[i]));
+      *reinterpret_cast<uint4*>(out + (row * Lp + col) * 4) = make_uint4(w[0], w[1], w[2], w[3]);
+      return;
+   }
+   float r[4] = {v.x, v.y, v.z, v.w};
+   for(int j = 0; j < np; j++)
+   {
+      __nv_bfloat16 b[4];
+#pragma unroll
+      for(int i = 0; i < 4; i++)
+      {
+         b[i] = __float2bfloat16_rn(r[i]);
+         r[i] -= __bfloat162float(b[i]);
+      }
+      uint2 pk;
+      pk.x = uint32_t(__bfloat16_as_ushort(b[0])) | (uint32_t(__bfloat16_as_ushort(b[1])) << 16);
+      pk.y = uint32_t(__bfloat16_as_ushort(b[2])) | (uint32_t(__bfloat16_as_ushort(b[3])) << 16);
+      *reinterpret_cast<uint2*>(out + ((row * np + j) * Lp + col) * 2) = pk;
+   }
+}
 
 fmm_status setError(fmm_status s, const char* fmt, ...);
 
@@ -138,6 +171,7 @@ struct Plan
    std::vector<int> l2lStart;            // [8 level + octant], up to [8 nLevels]
    DevBuf opM2Mbf, opL2Lbf;              // their operator images
    int opTrImgTag = -1;
+   int p2mPiecesTag = -1;                // the piece format kP2MWarp also wrote the leaves in (-1: none)
    int multBfTag = -1;                   // pieces/format multBf holds the multipoles of every node in
                                          // (levels >= 1), -1 when it holds anything else
    int tcTranslate = 1;                  // M2M (1) / L2L (2) on the tensor cores in tensor-core M2L plans
@@ -230,6 +264,7 @@ fmm_status buildOperators(Plan& P, cudaStream_t st);
 fmm_status initOffsetTables();
 fmm_status m2lTensorCore(Plan& P, cudaStream_t st);
 fmm_status m2mTensorCore(Plan& P, cudaStream_t st);
+int m2mPieces(const Plan& P);   // operand pieces of the tensor-core M2M: 1 (tf32), 2 or 3 (bf16)
 fmm_status l2lTensorCore(Plan& P, cudaStream_t st);
 template <class T> fmm_status regatherStrengthsT(Plan& P, cudaStream_t st);
 template <class T> fmm_status scaleCopyT(Plan& P, const void* src, void* dst, int64_t count, double scale, cudaStream_t st);

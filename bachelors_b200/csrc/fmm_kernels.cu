@@ -640,7 +640,8 @@ template <class T>
 __global__ void __launch_bounds__(32 * P2MW_WARPS) kP2MWarp(Tree t, const RootBox* __restrict__ rootp,
                                                           const typename Vec4<T>::type* __restrict__ pos,
                                                           const typename Vec4<T>::type* __restrict__ q, int p,
-                                                          int Lp, T* __restrict__ M)
+                                                          int Lp, T* __restrict__ M, uint8_t* __restrict__ Mpieces,
+                                                          int np)
 {
    typedef typename Vec4<T>::type V4;
    extern __shared__ __align__(16) unsigned char smraw[];
@@ -771,6 +772,16 @@ __global__ void __launch_bounds__(32 * P2MW_WARPS) kP2MWarp(Tree t, const RootBo
    __syncwarp();
    T* out = M + int64_t(node) * 3 * Lp;
    for(int e = lane; e < 3 * Lp; e += 32) out[e] = Mst[e];
+   // the same coefficients as tensor-core operand pieces (the M2M's and M2L's input format), so the
+   // upward pass needs no separate split of the leaves
+   if constexpr(sizeof(T) == 4)
+      if(Mpieces)
+         for(int e4 = lane; e4 < 3 * Lp / 4; e4 += 32)
+         {
+            const int e = 4 * e4;
+            const float4 v = make_float4(Mst[e], Mst[e + 1], Mst[e + 2], Mst[e + 3]);
+            storePieces4(Mpieces, int64_t(node) * 3 + e / Lp, e % Lp, Lp, np, v);
+         }
 }
 
 // ====================================================================================
@@ -1715,15 +1726,26 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
       const size_t shw = p2mWarpSmem<T>(P.p, Lp);
       if(shw > 48 * 1024)
          FMM_CUDA(cudaFuncSetAttribute(kP2MWarp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shw)));
+      // tensor-core M2M plans: the leaves' multipoles also leave as the M2M's operand pieces
+      int np = 0;
+      if(sizeof(T) == 4 && P.tcTranslations(1) && P.tcDrainMode != 0) np = m2mPieces(P);
+      if(np)
+         FMM_TRY(P.multBf.reserve(size_t(np == 1 ? 4 : 2 * np) * size_t(N) * 3 * Lp));
       kP2MWarp<T><<<int((N + P2MW_WARPS - 1) / P2MW_WARPS), 32 * P2MW_WARPS, shw, st>>>(
-         P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp, (T*)P.mult.ptr);
+         P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp, (T*)P.mult.ptr,
+         np ? (uint8_t*)P.multBf.ptr : nullptr, np);
+      P.p2mPiecesTag = np ? (np == 1 ? 3 : 2 * np) : -1;
    }
-   else if(P.p2mChunk == 32)
-      kP2M<T, NT, 32><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
-                                              (T*)P.mult.ptr);
    else
-      kP2M<T, NT, 16><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p, Lp,
-                                              (T*)P.mult.ptr);
+   {
+      P.p2mPiecesTag = -1;
+      if(P.p2mChunk == 32)
+         kP2M<T, NT, 32><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p,
+                                                 Lp, (T*)P.mult.ptr);
+      else
+         kP2M<T, NT, 16><<<int(N), NT, shm, st>>>(P.tree, P.root, (const V4*)P.sPos.ptr, (const V4*)P.sQ.ptr, P.p,
+                                                 Lp, (T*)P.mult.ptr);
+   }
    FMM_TRY(launched(P, "kP2M", st));
    FMM_CHECK_LAUNCH();
    if(P.tcTranslations(1)) return m2mTensorCore(P, st);

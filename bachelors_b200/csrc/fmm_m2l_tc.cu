@@ -333,12 +333,13 @@ __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int 
 }
 
 // 18 warps: five of them share one SM sub-partition's 16K registers, so 96 per thread at most.
-template <int NP, class Lay>
+// PIECES: the final outputs are also stored as operand pieces (Mout); the M2M's form.
+template <int NP, class Lay, bool PIECES = false>
 __global__ void __maxnreg__(96)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int nOps, int L, int Lp,
        int nChunks, const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc,
-       int addOut, int drainEvery, int drainItems, int nStages, int drainMode, const M2LCols cols,
-       unsigned long long* counters, int* err)
+       int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainItems, int nStages, int drainMode,
+       const M2LCols cols, unsigned long long* counters, int* err)
 {
    using namespace tc;
    constexpr int KCH = Lay::KC;
@@ -603,6 +604,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                         v = make_float4(w.x + v.x, w.y + v.y, w.z + v.z, w.w + v.w);
                      }
                      o4[i] = v;
+                     if(PIECES) storePieces4(Mout, int64_t(et) * 3 + ec, c0 + 4 * i, Lp, Lay::TF32 ? 1 : NP, v);
                   }
                }
             }
@@ -635,6 +637,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                      v = make_float4(w.x + v.x, w.y + v.y, w.z + v.z, w.w + v.w);
                   }
                   o4[i] = v;
+                  if(PIECES) storePieces4(Mout, int64_t(et) * 3 + ec, c0 + 4 * i, Lp, Lay::TF32 ? 1 : NP, v);
                }
             }
          }
@@ -660,8 +663,13 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                const float4 v = make_float4(__uint_as_float(u[4 * i]), __uint_as_float(u[4 * i + 1]),
                                             __uint_as_float(u[4 * i + 2]), __uint_as_float(u[4 * i + 3]));
                if(drainMode == 0) atomicAdd(o4 + i, v);
-               else if(!rmw) o4[i] = v;
-               else o4[i] = make_float4(old[i].x + v.x, old[i].y + v.y, old[i].z + v.z, old[i].w + v.w);
+               else
+               {
+                  const float4 f = rmw ? make_float4(old[i].x + v.x, old[i].y + v.y, old[i].z + v.z, old[i].w + v.w) : v;
+                  o4[i] = f;
+                  // (Mout is only given with drainMode != 0: atomics leave the final value unknown here)
+                  if(PIECES && last) storePieces4(Mout, int64_t(et) * 3 + ec, c0 + 4 * i, Lp, Lay::TF32 ? 1 : NP, f);
+               }
             }
          }
          fenceBeforeSync();
@@ -789,7 +797,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    }
    kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
                                                       nChunks, (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
-                                                      (float*)P.local.ptr, 0, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
+                                                      (float*)P.local.ptr, 0, nullptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
                                                       0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
@@ -834,6 +842,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core translation: %zu-byte stages do not fit twice", stageBytes);
    const size_t smem = fixed + nStages * stageBytes;
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    M2LCols cols{};
    const int nSteps = nChunks * (Lay::KC / Lay::KSTEP);
    if(nSteps > MAXKSTEPS) return setError(FMM_E_INVALID, "tensor-core translation: %d K steps exceed the column table", nSteps);
@@ -853,15 +862,20 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
    };
    if(up)
    {
+      // the warp P2M already wrote the leaves in this piece format: then every parent's pieces come out
+      // of its M2M launch (Mout) and no level is split separately
+      const int tag = NP * 2 + (Lay::TF32 ? 1 : 0);
+      const bool fused = P.p2mPiecesTag == tag && P.tcDrainMode != 0;
       for(int level = t.nLevels - 2; level >= 0; level--)
       {
          const int a = P.parStart[level], b = P.parStart[level + 1];
          if(b <= a) continue;
-         FMM_TRY(split((const float*)P.mult.ptr, level + 1));
-         kM2LTc<NP, Lay><<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
+         if(!fused) FMM_TRY(split((const float*)P.mult.ptr, level + 1));
+         auto kern = fused ? kM2LTc<NP, Lay, true> : kM2LTc<NP, Lay, false>;
+         kern<<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.parList.ptr + a, b - a, (const int*)P.vtabUp.ptr, 8, L, Lp, nChunks,
-            (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0, drainEvery, P.tcTrDrainItems, nStages,
-            P.tcDrainMode, cols, nullptr, P.err);
+            (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0,
+            (uint8_t*)P.multBf.ptr, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.err);
          FMM_TRY(launched(P, "kM2LTc<M2M>", st));
       }
       P.multBfTag = NP * 2 + (Lay::TF32 ? 1 : 0);
@@ -875,7 +889,8 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          FMM_TRY(split((const float*)P.local.ptr, level));
          kM2LTc<NP, Lay><<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.l2lTargets.ptr + a, b - a, (const int*)P.vtabDn.ptr, 8, L, Lp, nChunks,
-            (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, drainEvery, P.tcTrDrainItems, nStages,
+            (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, nullptr, drainEvery,
+            P.tcTrDrainItems, nStages,
             P.tcDrainMode, cols, nullptr, P.err);
          FMM_TRY(launched(P, "kM2LTc<L2L>", st));
       }
@@ -903,6 +918,14 @@ static fmm_status translateTensorCore(Plan& P, cudaStream_t st, bool up)
    if(P.cfg.m2l_mode == FMM_M2L_BF16X6)
       return P.tcKChunk == 64 ? translateTc<3, Layout<64>>(P, st, up) : translateTc<3, Layout<32>>(P, st, up);
    return translateTc<1, tc::LayoutTf32>(P, st, up);
+}
+
+int m2mPieces(const Plan& P)
+{
+   if(P.tcTrPiecesUp == 2 || P.tcTrPiecesUp == 3) return P.tcTrPiecesUp;
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X3) return 2;
+   if(P.cfg.m2l_mode == FMM_M2L_BF16X6) return 3;
+   return 1;
 }
 
 fmm_status m2mTensorCore(Plan& P, cudaStream_t st) { return translateTensorCore(P, st, true); }
