@@ -96,6 +96,8 @@ fmm_status Plan::init(const fmm_config& c)
    }
    if(const char* e = getenv("FMM_TC_KC")) tcKChunk = atoi(e) == 32 ? 32 : 64;
    if(const char* e = getenv("FMM_TC_DRAIN")) tcDrainEvery = std::max(1, atoi(e));
+   tcDrainFar = tcDrainEvery;
+   if(const char* e = getenv("FMM_TC_DRAINFAR")) tcDrainFar = std::max(1, atoi(e));
    if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(3, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
    if(const char* e = getenv("FMM_L2P_SPLIT")) l2pSplit = atoi(e) != 0;

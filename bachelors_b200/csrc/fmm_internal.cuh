@@ -196,6 +196,7 @@ struct Plan
    int opOrder = -1;
    // tensor-core M2L tile choices (autotuned per order and leaf capacity, or set by environment)
    int tcKChunk = 0;                     // K chunk width 32 or 64 (0: 64 for BF16X3, 32 for BF16X6)
+   int tcDrainFar = 8;                   // the same through the first (far) half of a tile's offsets
    int tcDrainEvery = 8;                 // offsets accumulated in tensor memory between drains (BF16X6,
                                          // with twice the accumulations per offset, drains twice as often)
    int tcDrainMode = 3;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1,

@@ -332,13 +332,26 @@ __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int 
    }
 }
 
+// Whether the accumulator is drained after the oi-th of nOff offsets: every dNear offsets, and, when
+// dFar differs, every dFar offsets through the first (far) half of the offsets, which ends with a drain.
+// Offsets run far first, so the first half holds the small contributions: the tensor core's accumulation
+// error grows with the magnitude accumulated, and longer chains there cost little accuracy.
+__device__ __forceinline__ bool drainAfter(int oi, int nOff, int dNear, int dFar)
+{
+   if(oi == nOff - 1) return true;
+   if(dFar == dNear) return (oi + 1) % dNear == 0;
+   const int half = nOff / 2;
+   if(oi < half) return (oi + 1) % dFar == 0 || oi == half - 1;
+   return (oi + 1 - half) % dNear == 0;
+}
+
 // 18 warps: five of them share one SM sub-partition's 16K registers, so 96 per thread at most.
 // PIECES: the final outputs are also stored as operand pieces (Mout); the M2M's form.
 template <int NP, class Lay, bool PIECES = false>
 __global__ void __maxnreg__(96)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int nOps, int L, int Lp,
        int nChunks, const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc,
-       int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainItems, int nStages, int drainMode,
+       int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainFar, int drainItems, int nStages, int drainMode,
        const M2LCols cols, unsigned long long* counters, int* err)
 {
    using namespace tc;
@@ -498,7 +511,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             // a fresh accumulation must start with an MMA that writes every column)
             const bool drainNow = drainItems > 0 ? ((it + 1) % drainItems == 0 || it == nItems - 1)
                                                  : (it % nChunks == nChunks - 1 &&
-                                                    ((it / nChunks + 1) % drainEvery == 0 || it == nItems - 1));
+                                                    drainAfter(it / nChunks, nOff, drainEvery, drainFar));
             {
                if(drainNow)
                {
@@ -547,7 +560,10 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       const int et = r < 3 * TT ? tileNode[r / 3] : -1, ec = r % 3;
       float* out = Lc + (int64_t(et) * 3 + ec) * Lp;
       const uint32_t tAcc = tmem + (uint32_t(lanes) << 16);
-      const int nDrains = drainItems > 0 ? (nItems + drainItems - 1) / drainItems : (nOff + drainEvery - 1) / drainEvery;
+      int nDrains = 0;
+      if(drainItems > 0) nDrains = (nItems + drainItems - 1) / drainItems;
+      else
+         for(int oi = 0; oi < nOff; oi++) nDrains += drainAfter(oi, nOff, drainEvery, drainFar) ? 1 : 0;
       // The running sum is FP32, rounded to nearest, and has one writer per row and column (this
       // thread); the locals start at zero and no other CTA touches these rows, so the result is
       // deterministic. Its columns live in three parts:
@@ -798,7 +814,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
                                                       nChunks, (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
                                                       (float*)P.local.ptr, 0, nullptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
-                                                      0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.err);
+                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.err);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
    int herr = 0;
@@ -875,7 +891,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          kern<<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.parList.ptr + a, b - a, (const int*)P.vtabUp.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0,
-            (uint8_t*)P.multBf.ptr, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.err);
+            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.err);
          FMM_TRY(launched(P, "kM2LTc<M2M>", st));
       }
       P.multBfTag = NP * 2 + (Lay::TF32 ? 1 : 0);
@@ -889,7 +905,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          FMM_TRY(split((const float*)P.local.ptr, level));
          kM2LTc<NP, Lay><<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.l2lTargets.ptr + a, b - a, (const int*)P.vtabDn.ptr, 8, L, Lp, nChunks,
-            (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, nullptr, drainEvery,
+            (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, nullptr, drainEvery, drainEvery,
             P.tcTrDrainItems, nStages,
             P.tcDrainMode, cols, nullptr, P.err);
          FMM_TRY(launched(P, "kM2LTc<L2L>", st));
