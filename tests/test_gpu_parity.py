@@ -1,5 +1,5 @@
 """Parity of the device pipeline (through the C ABI) with the CPU restatement on the same
-inputs, tree and lists. FP64: relative L2 <= 1e-12; FP32: <= 1e-5 (BASELINE tolerances)."""
+inputs, tree and lists. FP64: relative L2 <= 1e-12; FP32: <= 1e-5."""
 import numpy as np
 import pytest
 
