@@ -522,6 +522,17 @@ void orc_solid_harmonics_grad(int p, int regular, const double* xyz, double* out
       for(int j = 0; j < 3; j++) out[3 * k + j] = h[k].d[j];
 }
 
+// The same gradient in either convention (compat != 0: the reference's).
+void orc_solid_harmonics_grad2(int p, int regular, int compat, const double* xyz, double* out)
+{
+   std::vector<Dual> h(nharm(p));
+   Dual x(xyz[0]), y(xyz[1]), z(xyz[2]);
+   x.d[0] = 1; y.d[1] = 1; z.d[2] = 1;
+   solidHarmonics<Dual>(p, x, y, z, regular != 0, compat != 0, h.data());
+   for(int k = 0; k < nharm(p); k++)
+      for(int j = 0; j < 3; j++) out[3 * k + j] = h[k].d[j];
+}
+
 // P2M about `center` from n points xyz[3n] with weights w[n] and current directions J[3n]
 // (J == nullptr: the reference's azimuthal direction). out[(p+1)^2][3].
 void orc_p2m(int p, int compat, int64_t n, const double* xyz, const double* w, const double* J,

@@ -60,6 +60,71 @@ def solid_harmonics_grad(p, xyz, regular=True):
     return out
 
 
+def solid_harmonics_grad2(p, xyz, regular=True, compat=False):
+    """Gradient of the real solid harmonics in either convention: out[(p+1)^2][3]."""
+    out = np.zeros((nharm(p), 3))
+    _load().orc_solid_harmonics_grad2(p, int(regular), int(compat), _d(_c64(xyz)), _d(out))
+    return out
+
+
+# ----------------------------------------------------------------------------------------------
+# BEM problem (the reference's Problem::BEM; FMM/FMMGPU/integration.cpp:191-215, 295-353). A BEM
+# quadrature carries a point q, a weight w, a field value B and a surface normal n; its kernel at x is
+#   K(x) = w [d (B . n) + d x (B x n)] / |d|^3,   d = q - x,
+# and the integral is sum_q K(x) / (4 pi). Each component c is the potential of point dipoles
+# (d / |d|^3 = grad_x 1/|x - q|), so its multipole about a centre c0 is
+#   M_k = -sum_q w [g_k (B . n) + g_k x (B x n)],   g_k = grad R_k(q - c0),
+# evaluated as sum_k M_k I_k(x - c0) / (4 pi) (calcBEM: the potential path, no current factor).
+# ----------------------------------------------------------------------------------------------
+REF_PI = 3.14159265359   # the reference's math::PI
+
+
+def bem_direct(src, w, B, nrm, tgt):
+    """Direct BEM integral at tgt (math::calcBEMIntegral, integration.cpp:191-215), FP64; a quadrature
+    that coincides with a target contributes nothing."""
+    src = _c64(src).reshape(-1, 3)
+    tgt = _c64(tgt).reshape(-1, 3)
+    w = _c64(w)
+    Bn = np.einsum("ij,ij->i", _c64(B).reshape(-1, 3), _c64(nrm).reshape(-1, 3))
+    v = np.cross(_c64(B).reshape(-1, 3), _c64(nrm).reshape(-1, 3))
+    out = np.zeros((len(tgt), 3))
+    for j, x in enumerate(tgt):
+        d = src - x
+        r = np.sqrt(np.einsum("ij,ij->i", d, d))
+        ok = r > 0
+        inv3 = np.zeros_like(r)
+        inv3[ok] = 1.0 / r[ok] ** 3
+        k = (d * Bn[:, None] + np.cross(d, v)) * (w * inv3)[:, None]
+        out[j] = k.sum(axis=0) / (4 * REF_PI)
+    return out
+
+
+def bem_p2m(p, src, w, B, nrm, center, compat=True, fd_eps=None):
+    """BEM multipole about `center` (calcBEMIntegralContribution, integration.cpp:295-353): out[(p+1)^2][3].
+    fd_eps=None takes the analytic gradient of the regular harmonics; a value takes the reference's central
+    differences with that step (the reference uses math::eps = 1e-3)."""
+    src = _c64(src).reshape(-1, 3)
+    w = _c64(w)
+    Bv = _c64(B).reshape(-1, 3)
+    nv = _c64(nrm).reshape(-1, 3)
+    c0 = _c64(center)
+    out = np.zeros((nharm(p), 3))
+    for i in range(len(src)):
+        t = src[i] - c0
+        if fd_eps is None:
+            g = solid_harmonics_grad2(p, t, True, compat)
+        else:
+            g = np.zeros((nharm(p), 3))
+            for a in range(3):
+                e = np.zeros(3)
+                e[a] = fd_eps
+                g[:, a] = (solid_harmonics(p, t + e, True, compat) - solid_harmonics(p, t - e, True, compat)) / (2 * fd_eps)
+        first = g * np.dot(Bv[i], nv[i])
+        second = np.cross(g, np.cross(Bv[i], nv[i]))
+        out -= (first + second) * w[i]
+    return out
+
+
 def p2m(p, xyz, w, J=None, center=(0, 0, 0), compat=False):
     xyz = _c64(xyz).reshape(-1, 3)
     w = _c64(w)
@@ -198,6 +263,26 @@ class Reference:
     def irregular(self, p, xyz):
         out = np.zeros(nharm(p))
         self.lib.ref_irregular(p, _d(_c64(xyz)), _d(out))
+        return out
+
+    @staticmethod
+    def _bem_rows(src, w, B, nrm):
+        return np.ascontiguousarray(np.concatenate([_c64(src).reshape(-1, 3), _c64(w).reshape(-1, 1),
+                                                    _c64(B).reshape(-1, 3), _c64(nrm).reshape(-1, 3)], axis=1))
+
+    def bem_direct(self, src, w, B, nrm, tgt):
+        """math::calcBEMIntegral at each target."""
+        q = self._bem_rows(src, w, B, nrm)
+        tgt = _c64(tgt).reshape(-1, 3)
+        out = np.zeros((len(tgt), 3))
+        self.lib.ref_bem_direct(len(q), _d(q), len(tgt), _d(tgt), _d(out))
+        return out
+
+    def bem_p2m(self, p, src, w, B, nrm, center):
+        """math::calcBEMIntegralContribution about `center`."""
+        q = self._bem_rows(src, w, B, nrm)
+        out = np.zeros((nharm(p), 3))
+        self.lib.ref_bem_p2m(p, len(q), _d(q), _d(_c64(center)), _d(out))
         return out
 
     def p2m(self, p, xyzw, center):

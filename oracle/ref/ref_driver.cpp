@@ -16,6 +16,7 @@
 //   kernels::translateAllCPU, translateAllCPUMatrixBLAS                   translation_algorithms_cpu.cpp:9-135
 //   Torus (hexahedra -> 5 tetrahedra) + math::tetrahedraToQuadratures     torus.cpp:9-117, integration.cpp:163-187
 //   FastMultipoleSolver full B / A pipeline                               fast_multipole_solver.cpp:12-231
+//   math::calcBEMIntegral, calcBEMIntegralContribution (BEM problem)     integration.cpp:191-215, 295-353
 #include <chrono>
 #include <cstdint>
 #include <cstring>
@@ -30,6 +31,7 @@
 #include "translation_algorithms.hpp"
 #include "torus.hpp"
 #include "basis_quadratures.hpp"
+#include "bem_quadrature.hpp"
 
 namespace {
 HarmonicSeries<Vector3> toSeries(int order, const double* in)
@@ -62,6 +64,19 @@ struct KeyHash
       return h;
    }
 };
+// BEM quadratures from rows (x, y, z, weight, Bx, By, Bz, nx, ny, nz).
+std::vector<BEMQuadrature> bemQuadratures(int n, const double* q)
+{
+   std::vector<BEMQuadrature> r;
+   r.reserve(n);
+   for(int i = 0; i < n; i++)
+   {
+      const double* e = q + 10 * i;
+      r.emplace_back(Vector3(real(e[0]), real(e[1]), real(e[2])), real(1), real(e[3]),
+                     Vector3(real(e[4]), real(e[5]), real(e[6])), Vector3(real(e[7]), real(e[8]), real(e[9])));
+   }
+   return r;
+}
 double seconds(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b)
 {
    return std::chrono::duration<double>(b - a).count();
@@ -162,6 +177,28 @@ int ref_torus_quadratures(double radius, double width, int nL, int nW, int nH, c
          out[4 * i] = q[i].x; out[4 * i + 1] = q[i].y; out[4 * i + 2] = q[i].z; out[4 * i + 3] = q[i].weight;
       }
    return int(q.size());
+}
+
+// math::calcBEMIntegral at m points over n BEM quadratures (rows as bemQuadratures): out[3m].
+void ref_bem_direct(int n, const double* q, int m, const double* pts, double* out)
+{
+   const std::vector<BEMQuadrature> bq = bemQuadratures(n, q);
+   for(int j = 0; j < m; j++)
+   {
+      Vector3 r = math::calcBEMIntegral(Vector3(real(pts[3 * j]), real(pts[3 * j + 1]), real(pts[3 * j + 2])), bq);
+      out[3 * j] = r.x; out[3 * j + 1] = r.y; out[3 * j + 2] = r.z;
+   }
+}
+
+// math::calcBEMIntegralContribution (the BEM P2M, central differences of the regular harmonics) about
+// `center`: out[(p+1)^2][3].
+void ref_bem_p2m(int order, int n, const double* q, const double* center, double* out)
+{
+   std::vector<BEMQuadrature> bq = bemQuadratures(n, q);
+   std::vector<Quadrature*> ptrs(n);
+   for(int i = 0; i < n; i++) ptrs[i] = &bq[i];
+   auto res = math::calcBEMIntegralContribution(ptrs, order, Vector3(real(center[0]), real(center[1]), real(center[2])));
+   fromSeries(res, out);
 }
 
 // A(x) = sum_k local_k * R_k(d), d = x - center (no 1/(4 pi) or current factor).

@@ -4,7 +4,7 @@ Runs the patched reference build (oracle/_ref/libref_fmm_*.so, made by oracle/re
 from the reference sources) on seeded inputs and stores inputs and outputs as .npz. The
 reference is not needed afterwards: the tests read only the .npz files.
 
-Usage: python tests/golden/make_golden.py [main] [seam] [telma]   (default: all)
+Usage: python tests/golden/make_golden.py [main] [seam] [telma] [bem]   (default: all)
 The reference sources are read from REFERENCE_ROOT (default /root/reference).
 """
 import os
@@ -125,8 +125,39 @@ def telma():
     print("wrote", path, len(out), "arrays")
 
 
+def bem_case(rng, n=48, m=24):
+    """Seeded BEM quadratures on a cylinder surface (radius 0.3, height 0.6, outward normals, smooth B),
+    targets on a sphere of radius 3 around it."""
+    phi = rng.uniform(0, 2 * np.pi, n)
+    zz = rng.uniform(-0.3, 0.3, n)
+    src = np.stack([0.3 * np.cos(phi), 0.3 * np.sin(phi), zz], axis=1)
+    nrm = np.stack([np.cos(phi), np.sin(phi), np.zeros(n)], axis=1)
+    B = np.stack([0.2 * zz, 1.0 + 0.1 * np.sin(phi), 0.5 * np.cos(phi)], axis=1) + rng.normal(size=(n, 3)) * 0.05
+    w = rng.uniform(0.5, 1.5, n) * (2 * np.pi * 0.3 * 0.6 / n)
+    u = rng.normal(size=(m, 3))
+    tgt = 3.0 * u / np.linalg.norm(u, axis=1)[:, None]
+    return src, w, B, nrm, tgt
+
+
+def bem():
+    """The reference's BEM kernels (integration.cpp:191-215, 295-353): direct integral and P2M."""
+    rng = np.random.default_rng(20260006)
+    ref = Reference("f64", 10)
+    src, w, B, nrm, tgt = bem_case(rng)
+    out = {"src": src, "w": w, "B": B, "nrm": nrm, "tgt": tgt, "direct": ref.bem_direct(src, w, B, nrm, tgt)}
+    for p in (4, 10):
+        c = rng.normal(size=3) * 0.05
+        out[f"p2m_p{p}_center"] = c
+        out[f"p2m_p{p}"] = ref.bem_p2m(p, src, w, B, nrm, c)
+    path = os.path.join(HERE, "reference_bem.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, len(out), "arrays")
+
+
 if __name__ == "__main__":
-    what = sys.argv[1:] or ["main", "seam", "telma"]
+    what = sys.argv[1:] or ["main", "seam", "telma", "bem"]
+    if "bem" in what:
+        bem()
     if "telma" in what:
         telma()
     if "main" in what:
