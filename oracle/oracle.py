@@ -125,6 +125,84 @@ def bem_p2m(p, src, w, B, nrm, center, compat=True, fd_eps=None):
     return out
 
 
+# ----------------------------------------------------------------------------------------------
+# The reference's treecode (MultipoleSolver::calcB, multipole_solver.cpp:686-700): one source octree,
+# leaf P2M and complex-translation M2M, then per point a descent that takes a node's multipole when
+# 4 r^2 < d^2 (r the box radius, d the distance to its centre) and otherwise its children; a close
+# leaf contributes nothing (quadrature_octree.cpp:196-258). The curl uses central differences of the
+# irregular harmonics (step 1e-3), as there.
+# ----------------------------------------------------------------------------------------------
+REF_MU0 = 1.2566370614e-6   # the reference's math::MU0
+_OCTANTS = ((-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1), (-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1))
+
+
+def _tc_build(xyz, idx, c, h, cap):
+    """Node of the reference's quadrature octree (quadrature_octree.cpp:23-97): a box with cap or more
+    points is split into 8 children whose centres and half-widths are computed in float; points are
+    assigned by the half-open box test (box.cpp:13-24), keeping their input order."""
+    node = {"c": c, "h": h, "idx": idx, "children": []}
+    if len(idx) >= cap:
+        fc = np.float32(c)
+        fh = np.float32(h)
+        ch = (fh / np.float32(2)).astype(np.float64)
+        for sgn in _OCTANTS:
+            cc = np.array([fc[a] + np.float32(sgn[a]) * (fh[a] / np.float32(2)) for a in range(3)],
+                          dtype=np.float32).astype(np.float64)
+            p = xyz[idx]
+            inside = np.all((cc - ch <= p) & (p < cc + ch), axis=1)
+            node["children"].append(_tc_build(xyz, idx[inside], cc, ch, cap))
+        node["idx"] = idx[:0]
+    return node
+
+
+def _tc_upward(node, p, xyz, w):
+    if len(node["idx"]) > 0:   # a leaf with points: P2M (integration.cpp:137-161)
+        node["M"] = p2m(p, xyz[node["idx"]], w[node["idx"]], None, node["c"], compat=True)
+        return
+    node["M"] = np.zeros((nharm(p), 3))
+    for ch in node["children"]:
+        _tc_upward(ch, p, xyz, w)
+    for ch in node["children"]:   # non-empty leaves and subdivided nodes (quadrature_octree.cpp:116-135)
+        if len(ch["idx"]) > 0 or ch["children"]:
+            node["M"] += m2m(p, ch["M"], ch["c"] - node["c"], compat=True)
+
+
+def _tc_rot(node, p, x, eps):
+    d2 = float(np.sum((x - node["c"]) ** 2))
+    r2 = float(np.sum(node["h"] ** 2))
+    if 4 * r2 < d2:
+        v = x - node["c"]
+        hd = []
+        for a in range(3):
+            e = np.zeros(3)
+            e[a] = eps
+            hd.append(solid_harmonics(p, v + e, False, True) - solid_harmonics(p, v - e, False, True))
+        M = node["M"]
+        t = np.array([np.dot(M[:, 2], hd[1]) - np.dot(M[:, 1], hd[2]),
+                      np.dot(M[:, 0], hd[2]) - np.dot(M[:, 2], hd[0]),
+                      np.dot(M[:, 1], hd[0]) - np.dot(M[:, 0], hd[1])])
+        return t / (2 * eps)
+    out = np.zeros(3)
+    for ch in node["children"]:
+        out += _tc_rot(ch, p, x, eps)
+    return out
+
+
+def treecode_B(p, cap, xyz, w, pts, current=1.0, half=3.0, eps=1e-3):
+    """B at pts by the reference's treecode, FP64 (root: centre 0, half-width `half`; points outside it
+    are not inserted). Returns [m, 3]."""
+    xyz = _c64(xyz).reshape(-1, 3)
+    w = _c64(w)
+    pts = _c64(pts).reshape(-1, 3)
+    c0 = np.zeros(3)
+    h0 = np.full(3, float(half))
+    inside = np.all((c0 - h0 <= xyz) & (xyz < c0 + h0), axis=1)
+    root = _tc_build(xyz, np.nonzero(inside)[0], c0, h0, cap)
+    _tc_upward(root, p, xyz, w)
+    out = np.stack([_tc_rot(root, p, x, eps) for x in pts])
+    return out / (4.0 * REF_PI) * current * REF_MU0
+
+
 def p2m(p, xyz, w, J=None, center=(0, 0, 0), compat=False):
     xyz = _c64(xyz).reshape(-1, 3)
     w = _c64(w)
@@ -269,6 +347,14 @@ class Reference:
     def _bem_rows(src, w, B, nrm):
         return np.ascontiguousarray(np.concatenate([_c64(src).reshape(-1, 3), _c64(w).reshape(-1, 1),
                                                     _c64(B).reshape(-1, 3), _c64(nrm).reshape(-1, 3)], axis=1))
+
+    def treecode_B(self, xyzw, pts, cap, current=1.0):
+        """The reference's MultipoleSolver treecode B at pts (multipole_solver.cpp:686-700)."""
+        xyzw = _c64(xyzw).reshape(-1, 4)
+        pts = _c64(pts).reshape(-1, 3)
+        out = np.zeros((len(pts), 3))
+        self.lib.ref_treecode_B(len(xyzw), _d(xyzw), len(pts), _d(pts), int(cap), ctypes.c_double(current), _d(out))
+        return out
 
     def bem_direct(self, src, w, B, nrm, tgt):
         """math::calcBEMIntegral at each target."""

@@ -17,6 +17,7 @@
 //   Torus (hexahedra -> 5 tetrahedra) + math::tetrahedraToQuadratures     torus.cpp:9-117, integration.cpp:163-187
 //   FastMultipoleSolver full B / A pipeline                               fast_multipole_solver.cpp:12-231
 //   math::calcBEMIntegral, calcBEMIntegralContribution (BEM problem)     integration.cpp:191-215, 295-353
+//   MultipoleSolver treecode B (single source tree, no locals)           multipole_solver.cpp:20-139, 686-700
 #include <chrono>
 #include <cstdint>
 #include <cstring>
@@ -25,6 +26,7 @@
 #include <vector>
 
 #include "fast_multipole_solver.hpp"
+#include "multipole_solver.hpp"
 #include "harmonics.hpp"
 #include "integration.hpp"
 #include "multipole_translator.hpp"
@@ -199,6 +201,25 @@ void ref_bem_p2m(int order, int n, const double* q, const double* center, double
    for(int i = 0; i < n; i++) ptrs[i] = &bq[i];
    auto res = math::calcBEMIntegralContribution(ptrs, order, Vector3(real(center[0]), real(center[1]), real(center[2])));
    fromSeries(res, out);
+}
+
+// The reference's treecode: MultipoleSolver over n quadratures (x, y, z, weight; J the azimuthal default)
+// with leaf capacity `cap`, leaf P2M, complex-translation M2M, then calcB(current, point) at m points:
+// out[3m]. The source tree's root is the reference's fixed box (centre 0, half-width 3).
+void ref_treecode_B(int n, const double* xyzw, int m, const double* pts, int cap, double current, double* out)
+{
+   std::vector<Quadrature> q(n);
+   for(int i = 0; i < n; i++)
+      q[i] = Quadrature(Vector3(real(xyzw[4 * i]), real(xyzw[4 * i + 1]), real(xyzw[4 * i + 2])),
+                        real(xyzw[4 * i + 3]), real(1));
+   MultipoleSolver solver(q, Problem::BioSavartLaplace, size_t(cap));
+   solver.calcMultipoleExpansionsAtLeaves();
+   solver.calclMultipoleExpansions(M2MAlg::ComplexTranslation, Device::CPU);
+   for(int j = 0; j < m; j++)
+   {
+      Vector3 b = solver.calcB(real(current), Vector3(real(pts[3 * j]), real(pts[3 * j + 1]), real(pts[3 * j + 2])));
+      out[3 * j] = b.x; out[3 * j + 1] = b.y; out[3 * j + 2] = b.z;
+   }
 }
 
 // A(x) = sum_k local_k * R_k(d), d = x - center (no 1/(4 pi) or current factor).

@@ -4,7 +4,7 @@ Runs the patched reference build (oracle/_ref/libref_fmm_*.so, made by oracle/re
 from the reference sources) on seeded inputs and stores inputs and outputs as .npz. The
 reference is not needed afterwards: the tests read only the .npz files.
 
-Usage: python tests/golden/make_golden.py [main] [seam] [telma] [bem]   (default: all)
+Usage: python tests/golden/make_golden.py [main] [seam] [telma] [bem] [treecode]   (default: all)
 The reference sources are read from REFERENCE_ROOT (default /root/reference).
 """
 import os
@@ -154,8 +154,28 @@ def bem():
     print("wrote", path, len(out), "arrays")
 
 
+def treecode():
+    """The reference's treecode B (MultipoleSolver::calcB) on a small torus, near and far points."""
+    rng = np.random.default_rng(20260007)
+    xyz, w, J = geometry.torus(24, 8, 4, 2.0, 0.5)
+    near = rng.uniform(-2.9, 2.9, size=(16, 3))
+    u = rng.normal(size=(8, 3))
+    far = u / np.linalg.norm(u, axis=1)[:, None] * rng.uniform(6.0, 8.0, size=(8, 1))
+    pts = np.concatenate([near, far])
+    xyzw = np.concatenate([xyz, w[:, None]], axis=1)
+    out = {"xyzw": xyzw, "pts": pts}
+    # the solver's order is the build's compile-time FMM_ORDER: one build per order
+    for p, cap in ((10, 16), (12, 32)):
+        out[f"B_p{p}_cap{cap}"] = Reference("f64", p).treecode_B(xyzw, pts, cap, 1.0)
+    path = os.path.join(HERE, "reference_treecode.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, len(out), "arrays")
+
+
 if __name__ == "__main__":
-    what = sys.argv[1:] or ["main", "seam", "telma", "bem"]
+    what = sys.argv[1:] or ["main", "seam", "telma", "bem", "treecode"]
+    if "treecode" in what:
+        treecode()
     if "bem" in what:
         bem()
     if "telma" in what:
