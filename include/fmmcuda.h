@@ -82,6 +82,8 @@ typedef struct fmm_plan fmm_plan;
 typedef struct fmm_stats {
    double ms_tree, ms_upward, ms_m2l, ms_downward, ms_near, ms_total;
    int64_t nodes, leaves, levels, v_pairs, p2p_pairs, p2p_interactions;
+   /* boxes, leaf boxes, levels, M2L (V-list) box pairs, direct (leaf, source box) pairs, and the direct
+      (target, source) point pairs the near field evaluates */
    int64_t n_sources, n_targets;
    double ms_adjoint; /* the last fmm_adjoint call */
    int64_t coils;     /* independent problems in the plan (1 unless batched) */
