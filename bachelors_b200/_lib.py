@@ -22,7 +22,7 @@ EXPORTS = [
     "fmm_build_tree", "fmm_upward", "fmm_downward", "fmm_evaluate", "fmm_solve", "fmm_direct",
     "fmm_direct_fp64_subset", "fmm_adjoint", "fmm_adjoint_direct", "fmm_autotune", "fmm_get_tuning",
     "fmm_set_tuning", "fmm_batch_set_coils", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
-    "fmm_get_stats", "fmm_get_operator", "fmm_direct_B_noalloc", "fmm_translate_all", "fmm_translate_all_matrix",
+    "fmm_set_wait_limit", "fmm_get_stats", "fmm_get_operator", "fmm_direct_B_noalloc", "fmm_translate_all", "fmm_translate_all_matrix",
     "fmm_translate_all_matrix_complex", "fmm_add_vectors",
     "fmm_last_error_string", "fmm_version",
 ]
@@ -100,6 +100,7 @@ def load():
         "fmm_update_sources": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
         "fmm_graph_capture": (ctypes.c_int, [vp, ctypes.c_int, vp]),
         "fmm_graph_launch": (ctypes.c_int, [vp, dbl, vp, vp, ctypes.c_int, vp]),
+        "fmm_set_wait_limit": (ctypes.c_int, [vp, dbl]),
         "fmm_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(FmmStats)]),
         "fmm_get_operator": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
         "fmm_direct_B_noalloc": (ctypes.c_int, [vp, vp, vp, i64, vp, i64, dbl, vp, vp]),

@@ -27,19 +27,37 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [NVCC, *FLAGS, "-shared", "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
+OBJ = os.path.join(HERE, "_build")
+
+
+def _compile(src: str, verbose: bool) -> tuple[str, subprocess.CompletedProcess]:
+    obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+    cmd = [NVCC, *FLAGS, "-dc", "-o", obj, os.path.join(CSRC, src)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
+    return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every translation unit in parallel (relocatable device code), then links them, with
+    the device link step, into libfmmcuda.so."""
+    if not force and up_to_date():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(OBJ, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
+    for obj, r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed compiling {os.path.basename(obj)}")
+        if verbose:
+            sys.stderr.write(r.stderr)
+    cmd = [NVCC, *FLAGS, "-shared", "-o", LIB + ".tmp", *[o for o, _ in results]]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libfmmcuda.so")
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libfmmcuda.so")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

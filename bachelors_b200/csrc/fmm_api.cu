@@ -108,10 +108,14 @@ fmm_status Plan::init(const fmm_config& c)
    if(const char* e = getenv("FMM_TC_TRNP_DN")) tcTrPiecesDn = std::min(3, std::max(0, atoi(e)));
 
    FMM_TRY(rootb.reserve(sizeof(RootBox)));
-   FMM_TRY(errb.reserve(sizeof(int)));
+   FMM_TRY(errb.reserve(2 * sizeof(int)));
    FMM_TRY(initOffsetTables());
    root = (RootBox*)rootb.ptr;
    err = (int*)errb.ptr;
+   pipeErr = err + 1;
+   FMM_CUDA(cudaMemset(errb.ptr, 0, 2 * sizeof(int)));
+   FMM_CUDA(cudaMallocHost((void**)&hostErr, sizeof(int)));
+   *hostErr = 0;
    for(int i = 0; i < 8; i++) cudaEventCreate(&ev[i]);
    eventsMade = true;
    return FMM_OK;
@@ -133,6 +137,9 @@ void Plan::release()
    for(DevBuf* b : bufs) b->release();
    for(auto& b : nodeBufs) b.release();
    for(auto& b : listBufs) b.release();
+   if(hostErr) cudaFreeHost(hostErr);
+   hostErr = nullptr;
+   err = pipeErr = nullptr;
    if(eventsMade)
       for(int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
    eventsMade = false;
@@ -195,6 +202,42 @@ fmm_status copyOut(void* dst, const DevBuf& buf, size_t bytes, int onDevice, cud
    if(!dst || !bytes) return FMM_OK;
    FMM_CUDA(cudaMemcpyAsync(dst, buf.ptr, bytes, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
    if(!onDevice) FMM_CUDA(cudaStreamSynchronize(st));
+   return FMM_OK;
+}
+
+// The tensor-core pipelines' error word: cleared on the stream when a solve (or a phase called on
+// its own) starts, read once when it ends, so the phases between queue their kernels without a
+// host wait.
+fmm_status pipeBegin(Plan& P, cudaStream_t st)
+{
+   FMM_CUDA(cudaMemsetAsync(P.pipeErr, 0, sizeof(int), st));
+   return FMM_OK;
+}
+
+fmm_status pipeCheck(Plan& P, cudaStream_t st, const char* what)
+{
+   FMM_CUDA(cudaMemcpyAsync(P.hostErr, P.pipeErr, sizeof(int), cudaMemcpyDeviceToHost, st));
+   FMM_CUDA(cudaStreamSynchronize(st));
+   if(*P.hostErr & ERR_TIMEOUT)
+      return setError(FMM_E_TIMEOUT, "%s: a tensor-core pipeline wait timed out (limit %.3g s)", what,
+                      double(P.tcWaitNs) * 1e-9);
+   return FMM_OK;
+}
+
+fmm_status upwardPhase(Plan& P, cudaStream_t st)
+{
+   FMM_TRY(P.fp64 ? upwardT<double>(P, st) : upwardT<float>(P, st));
+   cudaEventRecord(P.ev[2], st);
+   P.upReady = true;
+   P.downReady = false;
+   return FMM_OK;
+}
+
+fmm_status downwardPhase(Plan& P, cudaStream_t st)
+{
+   FMM_TRY(P.fp64 ? downwardT<double>(P, st) : downwardT<float>(P, st));
+   cudaEventRecord(P.ev[4], st);
+   P.downReady = true;
    return FMM_OK;
 }
 
@@ -341,11 +384,9 @@ fmm_status fmm_upward(fmm_plan* plan, void* stream)
    if(!P.treeReady) return setError(FMM_E_INVALID, "fmm_upward: tree not built");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
-   FMM_TRY(P.fp64 ? upwardT<double>(P, st) : upwardT<float>(P, st));
-   cudaEventRecord(P.ev[2], st);
-   P.upReady = true;
-   P.downReady = false;
-   return FMM_OK;
+   FMM_TRY(pipeBegin(P, st));
+   FMM_TRY(upwardPhase(P, st));
+   return pipeCheck(P, st, "fmm_upward");
 }
 
 fmm_status fmm_downward(fmm_plan* plan, void* stream)
@@ -355,10 +396,9 @@ fmm_status fmm_downward(fmm_plan* plan, void* stream)
    if(!P.upReady) return setError(FMM_E_INVALID, "fmm_downward: multipoles are not ready");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
-   FMM_TRY(P.fp64 ? downwardT<double>(P, st) : downwardT<float>(P, st));
-   cudaEventRecord(P.ev[4], st);
-   P.downReady = true;
-   return FMM_OK;
+   FMM_TRY(pipeBegin(P, st));
+   FMM_TRY(downwardPhase(P, st));
+   return pipeCheck(P, st, "fmm_downward");
 }
 
 fmm_status fmm_evaluate(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device,
@@ -400,10 +440,16 @@ fmm_status fmm_evaluate(fmm_plan* plan, double current, int want, void* out_B, v
 fmm_status fmm_solve(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device, void* stream)
 {
    FMM_TRY(fmm_build_tree(plan, stream));
-   FMM_TRY(fmm_upward(plan, stream));
-   FMM_TRY(fmm_downward(plan, stream));
+   Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   // upward, M2L and downward are queued without a host wait; the pipeline error word is read
+   // once, after the evaluation
+   FMM_TRY(pipeBegin(P, st));
+   FMM_TRY(upwardPhase(P, st));
+   FMM_TRY(downwardPhase(P, st));
    FMM_TRY(fmm_evaluate(plan, current, want, out_B, out_A, on_device, stream));
-   return FMM_OK;
+   return pipeCheck(P, st, "fmm_solve");
 }
 
 fmm_status fmm_direct(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device, void* stream)
@@ -471,6 +517,7 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
       if(s != FMM_OK) { P.adj->release(); delete P.adj; P.adj = nullptr; return s; }
    }
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   P.adj->tcWaitNs = P.tcWaitNs;
    // the coils keep their pairing with the roles swapped
    P.adj->nCoils = P.nCoils;
    P.adj->batch = P.batch;
@@ -489,9 +536,11 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
       dx = dL_dx ? (char*)P.adjOut.ptr + es * 3 * P.n : nullptr;
    }
    cudaEventRecord(P.ev[6], st);
+   FMM_TRY(pipeBegin(*P.adj, st));
    FMM_TRY(P.fp64 ? adjointT<double>(P, *P.adj, current, gDev, dJ, dx, st)
                   : adjointT<float>(P, *P.adj, current, gDev, dJ, dx, st));
    cudaEventRecord(P.ev[7], st);
+   FMM_TRY(pipeCheck(*P.adj, st, "fmm_adjoint"));
    P.adjointDone = true;
    if(!on_device)
    {
@@ -572,6 +621,7 @@ fmm_status fmm_autotune(fmm_plan* plan, fmm_tuning* out, void* stream)
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
    P.dropGraph();
+   FMM_TRY(pipeBegin(P, st));
    cudaEvent_t e0, e1;
    FMM_CUDA(cudaEventCreate(&e0));
    cudaError_t ce = cudaEventCreate(&e1);
@@ -647,6 +697,7 @@ fmm_status fmm_autotune(fmm_plan* plan, fmm_tuning* out, void* stream)
    cudaEventDestroy(e0);
    cudaEventDestroy(e1);
    FMM_TRY(s);
+   FMM_TRY(pipeCheck(P, st, "fmm_autotune"));
    {
       std::lock_guard<std::mutex> lock(g_tuneMutex);
       g_tuned[tuneKey(P.cfg)] = best;
@@ -771,7 +822,7 @@ fmm_status fmm_graph_launch(fmm_plan* plan, double current, void* out_B, void* o
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
-   FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   FMM_TRY(pipeBegin(P, st));
    FMM_CUDA(cudaGraphLaunch(P.graphExec, st));
    const int64_t cnt = 3 * P.m;
    if(on_device)
@@ -789,10 +840,17 @@ fmm_status fmm_graph_launch(fmm_plan* plan, double current, void* out_B, void* o
                                       : scaleCopyT<float>(P, P.outA.ptr, P.outA.ptr, cnt, current, st));
    if(P.graphWant & 1) FMM_CUDA(cudaMemcpyAsync(out_B, P.outB.ptr, es * cnt, cudaMemcpyDeviceToHost, st));
    if(P.graphWant & 2) FMM_CUDA(cudaMemcpyAsync(out_A, P.outA.ptr, es * cnt, cudaMemcpyDeviceToHost, st));
-   int herr = 0;
-   FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-   FMM_CUDA(cudaStreamSynchronize(st));
-   if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "graph solve: a tensor-core pipeline wait timed out");
+   return pipeCheck(P, st, "fmm_graph_launch");
+}
+
+fmm_status fmm_set_wait_limit(fmm_plan* plan, double seconds)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   if(!(seconds > 0) || seconds > 60)
+      return setError(FMM_E_INVALID, "fmm_set_wait_limit: %g s outside (0, 60]", seconds);
+   Plan& P = plan->P;
+   P.tcWaitNs = std::max<uint64_t>(1, uint64_t(seconds * 1e9));
+   P.dropGraph();   // a captured graph holds the old limit
    return FMM_OK;
 }
 

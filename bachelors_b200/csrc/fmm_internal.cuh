@@ -182,7 +182,11 @@ struct Plan
    {
       return !fp64 && cfg.m2l_mode != FMM_M2L_SIMT && (tcTranslate & which) != 0;
    }
-   int* err = nullptr;
+   int* err = nullptr;                   // tree build: list-capacity flags
+   int* pipeErr = nullptr;               // tensor-core pipelines: ERR_TIMEOUT; cleared when a solve (or a
+                                         // phase called on its own) starts and read once when it ends
+   int* hostErr = nullptr;               // pinned host word the pipeline error is read into
+   uint64_t tcWaitNs = 2000000000ull;    // limit of one tensor-core pipeline wait (fmm_set_wait_limit)
    DevBuf errb;
    // expansions [node][3][Lp] and outputs
    DevBuf mult, local, outB, outA;

@@ -1670,7 +1670,7 @@ __global__ void __launch_bounds__(NT) kDirect(const typename Vec4<T>::type* __re
    if(tBeg + int(blockIdx.x) * NT >= tEnd) return;
    const bool active = ti < tEnd;
    U x = 0, y = 0, z = 0;
-   if(active) { x = tgt[3 * ti]; y = tgt[3 * ti + 1]; z = tgt[3 * ti + 2]; }
+   if(active) { x = tgt[3 * int64_t(ti)]; y = tgt[3 * int64_t(ti) + 1]; z = tgt[3 * int64_t(ti) + 2]; }
    U B[3] = {0, 0, 0}, A[3] = {0, 0, 0};
    for(int sb = sBeg; sb < sEnd; sb += NT)
    {

@@ -28,8 +28,13 @@
 //               registers, the rest in the local expansions in global memory. Each TMEM lane
 //               quadrant has two drain warps, one per half of the columns
 // Stages hold one K chunk of every piece of A and of T_o; two stages rotate through mbarriers
-// (full: producers + bulk-copy bytes, empty: tcgen05.commit). Every wait is bounded by
-// a 2 s global-timer limit; on expiry the CTA records FMM timeout in the error word and stops.
+// (full: the producers' arrivals, op: the operator bulk copy's bytes, empty: tcgen05.commit).
+// Every pipeline wait is bounded by a global-timer limit (2 s unless the plan sets another); on
+// expiry the CTA records a timeout in the error word and every role leaves its loop. Before the
+// CTA exits it still waits, whatever the abort flag says and again with a 2 s bound, for the
+// asynchronous work it started: the producers for their cp.async copies, warp 1 for its bulk
+// copies (the last phase of each stage's op barrier), warp 0 for its MMAs (tcgen05.commit to
+// the done barrier); only then is the tensor memory freed.
 #include <cstdlib>
 
 #include <cuda_bf16.h>
@@ -84,8 +89,10 @@ __device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t parity)
    return ok != 0;
 }
 
-// Bounded wait; returns false (and raises the error word) when the limit expires.
-__device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity, int* err, volatile int* abortFlag)
+// Bounded pipeline wait; returns false when another role of the CTA has given up, or (raising
+// the error word and the CTA's abort flag) when limitNs expires.
+__device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity, int* err, volatile int* abortFlag,
+                                         uint64_t limitNs)
 {
    if(mbarTryWait(bar, parity)) return true;
    const uint64_t t0 = globalTimer();
@@ -93,10 +100,28 @@ __device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity, int* err
    {
       if(mbarTryWait(bar, parity)) return true;
       if(*abortFlag) return false;
-      if(globalTimer() - t0 > TIMEOUT_NS)
+      if(globalTimer() - t0 > limitNs)
       {
          atomicOr(err, ERR_TIMEOUT);
          *abortFlag = 1;
+         return false;
+      }
+   }
+}
+
+// Wait for asynchronous work this CTA issued itself (bulk copies, MMAs) before it releases the
+// shared and tensor memory that work writes: the abort flag is ignored, since such work always
+// completes; the 2 s bound only keeps a broken device from holding the CTA forever.
+__device__ __forceinline__ bool mbarWaitIssued(uint32_t bar, uint32_t parity, int* err)
+{
+   if(mbarTryWait(bar, parity)) return true;
+   const uint64_t t0 = globalTimer();
+   while(true)
+   {
+      if(mbarTryWait(bar, parity)) return true;
+      if(globalTimer() - t0 > TIMEOUT_NS)
+      {
+         atomicOr(err, ERR_TIMEOUT);
          return false;
       }
    }
@@ -352,7 +377,7 @@ __global__ void __maxnreg__(96)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int nOps, int L, int Lp,
        int nChunks, const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc,
        int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainFar, int drainItems, int nStages, int drainMode,
-       const M2LCols cols, unsigned long long* counters, int* err)
+       const M2LCols cols, unsigned long long* counters, int* err, uint64_t waitNs)
 {
    using namespace tc;
    constexpr int KCH = Lay::KC;
@@ -373,11 +398,12 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    uint8_t* sbase = smraw + (base - rawAddr);
    const int NS = nStages;
    uint8_t* ctrl = sbase + NS * stageBytes;
-   uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);          // full[NS], empty[NS], done, drainFull, drainEmpty
-   uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 128);
-   volatile int* abortFlag = reinterpret_cast<volatile int*>(ctrl + 132);
-   uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 136); // 10 words: offsets present in the tile
-   int* itemOffset = reinterpret_cast<int*>(ctrl + 192);        // compacted present offsets [316] + count
+   // full[NS], empty[NS], done, drainFull, drainEmpty, op[NS]: at most 3 MAXSTAGE + 3 = 21 barriers
+   uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);
+   uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 192);
+   volatile int* abortFlag = reinterpret_cast<volatile int*>(ctrl + 196);
+   uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 200); // 10 words: offsets present in the tile
+   int* itemOffset = reinterpret_cast<int*>(ctrl + 256);        // compacted present offsets [316] + count
    int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
    int* colTab = tileNode + 64;                                 // output columns per K step [MAXKSTEPS]
 
@@ -387,6 +413,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    const int nTile = min(TT, nTargets - first);
    const uint32_t fullBar0 = smemAddr(&bars[0]), emptyBar0 = smemAddr(&bars[NS]), doneBar = smemAddr(&bars[2 * NS]);
    const uint32_t drainFull = smemAddr(&bars[2 * NS + 1]), drainEmpty = smemAddr(&bars[2 * NS + 2]);
+   const uint32_t opBar0 = smemAddr(&bars[2 * NS + 3]);
 
    if(tid < 10) present[tid] = 0;
    if(tid < TT) tileNode[tid] = tid < nTile ? targets[first + tid] : -1;
@@ -400,8 +427,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       *abortFlag = 0;
       for(int s = 0; s < NS; s++)
       {
-         mbarInit(fullBar0 + 8 * s, NPROD + 1);
+         mbarInit(fullBar0 + 8 * s, NPROD);
          mbarInit(emptyBar0 + 8 * s, 1);
+         mbarInit(opBar0 + 8 * s, 1);
       }
       mbarInit(doneBar, 1);
       mbarInit(drainFull, 1);
@@ -460,7 +488,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             int nColK[KCH / KS];
 #pragma unroll
             for(int ks = 0; ks < KCH / KS; ks++) nColK[ks] = colTab[(it % nChunks) * (KCH / KS) + ks];
-            if(!mbarWait(fullBar0 + 8 * s, (it / NS) & 1, err, abortFlag)) break;
+            if(!mbarWait(fullBar0 + 8 * s, (it / NS) & 1, err, abortFlag, waitNs)) break;
+            if(!mbarWait(opBar0 + 8 * s, (it / NS) & 1, err, abortFlag, waitNs)) break;
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
             const uint32_t aSt = st, bSt = st + NP * aBytes;
@@ -518,7 +547,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                   mmaCommit(drainFull);
                   if(it != nItems - 1)
                   {
-                     if(!mbarWait(drainEmpty, drains & 1, err, abortFlag)) break;
+                     if(!mbarWait(drainEmpty, drains & 1, err, abortFlag, waitNs)) break;
                      fenceAfterSync();
                   }
                   drains++;
@@ -534,18 +563,28 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    {
       if(lane == 0)
       {
+         int issued = 0;
          for(int it = 0; it < nItems; it++)
          {
             const int s = it % NS;
-            if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag)) break;
+            if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag, waitNs)) break;
             const int o = itemOffset[it / nChunks], c = it % nChunks;
             const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
             const uint32_t dst = base + s * stageBytes + NP * aBytes;
             // only the operator rows (output columns) this chunk's widest K step uses
             const uint32_t rowBytes = uint32_t(colTab[c * (KCH / KS)]) * Lay::RB;
-            mbarArriveExpectTx(fullBar0 + 8 * s, NP * rowBytes);
+            mbarArriveExpectTx(opBar0 + 8 * s, NP * rowBytes);
 #pragma unroll
-            for(int j = 0; j < NP; j++) bulkLoad(dst + j * bBytes, src + j * bBytes, rowBytes, fullBar0 + 8 * s);
+            for(int j = 0; j < NP; j++) bulkLoad(dst + j * bBytes, src + j * bBytes, rowBytes, opBar0 + 8 * s);
+            issued = it + 1;
+         }
+         // the copies in flight write this CTA's shared memory: wait for them before it can exit. A stage
+         // is reused only after the MMAs consumed its previous item, which waited for that item's copy, so
+         // only the last item issued on each stage can still be in flight.
+         for(int s = 0; s < NS && s < issued; s++)
+         {
+            const int last = s + ((issued - 1 - s) / NS) * NS;
+            mbarWaitIssued(opBar0 + 8 * s, (last / NS) & 1, err);
          }
       }
       __syncwarp();
@@ -591,7 +630,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       for(int i = 0; i < RHALF; i++) rsum[i] = 0.f;
       for(int d = 0; d < nDrains; d++)
       {
-         if(!mbarWait(drainFull, d & 1, err, abortFlag)) break;
+         if(!mbarWait(drainFull, d & 1, err, abortFlag, waitNs)) break;
          fenceAfterSync();
          const bool last = d == nDrains - 1;
          // tensor-memory part: S += acc (d > 0) or S = acc; the last drain writes S + acc to the locals
@@ -720,7 +759,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             mbarArrive(fullBar0 + 8 * (pending % NS));
             pending = -1;
          }
-         if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag)) break;
+         if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag, waitNs)) break;
          const uint32_t aSt = base + s * stageBytes;
          const int k0 = c * KCH + half * PER;
          const uint8_t* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp * Lay::ES;
@@ -749,8 +788,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    __syncthreads();
    if(warp == 0)
    {
-      // the accumulator must be idle before it is released, also after an aborted pipeline
-      if(lane == 0 && nItems > 0) mbarWait(doneBar, 0, err, abortFlag);
+      // the accumulator must be idle before it is released, also after an aborted pipeline: the
+      // commit to doneBar arrives once every MMA issued before it has completed
+      if(lane == 0 && nItems > 0) mbarWaitIssued(doneBar, 0, err);
       __syncwarp();
       fenceAfterSync();
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
@@ -776,13 +816,12 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    if(count <= 0) return FMM_OK;
    const int blocks = (count + tc::TT - 1) / tc::TT;
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 192 + 4 * (320 + 64 + MAXKSTEPS);
+   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + MAXKSTEPS);
    const size_t budget = 232448;
    const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
    const size_t smem = fixed + nStages * stageBytes;
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-   FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
    FMM_TRY(P.tcCounters.reserve(2 * sizeof(unsigned long long)));
    FMM_CUDA(cudaMemsetAsync(P.tcCounters.ptr, 0, 2 * sizeof(unsigned long long), st));
    P.tcTiles = blocks;
@@ -814,13 +853,9 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
                                                       nChunks, (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
                                                       (float*)P.local.ptr, 0, nullptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
-                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.err);
+                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.pipeErr, P.tcWaitNs);
    FMM_TRY(launched(P, "kM2LTc", st));
-   if(P.capturing) return FMM_OK;  // inside a graph capture the error word is checked after the launch
-   int herr = 0;
-   FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-   FMM_CUDA(cudaStreamSynchronize(st));
-   if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "tensor-core M2L: a pipeline wait timed out");
+   // a timed-out wait raises the pipeline error word, which the calling phase reads once at its end
    return FMM_OK;
 }
 
@@ -852,7 +887,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
       P.opTrImgTag = tag;
    }
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 192 + 4 * (320 + 64 + MAXKSTEPS);
+   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + MAXKSTEPS);
    const size_t budget = 232448;
    const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core translation: %zu-byte stages do not fit twice", stageBytes);
@@ -865,7 +900,6 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
    for(int g = 0; g < nSteps; g++) cols.n[g] = Lay::KSTEP * g < L ? Lp : 0;
    const int64_t rows = P.tree.nNodes * 3;
    FMM_TRY(P.multBf.reserve(size_t(Lay::ES) * rows * NP * Lp));
-   FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
    const int drainEvery = NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2);
    const size_t pieceRow = size_t(Lay::ES) * NP * Lp;   // bytes of one split row
    const Tree& t = P.tree;
@@ -891,7 +925,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          kern<<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.parList.ptr + a, b - a, (const int*)P.vtabUp.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0,
-            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.err);
+            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs);
          FMM_TRY(launched(P, "kM2LTc<M2M>", st));
       }
       P.multBfTag = NP * 2 + (Lay::TF32 ? 1 : 0);
@@ -907,17 +941,12 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
             (const int*)P.l2lTargets.ptr + a, b - a, (const int*)P.vtabDn.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, nullptr, drainEvery, drainEvery,
             P.tcTrDrainItems, nStages,
-            P.tcDrainMode, cols, nullptr, P.err);
+            P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs);
          FMM_TRY(launched(P, "kM2LTc<L2L>", st));
       }
       P.multBfTag = -1;
    }
    FMM_CHECK_LAUNCH();
-   if(P.capturing) return FMM_OK;
-   int herr = 0;
-   FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-   FMM_CUDA(cudaStreamSynchronize(st));
-   if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "tensor-core translation: a pipeline wait timed out");
    return FMM_OK;
 }
 

@@ -9,10 +9,14 @@
 // that the library image carries; it never calls cudaMalloc, cudaFree or an allocating library
 // routine.
 //
-// The array (g_noallocSources, NOALLOC_MAX_SOURCES sources, 8 MiB) exists on every GPU that
-// loads the library and stays allocated until the process exits. Its device address is looked
-// up once per device, on the first call made with that device current (cudaGetSymbolAddress);
-// make that first call before any stream capture. All calls share the array and it keeps the
+// The array (g_noallocSources, NOALLOC_MAX_SOURCES sources, 8 MiB) belongs to this file's device
+// module. Under CUDA's lazy module loading (the default) the module, and with it the array, is
+// loaded onto a device by the first call made with that device current, when the array's address
+// is looked up (cudaGetSymbolAddress); from then on it stays on that device until the process
+// exits. That first call can therefore allocate the array's device memory and synchronise, and it
+// fails (FMM_E_CUDA, with the runtime's reason) when another allocator has already reserved all of
+// the device's memory: make it once per device before the caller's allocator reserves the GPU,
+// outside latency-critical loops and before any stream capture. Later calls allocate nothing. All calls share the array and it keeps the
 // previous call's contents: each call overwrites the entries it reads before reading them, so
 // nothing needs clearing, but calls whose work overlaps on the GPU (other streams, or other
 // host threads) race on it and must be serialised by the caller.
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(NT) kDirectNoalloc(const float4* __restrict__ 
    const int ti = blockIdx.x * NT + threadIdx.x;
    const bool active = ti < m;
    float x = 0.f, y = 0.f, z = 0.f;
-   if(active) { x = tgt[3 * ti]; y = tgt[3 * ti + 1]; z = tgt[3 * ti + 2]; }
+   if(active) { x = tgt[3 * int64_t(ti)]; y = tgt[3 * int64_t(ti) + 1]; z = tgt[3 * int64_t(ti) + 2]; }
    float B[3] = {0.f, 0.f, 0.f};
    for(int sb = 0; sb < n; sb += NT)
    {
@@ -104,7 +108,10 @@ fmm_status noallocScratch(float4** out)
       if(e != cudaSuccess || !p)
       {
          cudaGetLastError();
-         return setError(FMM_E_CUDA, "fmm_direct_B_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+         return setError(FMM_E_CUDA,
+                         "fmm_direct_B_noalloc: loading the library's scratch array onto device %d failed (%s); "
+                         "make the first call on each device before another allocator reserves its memory",
+                         dev, cudaGetErrorString(e));
       }
       g_noallocPtr[dev] = static_cast<float4*>(p);
    }

@@ -94,7 +94,7 @@ def random_axis(rng):
 
 def torus_batch(n_coils=256, seed=20260004, count_range=(2 ** 12, 2 ** 18), targets_per_coil=2 ** 14,
                 major_range=(1.0, 3.0), minor_range=(0.2, 0.6), center_range=(-10.0, 10.0),
-                magnitude_range=(0.5, 2.0), n_theta=16, n_rho=4):
+                magnitude_range=(0.5, 2.0), n_theta=16, n_rho=4, params=False):
     """Many independent coils for the batched solver: coil i is a torus with major radius
     R ~ U(major_range), minor radius a ~ U(minor_range), an axis uniform on the sphere, a centre
     uniform in center_range^3, a point count log-uniform in count_range (n_phi x n_theta x n_rho
@@ -102,9 +102,9 @@ def torus_batch(n_coils=256, seed=20260004, count_range=(2 ** 12, 2 ** 18), targ
     `targets_per_coil` targets uniform in the cube of side 3R around its centre.
 
     Returns (xyz[N,3], w[N], J[N,3], tgt[M,3], src_offsets[K+1], tgt_offsets[K+1]) with each coil's
-    points contiguous."""
+    points contiguous; with params=True also [K, 3] rows (major radius, minor radius, current magnitude)."""
     rng = np.random.default_rng(seed)
-    xs, ws, Js, ts = [], [], [], []
+    xs, ws, Js, ts, prm = [], [], [], [], []
     so, to = [0], [0]
     lo, hi = np.log(count_range[0]), np.log(count_range[1])
     for _ in range(n_coils):
@@ -119,8 +119,10 @@ def torus_batch(n_coils=256, seed=20260004, count_range=(2 ** 12, 2 ** 18), targ
         t = c + rng.uniform(-1.5 * R, 1.5 * R, size=(targets_per_coil, 3))
         xs.append(x); ws.append(w); Js.append(J); ts.append(t)
         so.append(so[-1] + len(w)); to.append(to[-1] + len(t))
-    return (np.concatenate(xs), np.concatenate(ws), np.concatenate(Js), np.concatenate(ts),
-            np.array(so, dtype=np.int64), np.array(to, dtype=np.int64))
+        prm.append((R, a, mag))
+    out = (np.concatenate(xs), np.concatenate(ws), np.concatenate(Js), np.concatenate(ts),
+           np.array(so, dtype=np.int64), np.array(to, dtype=np.int64))
+    return out + (np.array(prm),) if params else out
 
 
 def hex_torus_tetrahedra(radius=2.0, section_width=0.2, n_length=20, n_width=4, n_height=4):

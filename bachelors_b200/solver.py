@@ -115,6 +115,9 @@ class Plan:
         self._keep = []
         self.device_mode = False
         self.m = 0
+        # bumped whenever the plan's inputs change (sources, targets, strengths, coils), so a caller
+        # holding results of an earlier input set can tell that the plan no longer describes them
+        self.generation = 0
 
     def close(self):
         if getattr(self, "handle", None):
@@ -142,6 +145,7 @@ class Plan:
                                             ctypes.c_void_p(jb.ptr) if jb else None, x.n, int(x.device),
                                             self._stream()))
         self._keep = [x, wb, jb]
+        self.generation += 1
 
     def set_targets(self, xyz):
         t = _Buffer(xyz, self.np_dtype, self.torch_dtype, (3,))
@@ -149,11 +153,13 @@ class Plan:
         _lib.check(self.lib.fmm_set_targets(self.handle, ctypes.c_void_p(t.ptr), t.n, int(t.device), self._stream()))
         self.m = t.n
         self._keep.append(t)
+        self.generation += 1
 
     def set_targets_to_sources(self):
         """Targets = the source points just set (fmm_set_targets_to_sources): a device-side copy."""
         _lib.check(self.lib.fmm_set_targets_to_sources(self.handle, self._stream()))
         self.m = self.n
+        self.generation += 1
 
     def _out(self, rows=None):
         rows = self.m if rows is None else rows
@@ -175,6 +181,7 @@ class Plan:
         """Independent problems in one plan (fmm_batch_set_coils): coil c owns sources
         src_offsets[c]:src_offsets[c+1] and targets tgt_offsets[c]:tgt_offsets[c+1]. Call after
         set_sources / set_targets; set_coils(None, None) returns to a single problem."""
+        self.generation += 1
         if src_offsets is None:
             _lib.check(self.lib.fmm_batch_set_coils(self.handle, 0, None, None))
             return
@@ -241,6 +248,7 @@ class Plan:
                                                ctypes.c_void_p(jb.ptr) if jb else None, int(wb.device),
                                                self._stream()))
         self._keep += [wb, jb]
+        self.generation += 1
 
     def graph_capture(self, want=1):
         """Capture P2M .. L2P + near field on the current tree as a CUDA graph."""
@@ -276,6 +284,10 @@ class Plan:
     def set_tuning(self, m2l_k_chunk=64, near_tile=256, p2m_chunk=0):
         t = _lib.FmmTuning(int(m2l_k_chunk), int(near_tile), int(p2m_chunk), 0.0, 0.0, 0.0)
         _lib.check(self.lib.fmm_set_tuning(self.handle, ctypes.byref(t)))
+
+    def set_wait_limit(self, seconds):
+        """Limit of one tensor-core pipeline wait (fmm_set_wait_limit); FmmError FMM_E_TIMEOUT when one runs out."""
+        _lib.check(self.lib.fmm_set_wait_limit(self.handle, ctypes.c_double(seconds)))
 
     def stats(self):
         s = _lib.FmmStats()

@@ -200,6 +200,15 @@ fmm_status fmm_update_sources(fmm_plan* plan, const void* w, const void* J, int 
 fmm_status fmm_graph_capture(fmm_plan* plan, int want, void* stream);
 fmm_status fmm_graph_launch(fmm_plan* plan, double current, void* out_B, void* out_A, int on_device, void* stream);
 
+/* Limit of one bounded wait in the tensor-core pipelines (no counterpart in the reference, whose
+ * kernels have no device-side waits). Every producer/consumer wait of the tcgen05 M2L, M2M and L2L
+ * gives up after this many seconds (default 2; range (0, 60]); the call that ran the pipeline then
+ * returns FMM_E_TIMEOUT, the plan stays usable, and the next call recomputes what it needs. The
+ * device error word is read once at the end of fmm_solve (and of fmm_upward, fmm_downward,
+ * fmm_adjoint, fmm_autotune, and fmm_graph_launch with host outputs), not after every launch.
+ * A graph captured earlier is dropped (it holds the old limit). */
+fmm_status fmm_set_wait_limit(fmm_plan* plan, double seconds);
+
 fmm_status fmm_get_stats(const fmm_plan* plan, fmm_stats* stats);
 
 /* Operator tables, for verification. kind 0 = M2M (index = child octant 0..7), 1 = L2L
@@ -216,8 +225,12 @@ fmm_status fmm_get_operator(fmm_plan* plan, int kind, int index, double* out);
  * `stream` and the call does not wait for it. The only scratch, the packed sources, lives in a
  * fixed 8 MiB device array inside the library, present on every GPU that loads it until the
  * process exits: n is limited to 262,144 sources (FMM_E_LIMIT beyond). The first call on a device
- * looks up that array's address (make it before any stream capture). All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. Never allocates. */
+ * loads the array onto it (CUDA loads a library's device module lazily) and looks up its address:
+ * that call may allocate the array's 8 MiB and synchronise, and fails with FMM_E_CUDA when another
+ * allocator has already reserved all of the device's memory, so make it once per device before such
+ * an allocator starts, outside latency-critical loops and before any stream capture. Later calls
+ * allocate nothing. All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 fmm_status fmm_direct_B_noalloc(const float* xyz, const float* w, const float* J, int64_t n, const float* tgt,
                                 int64_t m, double current, float* out_B, void* stream);
 

@@ -138,3 +138,53 @@ def test_autograd_gradcheck_fp64():
     f = lambda x, j: biot_savart(x, Wt, j, T, plan=plan) * 1e7   # scale B (~1e-7 T) to O(1)
     assert torch.autograd.gradcheck(f, (X, Jt), eps=1e-6, atol=1e-5, rtol=1e-3)
     plan.close()
+
+
+def test_autograd_backward_after_plan_reuse():
+    """Two forwards on one plan, then backward of the first: the gradients are those of the first
+    problem (the wrapper restores its inputs when the plan has been given others since)."""
+    import torch
+    from bachelors_b200 import Plan
+    from bachelors_b200.autograd import biot_savart
+    xyz, w, J = G.torus(16, 8, 4, 2.0, 0.5)
+    rng = np.random.default_rng(5)
+    t1 = rng.uniform(-3, 3, size=(200, 3))
+    t2 = rng.uniform(-3, 3, size=(150, 3))
+    d = lambda a, g=False: torch.tensor(a, dtype=torch.float64, device="cuda", requires_grad=g)
+    plan = Plan(order=10, leaf_capacity=16, precision="fp64")
+    X1, J1 = d(xyz, True), d(J, True)
+    B1 = biot_savart(X1, d(w), J1, d(t1), plan=plan)
+    X2, J2 = d(xyz * 1.1, True), d(J * 0.5, True)
+    B2 = biot_savart(X2, d(w), J2, d(t2), plan=plan)
+    g1 = d(rng.normal(size=t1.shape))
+    (B1 * g1).sum().backward()
+    ref = Plan(order=10, leaf_capacity=16, precision="fp64")
+    ref.set_sources(xyz, w, J)
+    ref.set_targets(t1)
+    rJ, rX = ref.adjoint_direct(g1.cpu().numpy())
+    ref.close()
+    # the adjoint FMM's accuracy at p = 10; the second problem's gradients differ by O(1)
+    assert np.linalg.norm(J1.grad.cpu().numpy() - rJ) / np.linalg.norm(rJ) < 5e-5
+    assert np.linalg.norm(X1.grad.cpu().numpy() - rX) / np.linalg.norm(rX) < 5e-5
+    assert B2.shape == (150, 3)
+    plan.close()
+
+
+def test_autograd_gradcheck_azimuthal_current_fp64():
+    """J = None (the reference's azimuthal direction): no gradient for J, and the position gradient
+    includes the direction's dependence on the source positions (gradcheck in FP64)."""
+    import torch
+    from bachelors_b200 import Plan
+    from bachelors_b200.autograd import biot_savart
+    xyz, w, _ = G.torus(8, 4, 2, 2.0, 0.5, current="azimuthal")
+    rng = np.random.default_rng(12)
+    tgt = rng.normal(size=(6, 3))
+    tgt = tgt / np.linalg.norm(tgt, axis=1, keepdims=True) * 6.0
+    c, H = G.root_cube(xyz, tgt)
+    plan = Plan(order=16, leaf_capacity=8, precision="fp64", root=(c, H * 1.01))
+    X = torch.tensor(xyz, dtype=torch.float64, device="cuda", requires_grad=True)
+    Wt = torch.tensor(w, dtype=torch.float64, device="cuda")
+    T = torch.tensor(tgt, dtype=torch.float64, device="cuda")
+    f = lambda x: biot_savart(x, Wt, None, T, plan=plan) * 1e7
+    assert torch.autograd.gradcheck(f, (X,), eps=1e-6, atol=1e-5, rtol=1e-3)
+    plan.close()
