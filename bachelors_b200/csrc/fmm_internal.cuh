@@ -203,6 +203,12 @@ struct Plan
    int tcDrainFar = 8;                   // the same through the first (far) half of a tile's offsets
    int tcDrainEvery = 8;                 // offsets accumulated in tensor memory between drains (BF16X6,
                                          // with twice the accumulations per offset, drains twice as often)
+   int tcProf = 0;                       // FMM_TC_PROF=1: per-role cycle counts of the M2L launch to stderr
+   DevBuf tcProfBuf;
+   int tcAsyncArrive = 1;                // tensor-core pipelines: producers arrive through cp.async.mbarrier
+                                         // (0: wait for their copies, then arrive; one item in flight)
+   int tcCorrCut = -2;                   // tensor-core M2L: correction products only for l + lambda <= this
+                                         // (-1: every term the degree cutoff keeps; -2: 10)
    int tcDrainMode = 3;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1,
                                          // 3: as 2 with 32 more columns in the drain threads' registers
    int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length

@@ -89,6 +89,22 @@ __device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t parity)
    return ok != 0;
 }
 
+// The same test, but a thread whose phase has not completed is suspended in hardware until it does or
+// until about suspendNs nanoseconds have passed: a waiting role then takes no issue slots from the
+// MMA-issuing warp that shares its scheduler (spinning roles slowed every MMA by half).
+__device__ __forceinline__ bool mbarTryWaitSleep(uint32_t bar, uint32_t parity, uint32_t suspendNs)
+{
+   uint32_t ok;
+   asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(suspendNs)
+      : "memory");
+   return ok != 0;
+}
+
 // Bounded pipeline wait; returns false when another role of the CTA has given up, or (raising
 // the error word and the CTA's abort flag) when limitNs expires.
 __device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity, int* err, volatile int* abortFlag,
@@ -96,9 +112,11 @@ __device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity, int* err
 {
    if(mbarTryWait(bar, parity)) return true;
    const uint64_t t0 = globalTimer();
+   // suspended tests of at most ~1 us (never beyond the limit) between the checks of the limit and the flag
+   const uint32_t hint = uint32_t(limitNs < 1000 ? limitNs : 1000);
    while(true)
    {
-      if(mbarTryWait(bar, parity)) return true;
+      if(mbarTryWaitSleep(bar, parity, hint)) return true;
       if(*abortFlag) return false;
       if(globalTimer() - t0 > limitNs)
       {
@@ -118,7 +136,7 @@ __device__ __forceinline__ bool mbarWaitIssued(uint32_t bar, uint32_t parity, in
    const uint64_t t0 = globalTimer();
    while(true)
    {
-      if(mbarTryWait(bar, parity)) return true;
+      if(mbarTryWaitSleep(bar, parity, 1000)) return true;
       if(globalTimer() - t0 > TIMEOUT_NS)
       {
          atomicOr(err, ERR_TIMEOUT);
@@ -133,6 +151,12 @@ __device__ __forceinline__ void cpAsync16(uint32_t dst, const void* src, uint32_
    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(srcBytes) : "memory");
 }
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Arrive on the mbarrier once every cp.async this thread issued so far has landed (counts as one of
+// the barrier's expected arrivals); the thread itself does not wait.
+__device__ __forceinline__ void cpAsyncArriveNoinc(uint32_t bar)
+{
+   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void bulkLoad(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
@@ -326,10 +350,16 @@ __global__ void kPrepM2LImage(const double* __restrict__ op64, int nOps, int L, 
 // Output columns each 16-wide K step of the M2L needs: with the degree cutoff l + lambda <= P, the
 // inputs of a K step (degrees >= lambda_min) only reach outputs of degree <= P - lambda_min,
 // which are the first (P - lambda_min + 1)^2 columns (rounded up to 16). Step 0 is always full.
+// The correction products (hi*lo, lo*hi, and the smaller ones of BF16X6) of a K step reach only the
+// outputs of degree <= C - lambda_min (nc, C <= P, rounded up to 16 as well): with box-size scaled
+// expansions a term of degrees (l, lambda) scales like q^(l + lambda) (q < 1 with the distance of the
+// offset), so far beyond degree C the hi*hi product's 2^-9 relative rounding is below the result's
+// accuracy, and those terms need no correction passes.
 constexpr int MAXKSTEPS = 64;   // K steps of one row (38 at p = 16 with 8-element TF32 steps)
 struct M2LCols
 {
-   int n[MAXKSTEPS];
+   int n[MAXKSTEPS];    // output columns of the leading product (hi * hi)
+   int nc[MAXKSTEPS];   // output columns of the correction products, <= n
 };
 
 template <int NP, bool TF32>
@@ -370,6 +400,33 @@ __device__ __forceinline__ bool drainAfter(int oi, int nOff, int dNear, int dFar
    return (oi + 1 - half) % dNear == 0;
 }
 
+// drainAfter as a running schedule, asked once per offset in order, without divisions (the MMA-issuing
+// thread runs it once per offset, on the pipeline's critical path)
+struct DrainSchedule
+{
+   int run = 0, half, nOff, dNear, dFar;
+   __device__ DrainSchedule(int n, int dn, int df) : half(dn == df ? -1 : n / 2), nOff(n), dNear(dn), dFar(df) {}
+   __device__ __forceinline__ bool after(int oi)
+   {
+      const int limit = oi < half ? dFar : dNear;
+      const bool d = oi == nOff - 1 || oi == half - 1 || run + 1 == limit;
+      run = d ? 0 : run + 1;
+      return d;
+   }
+};
+
+// Position in the pipeline kept by increments (no divisions in the loops): the stage s and the parity
+// of its current use, the K chunk c of the current offset and the offset's index oi.
+struct PipeCursor
+{
+   int s = 0, ph = 0, c = 0, oi = 0;
+   __device__ __forceinline__ void next(int NS, int nChunks)
+   {
+      if(++s == NS) { s = 0; ph ^= 1; }
+      if(++c == nChunks) { c = 0; ++oi; }
+   }
+};
+
 // 18 warps: five of them share one SM sub-partition's 16K registers, so 96 per thread at most.
 // PIECES: the final outputs are also stored as operand pieces (Mout); the M2M's form.
 template <int NP, class Lay, bool PIECES = false>
@@ -377,8 +434,11 @@ __global__ void __maxnreg__(96)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int nOps, int L, int Lp,
        int nChunks, const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc,
        int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainFar, int drainItems, int nStages, int drainMode,
-       const M2LCols cols, unsigned long long* counters, int* err, uint64_t waitNs)
+       const M2LCols cols, unsigned long long* counters, int* err, uint64_t waitNs, int asyncArrive,
+       unsigned long long* prof)
 {
+   // prof (developer switch): SM cycles per role, summed over CTAs, see TcProf
+   const long long tStart = prof ? clock64() : 0;
    using namespace tc;
    constexpr int KCH = Lay::KC;
    constexpr int KS = Lay::KSTEP;                      // K elements per MMA
@@ -406,6 +466,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    int* itemOffset = reinterpret_cast<int*>(ctrl + 256);        // compacted present offsets [316] + count
    int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
    int* colTab = tileNode + 64;                                 // output columns per K step [MAXKSTEPS]
+   int* corTab = colTab + MAXKSTEPS;                            // ... of the correction products [MAXKSTEPS]
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
@@ -420,7 +481,11 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    if(tid == 0)
    {
 #pragma unroll
-      for(int g = 0; g < MAXKSTEPS; g++) colTab[g] = cols.n[g];
+      for(int g = 0; g < MAXKSTEPS; g++)
+      {
+         colTab[g] = cols.n[g];
+         corTab[g] = cols.nc[g];
+      }
    }
    if(tid == 0)
    {
@@ -474,6 +539,11 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    const int nOff = itemOffset[316];
    const int nItems = nOff * nChunks;
    const uint32_t tmem = *tmemBase;
+   if(prof && tid == 0)
+   {
+      atomicAdd(prof + 10, (unsigned long long)(clock64() - tStart));
+      atomicAdd(prof + 11, (unsigned long long)nItems);
+   }
 
    if(warp == 0)
    {
@@ -481,21 +551,43 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       {
          bool firstMma = true;
          int drains = 0;
-         for(int it = 0; it < nItems; it++)
+         long long tw0 = 0, tw1 = 0, tw2 = 0;
+         long long tIssue[6] = {0, 0, 0, 0, 0, 0};   // per K chunk: from the stage's arrival to the commit
+         const long long tl = prof ? clock64() : 0;
+         DrainSchedule sched(nOff, drainEvery, drainFar);
+         PipeCursor cur;
+         int sinceDrain = 0;
+         for(int it = 0; it < nItems; it++, cur.next(NS, nChunks))
          {
-            const int s = it % NS;
+            const int s = cur.s;
             // this chunk's output widths per K step, read before the wait
-            int nColK[KCH / KS];
+            int nColK[KCH / KS], nCorK[KCH / KS];
 #pragma unroll
-            for(int ks = 0; ks < KCH / KS; ks++) nColK[ks] = colTab[(it % nChunks) * (KCH / KS) + ks];
-            if(!mbarWait(fullBar0 + 8 * s, (it / NS) & 1, err, abortFlag, waitNs)) break;
-            if(!mbarWait(opBar0 + 8 * s, (it / NS) & 1, err, abortFlag, waitNs)) break;
+            for(int ks = 0; ks < KCH / KS; ks++)
+            {
+               nColK[ks] = colTab[cur.c * (KCH / KS) + ks];
+               nCorK[ks] = corTab[cur.c * (KCH / KS) + ks];
+            }
+            long long t0 = prof ? clock64() : 0;
+            if(!mbarWait(fullBar0 + 8 * s, cur.ph, err, abortFlag, waitNs)) break;
+            long long t1 = prof ? clock64() : 0;
+            if(!mbarWait(opBar0 + 8 * s, cur.ph, err, abortFlag, waitNs)) break;
+            long long t2 = 0;
+            if(prof)
+            {
+               t2 = clock64();
+               tw0 += t1 - t0;
+               tw1 += t2 - t1;
+            }
+            // the producers' cp.async writes (generic proxy), observed through the barrier, before
+            // the tensor core reads the stage (async proxy)
+            if(asyncArrive) fenceProxyAsync();
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
             const uint32_t aSt = st, bSt = st + NP * aBytes;
             // K steps of 16 that reach a coefficient < L (the last chunk is partly padding); chunks run
             // in increasing K, so an accumulation always starts with a full-width MMA
-            const int cItem = it % nChunks;
+            const int cItem = cur.c;
             const int kSteps = min(KCH / KS, (L - cItem * KCH + KS - 1) / KS);
             // descriptors of the stage's pieces; an MMA's operand is the piece's descriptor plus its
             // byte offset / 16 (the start-address field, bits 0-13, holds every address of the stage)
@@ -505,15 +597,19 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             {
                if(ks >= kSteps) break;
                const uint32_t koff = ks * 32;
-               // this K step's output columns in one MMA (<= 256) or two (256 + the rest)
+               // this K step's output columns in one MMA (<= 256) or two (256 + the rest); the
+               // correction products over the first nCor of them
                const int nCol = nColK[ks];
                if(nCol == 0) break;
-               const int nA = min(nCol, 256), nB = nCol - nA;
-               const uint32_t idA = Lay::TF32 ? instrDescTf32(ROWS, nA) : instrDescBf16(ROWS, nA);
-               const uint32_t idB = Lay::TF32 ? instrDescTf32(ROWS, nB > 0 ? nB : 16) : instrDescBf16(ROWS, nB > 0 ? nB : 16);
+               const int nCor = nCorK[ks];
 #pragma unroll
                for(int pass = 0; pass < NPASS; pass++)
                {
+                  const int w = pass == 0 ? nCol : nCor;
+                  if(w == 0) break;
+                  const int nA = min(w, 256), nB = w - nA;
+                  const uint32_t idA = Lay::TF32 ? instrDescTf32(ROWS, nA) : instrDescBf16(ROWS, nA);
+                  const uint32_t idB = Lay::TF32 ? instrDescTf32(ROWS, nB > 0 ? nB : 16) : instrDescBf16(ROWS, nB > 0 ? nB : 16);
                   const int pa = NP == 1 ? 0 : (NP == 2 ? PA2[pass] : PA[pass]);
                   const int pb = NP == 1 ? 0 : (NP == 2 ? PB2[pass] : PB[pass]);
                   const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
@@ -533,21 +629,29 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                }
             }
             mmaCommit(emptyBar0 + 8 * s);
+            if(prof && cur.c < 6) tIssue[cur.c] += clock64() - t2;
             // every drainEvery offsets (and after the last) hand the accumulator to the drain warps
             // and start a fresh one: the tensor cores' FP32 accumulation truncates, so long chains
             // of accumulations into one TMEM value drift; the running sum is kept in FP32 instead
             // (drainItems > 0: every drainItems pipeline items instead, for full-width operators only:
             // a fresh accumulation must start with an MMA that writes every column)
-            const bool drainNow = drainItems > 0 ? ((it + 1) % drainItems == 0 || it == nItems - 1)
-                                                 : (it % nChunks == nChunks - 1 &&
-                                                    drainAfter(it / nChunks, nOff, drainEvery, drainFar));
+            bool drainNow;
+            if(drainItems > 0)
+            {
+               drainNow = ++sinceDrain == drainItems || it == nItems - 1;
+               if(drainNow) sinceDrain = 0;
+            }
+            else
+               drainNow = cur.c == nChunks - 1 && sched.after(cur.oi);
             {
                if(drainNow)
                {
                   mmaCommit(drainFull);
                   if(it != nItems - 1)
                   {
+                     const long long t3 = prof ? clock64() : 0;
                      if(!mbarWait(drainEmpty, drains & 1, err, abortFlag, waitNs)) break;
+                     if(prof) tw2 += clock64() - t3;
                      fenceAfterSync();
                   }
                   drains++;
@@ -556,6 +660,14 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             }
          }
          mmaCommit(doneBar);
+         if(prof)
+         {
+            atomicAdd(prof + 0, (unsigned long long)tw0);
+            atomicAdd(prof + 1, (unsigned long long)tw1);
+            atomicAdd(prof + 2, (unsigned long long)tw2);
+            atomicAdd(prof + 3, (unsigned long long)(clock64() - tl));
+            for(int c = 0; c < 6; c++) atomicAdd(prof + 16 + c, (unsigned long long)tIssue[c]);
+         }
       }
       __syncwarp();
    }
@@ -564,18 +676,27 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       if(lane == 0)
       {
          int issued = 0;
-         for(int it = 0; it < nItems; it++)
+         long long twe = 0;
+         PipeCursor cur;
+         for(int it = 0; it < nItems; it++, cur.next(NS, nChunks))
          {
-            const int s = it % NS;
-            if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag, waitNs)) break;
-            const int o = itemOffset[it / nChunks], c = it % nChunks;
+            const int s = cur.s;
+            const long long t0 = prof ? clock64() : 0;
+            // the stage's previous use (parity ph ^ 1) must have been consumed
+            if(it >= NS && !mbarWait(emptyBar0 + 8 * s, cur.ph ^ 1, err, abortFlag, waitNs)) break;
+            if(prof) twe += clock64() - t0;
+            const int o = itemOffset[cur.oi], c = cur.c;
             const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
             const uint32_t dst = base + s * stageBytes + NP * aBytes;
-            // only the operator rows (output columns) this chunk's widest K step uses
+            // only the operator rows (output columns) this chunk's widest K step uses: of the leading
+            // piece for the hi * hi product, of the others for the correction products
             const uint32_t rowBytes = uint32_t(colTab[c * (KCH / KS)]) * Lay::RB;
-            mbarArriveExpectTx(opBar0 + 8 * s, NP * rowBytes);
+            const uint32_t corBytes = uint32_t(corTab[c * (KCH / KS)]) * Lay::RB;
+            mbarArriveExpectTx(opBar0 + 8 * s, rowBytes + (NP - 1) * corBytes);
+            bulkLoad(dst, src, rowBytes, opBar0 + 8 * s);
 #pragma unroll
-            for(int j = 0; j < NP; j++) bulkLoad(dst + j * bBytes, src + j * bBytes, rowBytes, opBar0 + 8 * s);
+            for(int j = 1; j < NP; j++)
+               if(corBytes) bulkLoad(dst + j * bBytes, src + j * bBytes, corBytes, opBar0 + 8 * s);
             issued = it + 1;
          }
          // the copies in flight write this CTA's shared memory: wait for them before it can exit. A stage
@@ -586,6 +707,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             const int last = s + ((issued - 1 - s) / NS) * NS;
             mbarWaitIssued(opBar0 + 8 * s, (last / NS) & 1, err);
          }
+         if(prof) atomicAdd(prof + 4, (unsigned long long)twe);
       }
       __syncwarp();
    }
@@ -628,9 +750,13 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       float rsum[RHALF];
 #pragma unroll
       for(int i = 0; i < RHALF; i++) rsum[i] = 0.f;
+      long long twd = 0;
+      const long long tdl = prof ? clock64() : 0;
       for(int d = 0; d < nDrains; d++)
       {
+         const long long t0 = prof ? clock64() : 0;
          if(!mbarWait(drainFull, d & 1, err, abortFlag, waitNs)) break;
+         if(prof) twd += clock64() - t0;
          fenceAfterSync();
          const bool last = d == nDrains - 1;
          // tensor-memory part: S += acc (d > 0) or S = acc; the last drain writes S + acc to the locals
@@ -730,6 +856,11 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          fenceBeforeSync();
          mbarArrive(drainEmpty);
       }
+      if(prof && warp == 10 && lane == 0)
+      {
+         atomicAdd(prof + 7, (unsigned long long)twd);
+         atomicAdd(prof + 8, (unsigned long long)(clock64() - tdl));
+      }
    }
    else
    {
@@ -745,24 +876,33 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       const int tgt = row < 3 * TT ? tileNode[slot] : -1;
       int src = (tgt >= 0 && nItems > 0) ? vtab[int64_t(tgt) * nOps + itemOffset[0]] : -1;
       int srcNext = -1;
-      int pending = -1;
-      for(int it = 0; it < nItems; it++)
+      int pending = -1;   // stage of the item whose copies are still to be signalled (synchronous form)
+      long long twp = 0;
+      const long long tpl = prof ? clock64() : 0;
+      PipeCursor cur;
+      for(int it = 0; it < nItems; it++, cur.next(NS, nChunks))
       {
-         const int s = it % NS;
-         const int oi = it / nChunks, c = it % nChunks;
-         if(it % nChunks == 0 && oi + 1 < nOff)
+         const int s = cur.s;
+         const int oi = cur.oi, c = cur.c;
+         if(c == 0 && oi + 1 < nOff)
             srcNext = tgt >= 0 ? vtab[int64_t(tgt) * nOps + itemOffset[oi + 1]] : -1;
          if(pending >= 0)
          {
+            // (synchronous form: this thread waits for its previous item's copies, then arrives)
             cpAsyncWaitAll();
             fenceProxyAsync();
-            mbarArrive(fullBar0 + 8 * (pending % NS));
+            mbarArrive(fullBar0 + 8 * pending);
             pending = -1;
          }
-         if(it >= NS && !mbarWait(emptyBar0 + 8 * s, (it / NS - 1) & 1, err, abortFlag, waitNs)) break;
+         const long long t0 = prof ? clock64() : 0;
+         if(it >= NS && !mbarWait(emptyBar0 + 8 * s, cur.ph ^ 1, err, abortFlag, waitNs)) break;
+         if(prof) twp += clock64() - t0;
          const uint32_t aSt = base + s * stageBytes;
          const int k0 = c * KCH + half * PER;
          const uint8_t* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp * Lay::ES;
+         // the pieces after the leading one feed only the correction products: none in this chunk when
+         // its first (widest) K step has none
+         const int npc = corTab[c * (KCH / Lay::KSTEP)] > 0 ? NP : 1;
 #pragma unroll
          for(int q = 0; q < PER / EPC; q++)
          {
@@ -771,17 +911,30 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             const uint32_t off = Lay::off(uint32_t(row), uint32_t(half * PER + EPC * q));
 #pragma unroll
             for(int j = 0; j < NP; j++)
-               cpAsync16(aSt + j * aBytes + off, rowp + (int64_t(j) * Lp + (bytes ? k : 0)) * Lay::ES, bytes);
+               if(j < npc)
+                  cpAsync16(aSt + j * aBytes + off, rowp + (int64_t(j) * Lp + (bytes ? k : 0)) * Lay::ES, bytes);
          }
-         cpAsyncCommit();
-         pending = it;
-         if(it % nChunks == nChunks - 1) src = srcNext;
+         if(asyncArrive)
+            // the barrier completes when every producer's copies of this item have landed, while the
+            // thread goes on with the next free stage: up to NS items in flight
+            cpAsyncArriveNoinc(fullBar0 + 8 * s);
+         else
+         {
+            cpAsyncCommit();
+            pending = s;
+         }
+         if(c == nChunks - 1) src = srcNext;
       }
       cpAsyncWaitAll();
       if(pending >= 0 && !*abortFlag)
       {
          fenceProxyAsync();
-         mbarArrive(fullBar0 + 8 * (pending % NS));
+         mbarArrive(fullBar0 + 8 * pending);
+      }
+      if(prof && tid == 64)
+      {
+         atomicAdd(prof + 5, (unsigned long long)twp);
+         atomicAdd(prof + 6, (unsigned long long)(clock64() - tpl));
       }
    }
    fenceBeforeSync();
@@ -795,6 +948,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       fenceAfterSync();
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
    }
+   if(prof && tid == 0) atomicAdd(prof + 9, (unsigned long long)(clock64() - tStart));
 }
 
 template <int NP, class Lay>
@@ -815,21 +969,17 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    const int count = P.nM2LTargets;
    if(count <= 0) return FMM_OK;
    const int blocks = (count + tc::TT - 1) / tc::TT;
-   const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + MAXKSTEPS);
-   const size_t budget = 232448;
-   const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
-   if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
-   const size_t smem = fixed + nStages * stageBytes;
-   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_TRY(P.tcCounters.reserve(2 * sizeof(unsigned long long)));
    FMM_CUDA(cudaMemsetAsync(P.tcCounters.ptr, 0, 2 * sizeof(unsigned long long), st));
    P.tcTiles = blocks;
-   // first MMA's width: all of N up to 256, else 256 or (balanced) the multiple of 16 nearest N / 2;
-   // the second starts on an 8-row boundary of the swizzled operator block either way
    // the degree cutoff: 0 -> p + 8, negative -> none (l + lambda <= 2p, the full operator)
    const int cut = P.cfg.m2l_tc_degree_cutoff == 0 ? P.p + 8 : (P.cfg.m2l_tc_degree_cutoff < 0 ? 2 * P.p
                                                                 : std::max(P.cfg.m2l_tc_degree_cutoff, P.p));
+   // correction products: by default for l + lambda <= 10. The size of the terms they correct falls with
+   // l + lambda whatever p is (box-size scaled bases); at p = 16 this leaves the error against the FP64
+   // direct sum unchanged to 1 % and costs 40 % of three full passes.
+   const int corrSet = P.tcCorrCut == -2 ? 10 : P.tcCorrCut;
+   const int corr = corrSet < 0 ? -1 : std::min(cut, corrSet);
    M2LCols cols{};
    if(nChunks * (Lay::KC / Lay::KSTEP) > MAXKSTEPS)
       return setError(FMM_E_INVALID, "tensor-core M2L: %d K steps exceed the column table", nChunks * (Lay::KC / Lay::KSTEP));
@@ -841,8 +991,27 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
       int n = cut - lmin >= 0 ? std::min(L, (cut - lmin + 1) * (cut - lmin + 1)) : 0;
       n = std::min(Lp, (n + 15) / 16 * 16);
       cols.n[g] = k < L ? n : 0;
+      // correction products: up to degree corr - lambda_min (corr < 0: as the leading product)
+      int nc = corr - lmin >= 0 ? std::min(L, (corr - lmin + 1) * (corr - lmin + 1)) : 0;
+      nc = std::min(Lp, (nc + 15) / 16 * 16);
+      cols.nc[g] = corr < 0 ? cols.n[g] : std::min(cols.n[g], nc);
    }
+   const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
+   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS);
+   const size_t budget = 232448;
+   const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
+   if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
+   const size_t smem = fixed + nStages * stageBytes;
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    const int64_t rows = P.tree.nNodes * 3;
+   // developer switch FMM_TC_PROF=1: per-role SM cycles of this launch, printed to stderr
+   unsigned long long* prof = nullptr;
+   if(P.tcProf)
+   {
+      FMM_TRY(P.tcProfBuf.reserve(24 * sizeof(unsigned long long)));
+      prof = (unsigned long long*)P.tcProfBuf.ptr;
+      FMM_CUDA(cudaMemsetAsync(prof, 0, 24 * sizeof(unsigned long long), st));
+   }
    // the tensor-core M2M leaves every source level's multipoles split in this format
    if(P.multBfTag != NP * 2 + (Lay::TF32 ? 1 : 0))
    {
@@ -853,8 +1022,25 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
                                                       nChunks, (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
                                                       (float*)P.local.ptr, 0, nullptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
-                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.pipeErr, P.tcWaitNs);
+                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive,
+                                                      prof);
    FMM_TRY(launched(P, "kM2LTc", st));
+   if(prof)
+   {
+      unsigned long long h[24];
+      FMM_CUDA(cudaMemcpyAsync(h, prof, sizeof(h), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+      const double b = double(blocks), it = double(h[11]) / b;
+      fprintf(stderr,
+              "kM2LTc profile, SM cycles per CTA (%d CTAs, %.0f items each): total %.0f, prologue %.0f | MMA thread: "
+              "loop %.0f, wait producers %.0f, wait operator %.0f, wait drain %.0f | operator thread: wait stage %.0f "
+              "| producer: loop %.0f, wait stage %.0f | drain: loop %.0f, wait accumulator %.0f\n",
+              blocks, it, h[9] / b, h[10] / b, h[3] / b, h[0] / b, h[1] / b, h[2] / b, h[4] / b, h[6] / b, h[5] / b,
+              h[8] / b, h[7] / b);
+      fprintf(stderr, "kM2LTc profile, MMA thread cycles per item from the stage's arrival to its commit, by K chunk:");
+      for(int c = 0; c < std::min(nChunks, 6); c++) fprintf(stderr, " %.0f", h[16 + c] * double(nChunks) / double(h[11]));
+      fprintf(stderr, "\n");
+   }
    // a timed-out wait raises the pipeline error word, which the calling phase reads once at its end
    return FMM_OK;
 }
@@ -886,18 +1072,18 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
       FMM_TRY(launched(P, "kPrepM2LImage", st));
       P.opTrImgTag = tag;
    }
+   M2LCols cols{};
+   const int nSteps = nChunks * (Lay::KC / Lay::KSTEP);
+   if(nSteps > MAXKSTEPS) return setError(FMM_E_INVALID, "tensor-core translation: %d K steps exceed the column table", nSteps);
+   for(int g = 0; g < nSteps; g++) cols.n[g] = cols.nc[g] = Lay::KSTEP * g < L ? Lp : 0;
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + MAXKSTEPS);
+   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS);
    const size_t budget = 232448;
    const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core translation: %zu-byte stages do not fit twice", stageBytes);
    const size_t smem = fixed + nStages * stageBytes;
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
    FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-   M2LCols cols{};
-   const int nSteps = nChunks * (Lay::KC / Lay::KSTEP);
-   if(nSteps > MAXKSTEPS) return setError(FMM_E_INVALID, "tensor-core translation: %d K steps exceed the column table", nSteps);
-   for(int g = 0; g < nSteps; g++) cols.n[g] = Lay::KSTEP * g < L ? Lp : 0;
    const int64_t rows = P.tree.nNodes * 3;
    FMM_TRY(P.multBf.reserve(size_t(Lay::ES) * rows * NP * Lp));
    const int drainEvery = NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2);
@@ -925,7 +1111,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          kern<<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.parList.ptr + a, b - a, (const int*)P.vtabUp.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0,
-            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs);
+            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
          FMM_TRY(launched(P, "kM2LTc<M2M>", st));
       }
       P.multBfTag = NP * 2 + (Lay::TF32 ? 1 : 0);
@@ -941,7 +1127,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
             (const int*)P.l2lTargets.ptr + a, b - a, (const int*)P.vtabDn.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, nullptr, drainEvery, drainEvery,
             P.tcTrDrainItems, nStages,
-            P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs);
+            P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
          FMM_TRY(launched(P, "kM2LTc<L2L>", st));
       }
       P.multBfTag = -1;
