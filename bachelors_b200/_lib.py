@@ -14,13 +14,15 @@ LIB_PATH = os.path.join(HERE, "libfmmcuda.so")
 FMM_OK, FMM_E_INVALID, FMM_E_OOM, FMM_E_CUDA, FMM_E_TIMEOUT, FMM_E_LIMIT = range(6)
 FMM_FP32, FMM_FP64 = 0, 1
 FMM_M2L_SIMT, FMM_M2L_BF16X3, FMM_M2L_TF32, FMM_M2L_BF16X6 = 0, 1, 2, 3
+FMM_TREECODE_REFERENCE_NEAR, FMM_TREECODE_FD_CURL = 1, 2
 
 # Every extern "C" symbol include/fmmcuda.h declares.
 EXPORTS = [
-    "fmm_default_config", "fmm_plan_create", "fmm_plan_destroy", "fmm_set_sources", "fmm_set_targets",
+    "fmm_default_config", "fmm_plan_create", "fmm_plan_destroy", "fmm_set_sources", "fmm_set_bem_sources",
+    "fmm_set_targets",
     "fmm_set_targets_to_sources",
     "fmm_build_tree", "fmm_upward", "fmm_downward", "fmm_evaluate", "fmm_solve", "fmm_direct",
-    "fmm_direct_fp64_subset", "fmm_adjoint", "fmm_adjoint_direct", "fmm_autotune", "fmm_get_tuning",
+    "fmm_direct_fp64_subset", "fmm_treecode", "fmm_adjoint", "fmm_adjoint_direct", "fmm_autotune", "fmm_get_tuning",
     "fmm_set_tuning", "fmm_batch_set_coils", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
     "fmm_set_wait_limit", "fmm_get_stats", "fmm_get_operator", "fmm_direct_B_noalloc", "fmm_translate_all", "fmm_translate_all_matrix",
     "fmm_translate_all_matrix_complex", "fmm_add_vectors",
@@ -82,6 +84,7 @@ def load():
         "fmm_plan_create": (ctypes.c_int, [ctypes.POINTER(FmmConfig), ctypes.POINTER(vp)]),
         "fmm_plan_destroy": (ctypes.c_int, [vp]),
         "fmm_set_sources": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.c_int, vp]),
+        "fmm_set_bem_sources": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, ctypes.c_int, vp]),
         "fmm_set_targets": (ctypes.c_int, [vp, vp, i64, ctypes.c_int, vp]),
         "fmm_set_targets_to_sources": (ctypes.c_int, [vp, vp]),
         "fmm_build_tree": (ctypes.c_int, [vp, vp]),
@@ -91,6 +94,7 @@ def load():
         "fmm_solve": (ctypes.c_int, [vp, dbl, ctypes.c_int, vp, vp, ctypes.c_int, vp]),
         "fmm_direct": (ctypes.c_int, [vp, dbl, ctypes.c_int, vp, vp, ctypes.c_int, vp]),
         "fmm_direct_fp64_subset": (ctypes.c_int, [vp, dbl, vp, i64, vp]),
+        "fmm_treecode": (ctypes.c_int, [vp, dbl, ctypes.c_int, vp, i64, vp, vp, ctypes.c_int, ctypes.c_int, vp]),
         "fmm_adjoint": (ctypes.c_int, [vp, dbl, vp, vp, vp, ctypes.c_int, vp]),
         "fmm_adjoint_direct": (ctypes.c_int, [vp, dbl, vp, vp, vp, ctypes.c_int, vp]),
         "fmm_autotune": (ctypes.c_int, [vp, ctypes.POINTER(FmmTuning), vp]),

@@ -137,7 +137,7 @@ void Plan::release()
    DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
                      &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &parList, &m2lTargets, &m2lKeys, &errb,
                      &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf, &multBf, &tcCounters,
-                     &adjG, &adjOut, &nearCounts, &tcProfBuf, &curlTab, &vtabUp, &vtabDn, &l2lTargets, &l2lKeys, &opM2Mbf, &opL2Lbf};
+                     &adjG, &adjOut, &tcPts, &tcOut, &srcSigmab, &nearCounts, &tcProfBuf, &curlTab, &vtabUp, &vtabDn, &l2lTargets, &l2lKeys, &opM2Mbf, &opL2Lbf};
    for(DevBuf* b : bufs) b->release();
    for(auto& b : nodeBufs) b.release();
    for(auto& b : listBufs) b.release();
@@ -324,10 +324,61 @@ fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const
    P.hasJ = J != nullptr;
    if(P.hasJ) FMM_TRY(copyIn(P.srcJb, J, es * 3 * n, on_device, st, &P.srcJ));
    if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
+   P.bem = false;
    P.n = n;
    P.treeReady = P.upReady = P.downReady = false;
    P.dropGraph();
    return FMM_OK;
+}
+
+fmm_status fmm_set_bem_sources(fmm_plan* plan, const void* xyz, const void* w, const void* B, const void* normal,
+                               int64_t n, int on_device, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   if(n < 0 || n > (int64_t(1) << 31) - 1) return setError(FMM_E_INVALID, "source count %lld out of range", (long long)n);
+   if(n > 0 && (!xyz || !w || !B || !normal)) return setError(FMM_E_INVALID, "fmm_set_bem_sources: null argument");
+   Plan& P = plan->P;
+   if(P.batch) return setError(FMM_E_INVALID, "fmm_set_bem_sources: not available on a batched plan");
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_TRY(copyIn(P.srcXYZb, xyz, es * 3 * n, on_device, st, &P.srcXYZ));
+   FMM_TRY(copyIn(P.srcWb, w, es * n, on_device, st, &P.srcW));
+   FMM_TRY(P.srcJb.reserve(std::max<size_t>(es * 3 * n, 16)));
+   FMM_TRY(P.srcSigmab.reserve(std::max<size_t>(es * n, 16)));
+   P.srcJ = P.srcJb.ptr;
+   P.srcSigma = P.srcSigmab.ptr;
+   P.n = n;
+   P.hasJ = true;
+   P.bem = true;
+   // B and the normals (staged when on the host) become J = B x n and sigma = B . n
+   const void* dB = B;
+   const void* dN = normal;
+   DevBuf stage;
+   if(!on_device && n > 0)
+   {
+      FMM_TRY(stage.reserve(2 * es * 3 * n));
+      cudaError_t e = cudaMemcpyAsync(stage.ptr, B, es * 3 * n, cudaMemcpyHostToDevice, st);
+      if(e == cudaSuccess)
+         e = cudaMemcpyAsync((char*)stage.ptr + es * 3 * n, normal, es * 3 * n, cudaMemcpyHostToDevice, st);
+      if(e != cudaSuccess)
+      {
+         stage.release();
+         return setError(FMM_E_CUDA, "fmm_set_bem_sources: %s", cudaGetErrorString(e));
+      }
+      dB = stage.ptr;
+      dN = (char*)stage.ptr + es * 3 * n;
+   }
+   fmm_status s = P.fp64 ? bemPrepareT<double>(P, dB, dN, st) : bemPrepareT<float>(P, dB, dN, st);
+   if(!on_device || stage.ptr)
+   {
+      cudaError_t e = cudaStreamSynchronize(st);
+      if(s == FMM_OK && e != cudaSuccess) s = setError(FMM_E_CUDA, "fmm_set_bem_sources: %s", cudaGetErrorString(e));
+   }
+   stage.release();
+   P.treeReady = P.upReady = P.downReady = false;
+   P.dropGraph();
+   return s;
 }
 
 fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_device, void* stream)
@@ -412,6 +463,8 @@ fmm_status fmm_evaluate(fmm_plan* plan, double current, int want, void* out_B, v
    Plan& P = plan->P;
    if(!P.downReady) return setError(FMM_E_INVALID, "fmm_evaluate: local expansions are not ready");
    if(want < 1 || want > 3) return setError(FMM_E_INVALID, "want must be 1, 2 or 3");
+   if(P.bem && want != 2)
+      return setError(FMM_E_INVALID, "a plan with BEM sources evaluates the BEM integral into out_A (want = 2)");
    if(((want & 1) && !out_B) || ((want & 2) && !out_A)) return setError(FMM_E_INVALID, "null output buffer");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
@@ -443,6 +496,8 @@ fmm_status fmm_evaluate(fmm_plan* plan, double current, int want, void* out_B, v
 
 fmm_status fmm_solve(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device, void* stream)
 {
+   if(plan && plan->P.bem && want != 2)
+      return setError(FMM_E_INVALID, "a plan with BEM sources evaluates the BEM integral into out_A (want = 2)");
    FMM_TRY(fmm_build_tree(plan, stream));
    Plan& P = plan->P;
    DeviceGuard g(P.cfg.device);
@@ -462,6 +517,8 @@ fmm_status fmm_direct(fmm_plan* plan, double current, int want, void* out_B, voi
    Plan& P = plan->P;
    if(want < 1 || want > 3) return setError(FMM_E_INVALID, "want must be 1, 2 or 3");
    if(((want & 1) && !out_B) || ((want & 2) && !out_A)) return setError(FMM_E_INVALID, "null output buffer");
+   if(P.bem && want != 2)
+      return setError(FMM_E_INVALID, "a plan with BEM sources sums the BEM integral into out_A (want = 2)");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
    if(!P.treeReady) FMM_TRY(fmm_build_tree(plan, stream));
@@ -507,6 +564,7 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
    if(!plan) return setError(FMM_E_INVALID, "null plan");
    Plan& P = plan->P;
    if(P.n == 0 || P.m == 0) return setError(FMM_E_INVALID, "fmm_adjoint: sources and targets must be set");
+   if(P.bem) return setError(FMM_E_INVALID, "fmm_adjoint: not available for BEM sources");
    if(!dL_dB || (!dL_dJ && !dL_dx)) return setError(FMM_E_INVALID, "fmm_adjoint: null argument");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
@@ -555,12 +613,56 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
    return FMM_OK;
 }
 
+fmm_status fmm_treecode(fmm_plan* plan, double current, int want, const void* pts, int64_t m, void* out_B, void* out_A,
+                        int flags, int on_device, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   Plan& P = plan->P;
+   if(!P.upReady) return setError(FMM_E_INVALID, "fmm_treecode: multipoles are not ready (fmm_build_tree, fmm_upward)");
+   if(P.batch) return setError(FMM_E_INVALID, "fmm_treecode: a query point belongs to no coil of a batched plan");
+   if(want < 1 || want > 3) return setError(FMM_E_INVALID, "want must be 1, 2 or 3");
+   if(flags & ~(FMM_TREECODE_REFERENCE_NEAR | FMM_TREECODE_FD_CURL))
+      return setError(FMM_E_INVALID, "fmm_treecode: unknown flags 0x%x", flags);
+   if(P.bem && want != 2)
+      return setError(FMM_E_INVALID, "fmm_treecode: a plan with BEM sources evaluates the BEM integral (want = 2)");
+   if(m < 0 || m > (int64_t(1) << 31) - 1) return setError(FMM_E_INVALID, "query count %lld out of range", (long long)m);
+   if(m > 0 && (!pts || ((want & 1) && !out_B) || ((want & 2) && !out_A)))
+      return setError(FMM_E_INVALID, "fmm_treecode: null argument");
+   if(m == 0) return FMM_OK;
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   const size_t bytes = es * 3 * size_t(m);
+   const void* dPts = pts;
+   void* dB = out_B;
+   void* dA = out_A;
+   if(!on_device)
+   {
+      FMM_TRY(P.tcPts.reserve(bytes));
+      FMM_TRY(P.tcOut.reserve(2 * bytes));
+      FMM_CUDA(cudaMemcpyAsync(P.tcPts.ptr, pts, bytes, cudaMemcpyHostToDevice, st));
+      dPts = P.tcPts.ptr;
+      dB = (want & 1) ? P.tcOut.ptr : nullptr;
+      dA = (want & 2) ? (char*)P.tcOut.ptr + bytes : nullptr;
+   }
+   FMM_TRY(P.fp64 ? treecodeT<double>(P, current, want, dPts, m, dB, dA, flags, st)
+                  : treecodeT<float>(P, current, want, dPts, m, dB, dA, flags, st));
+   if(!on_device)
+   {
+      if(want & 1) FMM_CUDA(cudaMemcpyAsync(out_B, dB, bytes, cudaMemcpyDeviceToHost, st));
+      if(want & 2) FMM_CUDA(cudaMemcpyAsync(out_A, dA, bytes, cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+   }
+   return FMM_OK;
+}
+
 fmm_status fmm_adjoint_direct(fmm_plan* plan, double current, const void* dL_dB, void* dL_dJ, void* dL_dx,
                               int on_device, void* stream)
 {
    if(!plan) return setError(FMM_E_INVALID, "null plan");
    Plan& P = plan->P;
    if(!dL_dB || (!dL_dJ && !dL_dx)) return setError(FMM_E_INVALID, "fmm_adjoint_direct: null argument");
+   if(P.bem) return setError(FMM_E_INVALID, "fmm_adjoint_direct: not available for BEM sources");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
@@ -721,6 +823,7 @@ fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* sr
    }
    else
    {
+      if(P.bem) return setError(FMM_E_INVALID, "fmm_batch_set_coils: not available for BEM sources");
       if(ncoils < 0 || ncoils > FMM_MAX_COILS)
          return setError(FMM_E_INVALID, "fmm_batch_set_coils: %lld coils outside 0..%d", (long long)ncoils, FMM_MAX_COILS);
       if(!src_offsets || !tgt_offsets) return setError(FMM_E_INVALID, "fmm_batch_set_coils: null offsets");
@@ -747,6 +850,7 @@ fmm_status fmm_update_sources(fmm_plan* plan, const void* w, const void* J, int 
    Plan& P = plan->P;
    if(!P.treeReady) return setError(FMM_E_INVALID, "fmm_update_sources: the tree is not built");
    if(P.n > 0 && !w) return setError(FMM_E_INVALID, "fmm_update_sources: null weights");
+   if(P.bem) return setError(FMM_E_INVALID, "fmm_update_sources: set BEM sources again with fmm_set_bem_sources");
    if((J != nullptr) != P.hasJ)
       return setError(FMM_E_INVALID, "fmm_update_sources: J must be given exactly when the sources were set with J");
    DeviceGuard g(P.cfg.device);

@@ -137,6 +137,11 @@ struct Plan
    DevBuf srcXYZb, srcWb, srcJb, tgtXYZb;
    void* srcXYZ = nullptr; void* srcW = nullptr; void* srcJ = nullptr; void* tgtXYZ = nullptr;
    bool hasJ = false;
+   // the BEM problem (fmm_set_bem_sources): J = B x n and sigma = B . n per source, the plan's strengths
+   // then carry w J and w sigma (fmm_bem.cu)
+   bool bem = false;
+   DevBuf srcSigmab;
+   void* srcSigma = nullptr;
    int64_t n = 0, m = 0;
    // independent problems ("coils"): coil c owns sources [srcOff[c], srcOff[c+1]) and targets
    // [tgtOff[c], tgtOff[c+1]); one coil by default. Each coil is a root of the forest; node keys
@@ -245,6 +250,7 @@ struct Plan
    // adjoint: a plan on the swapped point sets, and staging for host inputs / outputs
    Plan* adj = nullptr;
    DevBuf adjG, adjOut;
+   DevBuf tcPts, tcOut;                  // fmm_treecode: staging of host query points and results
    bool adjointDone = false;
 
    fmm_status init(const fmm_config& c);
@@ -281,5 +287,12 @@ template <class T> fmm_status regatherStrengthsT(Plan& P, cudaStream_t st);
 template <class T> fmm_status scaleCopyT(Plan& P, const void* src, void* dst, int64_t count, double scale, cudaStream_t st);
 template <class T> fmm_status adjointT(Plan& P, Plan& A, double current, const void* g, void* dJ, void* dx, cudaStream_t st);
 template <class T> fmm_status adjointDirectT(Plan& P, double current, const void* g, void* dJ, void* dx, cudaStream_t st);
+template <class T> fmm_status bemPrepareT(Plan& P, const void* B, const void* nrm, cudaStream_t st);
+template <class T> fmm_status bemP2MT(Plan& P, cudaStream_t st);
+template <class T> fmm_status bemNearT(Plan& P, cudaStream_t st);
+template <class T> fmm_status bemDirectT(Plan& P, cudaStream_t st);
+template <class T>
+fmm_status treecodeT(Plan& P, double current, int want, const void* pts, int64_t m, void* outB, void* outA, int flags,
+                     cudaStream_t st);
 
 }  // namespace fmm

@@ -1721,7 +1721,13 @@ fmm_status upwardT(Plan& P, cudaStream_t st)
    typedef typename Vec4<T>::type V4;
    constexpr int NT = 64;
    const size_t shm = sizeof(T) * 3 * Lp;
-   if(P.p2mChunk == 0)
+   if(P.bem)
+   {
+      // dipole multipoles of the BEM sources (fmm_bem.cu); the translations below are the same
+      P.p2mPiecesTag = -1;
+      FMM_TRY(bemP2MT<T>(P, st));
+   }
+   else if(P.p2mChunk == 0)
    {
       const size_t shw = p2mWarpSmem<T>(P.p, Lp);
       if(shw > 48 * 1024)
@@ -1847,6 +1853,18 @@ fmm_status evaluateT(Plan& P, double current, int want, cudaStream_t st)
    const size_t coef = split ? 0 : (sizeof(T) * (3 * L + 3 * Lb) + 31) & ~size_t(31);
    size_t shm = coef + 2 * size_t(nearTileBytes<T>(TS)) + sizeof(double) * 6 * NT;
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
+   if(P.bem)
+   {
+      // BEM: the far field sum_k L_k R_k (the A form of the L2P), then the BEM kernel's near field and
+      // the 1 / (4 pi) of calcBEM (fast_multipole_solver.cpp:233-250; no current factor there)
+      const size_t sh = l2pWarpSmem<T, true>(P.p);
+      if(sh > 48 * 1024) FMM_CUDA(cudaFuncSetAttribute(kL2PWarp<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh)));
+      kL2PWarp<T, true><<<int((N + L2PW_WARPS - 1) / L2PW_WARPS), 32 * L2PW_WARPS, sh, st>>>(
+         P.tree, P.root, P.p, P.Lp, (const T*)P.local.ptr, (const V4*)P.tPos.ptr, (const int*)P.tIdx.ptr,
+         (const CurlEntry<T>*)P.curlTab.ptr, 2, (T*)P.outB.ptr, (T*)P.outA.ptr);
+      FMM_TRY(launched(P, "kL2PWarp", st));
+      return bemNearT<T>(P, st);
+   }
    if(split)
    {
       auto runL2P = [&](auto kernel, size_t sh) -> fmm_status {
@@ -1902,6 +1920,7 @@ fmm_status directT(Plan& P, double current, int want, cudaStream_t st)
    typedef typename Vec4<T>::type V4;
    constexpr int NT = 128;
    T scaleB = T(REF_MU0 / (4 * REF_PI) * current), scaleA = T(1.0 / (4 * REF_PI) * current);
+   if(P.bem) return bemDirectT<T>(P, st);
    int maxT = 0;
    for(int c = 0; c < P.nCoils; c++) maxT = std::max(maxT, P.tgtOff[c + 1] - P.tgtOff[c]);
    const int blocks = (maxT + NT - 1) / NT;
@@ -1941,7 +1960,8 @@ fmm_status directFp64Subset(Plan& P, double current, const double* tgtDev, int k
 // New strengths w J for the same source positions, in the tree's sorted order.
 template <class T>
 __global__ void kRegatherStrengths(const T* __restrict__ xyz, const T* __restrict__ w, const T* __restrict__ J,
-                                   const int* __restrict__ order, int64_t n, typename Vec4<T>::type* q)
+                                   const T* __restrict__ sigma, const int* __restrict__ order, int64_t n,
+                                   typename Vec4<T>::type* q)
 {
    int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
    if(i >= n) return;
@@ -1957,7 +1977,7 @@ __global__ void kRegatherStrengths(const T* __restrict__ xyz, const T* __restric
       jz = T(0);
    }
    const T ww = w[s];
-   q[i] = {ww * jx, ww * jy, ww * jz, T(0)};
+   q[i] = {ww * jx, ww * jy, ww * jz, sigma ? ww * sigma[s] : T(0)};
 }
 
 template <class T>
@@ -1974,6 +1994,7 @@ fmm_status regatherStrengthsT(Plan& P, cudaStream_t st)
    if(P.n == 0) return FMM_OK;
    kRegatherStrengths<T><<<int((P.n + 255) / 256), 256, 0, st>>>((const T*)P.srcXYZ, (const T*)P.srcW,
                                                                  (const T*)(P.hasJ ? P.srcJ : nullptr),
+                                                                 (const T*)(P.bem ? P.srcSigma : nullptr),
                                                                  (const int*)P.sIdx.ptr, P.n, (V4*)P.sQ.ptr);
    FMM_TRY(launched(P, "kRegatherStrengths", st));
    return FMM_OK;

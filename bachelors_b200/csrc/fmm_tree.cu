@@ -168,8 +168,8 @@ __global__ void kKeys(const T* __restrict__ xyz, int64_t n, const RootBox* __res
 
 template <class T>
 __global__ void kGatherSources(const T* __restrict__ xyz, const T* __restrict__ w, const T* __restrict__ J,
-                               const int* __restrict__ order, int64_t n, typename Vec4<T>::type* pos,
-                               typename Vec4<T>::type* q)
+                               const T* __restrict__ sigma, const int* __restrict__ order, int64_t n,
+                               typename Vec4<T>::type* pos, typename Vec4<T>::type* q)
 {
    int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
    if(i >= n) return;
@@ -187,7 +187,8 @@ __global__ void kGatherSources(const T* __restrict__ xyz, const T* __restrict__ 
    }
    T ww = w[s];
    pos[i] = {x, y, z, T(0)};
-   q[i] = {ww * jx, ww * jy, ww * jz, T(0)};
+   // the fourth lane carries w sigma for BEM sources (fmm_bem.cu), zero otherwise
+   q[i] = {ww * jx, ww * jy, ww * jz, sigma ? ww * sigma[s] : T(0)};
 }
 
 template <class T>
@@ -612,7 +613,8 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    if(n)
    {
       kGatherSources<T><<<(n + threads - 1) / threads, threads, 0, st>>>(
-         (const T*)P.srcXYZ, (const T*)P.srcW, (const T*)(P.hasJ ? P.srcJ : nullptr), si, n, (V4*)P.sPos.ptr,
+         (const T*)P.srcXYZ, (const T*)P.srcW, (const T*)(P.hasJ ? P.srcJ : nullptr),
+         (const T*)(P.bem ? P.srcSigma : nullptr), si, n, (V4*)P.sPos.ptr,
          (V4*)P.sQ.ptr);
       FMM_TRY(launched(P, "kGatherSources", st));
    }

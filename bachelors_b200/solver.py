@@ -147,6 +147,21 @@ class Plan:
         self._keep = [x, wb, jb]
         self.generation += 1
 
+    def set_bem_sources(self, xyz, w, B, normal):
+        """BEM sources (fmm_set_bem_sources): points, weights, field values and normals; the plan then
+        computes the reference's BEM integral (solve / direct / treecode with want=2 return it as A)."""
+        x = _Buffer(xyz, self.np_dtype, self.torch_dtype, (3,))
+        wb = _Buffer(w, self.np_dtype, self.torch_dtype, ())
+        bb = _Buffer(B, self.np_dtype, self.torch_dtype, (3,))
+        nb = _Buffer(normal, self.np_dtype, self.torch_dtype, (3,))
+        self.device_mode = x.device
+        self.n = x.n
+        _lib.check(self.lib.fmm_set_bem_sources(self.handle, ctypes.c_void_p(x.ptr), ctypes.c_void_p(wb.ptr),
+                                                ctypes.c_void_p(bb.ptr), ctypes.c_void_p(nb.ptr), x.n, int(x.device),
+                                                self._stream()))
+        self._keep = [x, wb, bb, nb]
+        self.generation += 1
+
     def set_targets(self, xyz):
         t = _Buffer(xyz, self.np_dtype, self.torch_dtype, (3,))
         self.device_mode = t.device
@@ -216,6 +231,20 @@ class Plan:
 
     def direct(self, current=1.0, want=1):
         return self._run(self.lib.fmm_direct, current, want)
+
+    def treecode(self, points, current=1.0, want=1, reference_near=False, fd_curl=False):
+        """Treecode point queries on this plan's source tree and multipoles (fmm_treecode; call build_tree
+        and upward first). reference_near / fd_curl reproduce the reference's dropped close leaves and its
+        central-difference curl. Returns (B, A) for `points` [M,3] (None where not wanted)."""
+        pb = _Buffer(points, self.np_dtype, self.torch_dtype, (3,))
+        if pb.device != self.device_mode:
+            raise ValueError("points must live where the plan's inputs live (host numpy or CUDA tensor)")
+        B = self._out(pb.n) if want & 1 else None
+        A = self._out(pb.n) if want & 2 else None
+        flags = (_lib.FMM_TREECODE_REFERENCE_NEAR if reference_near else 0) | (_lib.FMM_TREECODE_FD_CURL if fd_curl else 0)
+        _lib.check(self.lib.fmm_treecode(self.handle, ctypes.c_double(current), int(want), ctypes.c_void_p(pb.ptr), pb.n,
+                                         self._ptr(B), self._ptr(A), int(flags), int(self.device_mode), self._stream()))
+        return B, A
 
     def adjoint(self, g, current=1.0, want_dJ=True, want_dx=True):
         """Adjoint FMM: for g = dLoss/dB at the targets ([M,3]) returns (dLoss/dJ, dLoss/d(source
@@ -301,20 +330,31 @@ class Plan:
         return out
 
 
+def _set_quadratures(plan, quadratures, problem):
+    """Biot-Savart sources (xyz, w[, J]) or BEM sources (xyz, w, B, normal)."""
+    if problem == Problem.BEM:
+        xyz, w, B, normal = quadratures
+        plan.set_bem_sources(xyz, w, B, normal)
+    else:
+        xyz, w, J = (tuple(quadratures) + (None,))[:3]
+        plan.set_sources(xyz, w, J)
+
+
 class MultipoleSolver:
-    """Upward pass only (MultipoleSolver in the reference). Its calcA / calcB(current, point)
-    treecode evaluation is provided by FastMultipoleSolver with the points as targets."""
+    """Upward pass and treecode point queries (MultipoleSolver in the reference): calcA / calcB(current,
+    point) walk the source tree with the reference's acceptance test (fmm_treecode). Close leaves are
+    summed directly and B comes from the analytic curl unless reference_near / fd_curl are set, which
+    reproduce the reference's choices."""
 
     def __init__(self, quadratures, problem=Problem.BioSavartLaplace, quadratureOctreeLeafCapacity=1000, *,
                  order=10, precision="fp32", m2l="simt", m2l_truncate=False, device=0, root=None):
-        if Problem(problem) != Problem.BioSavartLaplace:
-            raise NotImplementedError("only Problem.BioSavartLaplace is supported")
         self.plan = Plan(order=order, leaf_capacity=quadratureOctreeLeafCapacity, precision=precision, m2l=m2l,
                          m2l_truncate=m2l_truncate, device=device, root=root)
-        xyz, w, J = (tuple(quadratures) + (None,))[:3]
-        self.plan.set_sources(xyz, w, J)
+        self.problem = Problem(problem)
+        _set_quadratures(self.plan, quadratures, self.problem)
         self._multipoles = False
         self.harmonicOrder = int(order)
+        self.treecode_flags = {"reference_near": False, "fd_curl": False}
 
     def calcMultipoleExpansionsAtLeaves(self):
         self.plan.build_tree()
@@ -325,18 +365,31 @@ class MultipoleSolver:
         if not self._multipoles:
             self.calcMultipoleExpansionsAtLeaves()
 
+    def _query(self, current, point, want):
+        if not self._multipoles:
+            raise RuntimeError("Multipoles are not ready!")
+        pts = point if _is_cuda_tensor(point) else np.asarray(point, dtype=self.plan.np_dtype).reshape(-1, 3)
+        out = self.plan.treecode(pts, current, want, **self.treecode_flags)[0 if want == 1 else 1]
+        return out[0] if not _is_cuda_tensor(point) and np.ndim(point) == 1 else out
+
+    def calcB(self, current, point):
+        """B at one point ([3]) or many ([M,3]) by the treecode."""
+        return self._query(current, point, 1)
+
+    def calcA(self, current, point):
+        return self._query(current, point, 2)
+
 
 class FastMultipoleSolver(MultipoleSolver):
     def __init__(self, quadratures, points, problem=Problem.BioSavartLaplace, quadratureOctreeLeafCapacity=1000,
                  calculationPointOctreeLeafCapacity=100, *, order=10, precision="fp32", m2l="simt",
                  m2l_truncate=False, device=0, root=None):
-        if Problem(problem) != Problem.BioSavartLaplace:
-            raise NotImplementedError("only Problem.BioSavartLaplace is supported")
         self.plan = Plan(order=order, leaf_capacity=quadratureOctreeLeafCapacity,
                          target_leaf_capacity=calculationPointOctreeLeafCapacity, precision=precision, m2l=m2l,
                          m2l_truncate=m2l_truncate, device=device, root=root)
-        xyz, w, J = (tuple(quadratures) + (None,))[:3]
-        self.plan.set_sources(xyz, w, J)
+        self.problem = Problem(problem)
+        _set_quadratures(self.plan, quadratures, self.problem)
+        xyz = quadratures[0]
         if points is xyz:
             self.plan.set_targets_to_sources()   # B at the quadrature points themselves
         else:
@@ -344,6 +397,7 @@ class FastMultipoleSolver(MultipoleSolver):
         self._multipoles = False
         self._locals = False
         self.harmonicOrder = int(order)
+        self.treecode_flags = {"reference_near": False, "fd_curl": False}
 
     def calcLocalMultipoleExpansions(self, algorithm=M2LAlg.ComplexTranslation, device=Device.GPU):
         if not self._multipoles:
@@ -355,13 +409,25 @@ class FastMultipoleSolver(MultipoleSolver):
         if not self._locals:
             raise RuntimeError("Local expansions are not ready!")
 
-    def calcB(self, current):
+    def calcB(self, current, point=None):
+        """calcB(current): B at the solver's points (FMM); calcB(current, point): the treecode."""
+        if point is not None:
+            return self._query(current, point, 1)
         self._ready()
         return self.plan.evaluate(current, 1)[0]
 
-    def calcA(self, current):
+    def calcA(self, current, point=None):
+        if point is not None:
+            return self._query(current, point, 2)
         self._ready()
         return self.plan.evaluate(current, 2)[1]
+
+    def calcBEM(self, current=1.0):
+        """The BEM integral at the points (FastMultipoleSolver::calcBEM: no current factor)."""
+        if self.problem != Problem.BEM:
+            raise ValueError("calcBEM needs Problem.BEM")
+        self._ready()
+        return self.plan.evaluate(1.0, 2)[1]
 
     def solve(self, current=1.0, want="B"):
         w = {"B": 1, "A": 2, "AB": 3}[want]

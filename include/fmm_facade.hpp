@@ -20,16 +20,22 @@
  *   - leaf capacities keep the reference's meaning "a box holding this many points splits": the plan's
  *     leaves hold at most capacity - 1 points;
  *   - MultipoleSolver::calcA / calcB(current, point) (the reference's single-tree treecode,
- *     multipole_solver.cpp:686-700) run one FMM solve for that point; evaluate many points through
- *     FastMultipoleSolver instead;
- *   - Problem::BEM is not supported (std::invalid_argument).
+ *     multipole_solver.cpp:686-700) run the device treecode (fmm_treecode) on the plan's tree and
+ *     multipoles: the reference's acceptance test, with close leaves summed directly and B from the analytic
+ *     curl (treecodeFlags = FMM_TREECODE_REFERENCE_NEAR | FMM_TREECODE_FD_CURL gives the reference's
+ *     choices); the root cube is the sources' bounding cube unless config() sets one (the reference's is
+ *     centre 0, half-width 3, and drops sources outside it);
+ *   - Problem::BEM takes BEMQuadrature sources (fmm_set_bem_sources); FastMultipoleSolver::calcBEM sums close
+ *     boxes directly (the reference drops close leaves) and the tree's root is a cube around the sources
+ *     (the reference's BEM root is the box of half-widths 1.1, 1.1, 1.6 at the origin);
  * The solvers keep references to the caller's vectors, as the reference does
  * (multipole_solver.cpp:27-32, fast_multipole_solver.hpp:16): they must outlive the solver. The
  * data is copied to the GPU when the first phase runs.
  *
  * Define FMM_FACADE_NO_GLOBAL_NAMES to keep everything inside namespace fmm (by default the
  * reference's global names Vector3, Quadrature, real, MultipoleSolver, FastMultipoleSolver,
- * Problem, M2MAlg, Device, M2LAlg are also declared at global scope).
+ * Problem, M2MAlg, Device, M2LAlg, BEMQuadrature and the Basic* solver templates are also declared at global
+ * scope).
  */
 #ifndef FMM_FACADE_HPP
 #define FMM_FACADE_HPP
@@ -98,6 +104,18 @@ struct Quadrature : public Vector3
    Quadrature(const Vector3& coordinates, real volume, real w) : Vector3(coordinates), weight(volume * w) {}
 };
 
+/* A surface quadrature of the BEM problem (bem_quadrature.hpp): point, weight, field value and normal. */
+struct BEMQuadrature : public Quadrature
+{
+   Vector3 B;
+   Vector3 normal;
+   BEMQuadrature() = default;
+   BEMQuadrature(const Vector3& coordinates, real area, real w, const Vector3& B_, const Vector3& normal_)
+      : Quadrature(coordinates, area, w), B(B_), normal(normal_)
+   {
+   }
+};
+
 enum class Problem { BioSavartLaplace = 0, BEM = 1 };
 enum class M2MAlg { NoTranslation = 0, ComplexTranslation, RealTranslation, Layers, Matrices };
 enum class Device { CPU = 0, GPU, Adaptive };
@@ -141,6 +159,28 @@ void packSources(const std::vector<Q>& q, std::vector<real>& xyz, std::vector<re
    }
 }
 
+/* BEM sources: only BEMQuadrature carries a field value and a normal. */
+inline void setBemSources(fmm_plan* plan, const std::vector<BEMQuadrature>& q)
+{
+   std::vector<real> xyz(3 * q.size()), w(q.size()), B(3 * q.size()), n(3 * q.size());
+   for(size_t i = 0; i < q.size(); i++)
+   {
+      for(int d = 0; d < 3; d++)
+      {
+         xyz[3 * i + d] = q[i][d];
+         B[3 * i + d] = q[i].B[d];
+         n[3 * i + d] = q[i].normal[d];
+      }
+      w[i] = q[i].weight;
+   }
+   check(fmm_set_bem_sources(plan, xyz.data(), w.data(), B.data(), n.data(), int64_t(q.size()), 0, nullptr));
+}
+template <class Q>
+void setBemSources(fmm_plan*, const std::vector<Q>&)
+{
+   throw std::invalid_argument("fmm facade: Problem::BEM needs BEMQuadrature sources");
+}
+
 template <class P>
 void packPoints(const P* p, size_t n, std::vector<real>& xyz)
 {
@@ -171,9 +211,11 @@ protected:
    bool _sourcesUploaded = false;
    bool _multipolesAtLeavesAreReady = false;
    bool _multipolesAreReady = false;
+   bool _upwardDone = false;   // the plan holds the tree and multipoles the treecode walks
 
 public:
    bool log = false;
+   int treecodeFlags = 0;      // fmm_treecode flags of calcA / calcB(current, point)
    const int harmonicOrder;
    const int harmonicLength;
    const size_t quadratureOctreeLeafCapacity;
@@ -183,7 +225,6 @@ public:
       : _quadratures(quadratures), _problem(problem), harmonicOrder(order),
         harmonicLength((order + 1) * (order + 1)), quadratureOctreeLeafCapacity(quadratureOctreeLeafCapacity_)
    {
-      if(problem != Problem::BioSavartLaplace) throw std::invalid_argument("fmm facade: only Problem::BioSavartLaplace");
       _plan.cfg.order = order;
       _plan.cfg.leaf_capacity = detail::leafCapacity(quadratureOctreeLeafCapacity_);
    }
@@ -203,7 +244,11 @@ public:
    }
 
    virtual PointT calcA(real current, const PointT& point) { return pointQuery(current, point, 2); }
-   virtual PointT calcB(real current, const PointT& point) { return pointQuery(current, point, 1); }
+   virtual PointT calcB(real current, const PointT& point)
+   {
+      if(_problem == Problem::BEM) throw std::invalid_argument("fmm facade: a BEM solver evaluates calcA");
+      return pointQuery(current, point, 1);
+   }
 
    fmm_stats stats()
    {
@@ -217,6 +262,11 @@ protected:
    {
       if(_sourcesUploaded) return;
       _sourcesUploaded = true;
+      if(_problem == Problem::BEM)
+      {
+         detail::setBemSources(_plan.get(), _quadratures);
+         return;
+      }
       std::vector<real> xyz, w;
       detail::packSources(_quadratures, xyz, w);
       check(fmm_set_sources(_plan.get(), xyz.data(), w.data(), nullptr, int64_t(_quadratures.size()), 0, nullptr));
@@ -225,12 +275,17 @@ protected:
    PointT pointQuery(real current, const PointT& point, int want)
    {
       if(!_multipolesAreReady) throw std::runtime_error("Multipoles are not ready!");
-      uploadSources();
+      if(!_upwardDone)
+      {
+         uploadSources();
+         check(fmm_build_tree(_plan.get(), nullptr));
+         check(fmm_upward(_plan.get(), nullptr));
+         _upwardDone = true;
+      }
       real xyz[3] = {point.x, point.y, point.z};
-      check(fmm_set_targets(_plan.get(), xyz, 1, 0, nullptr));
       real out[3];
-      check(fmm_solve(_plan.get(), double(current), want, want == 1 ? out : nullptr, want == 2 ? out : nullptr, 0,
-                      nullptr));
+      check(fmm_treecode(_plan.get(), double(current), want, xyz, 1, want == 1 ? out : nullptr,
+                         want == 2 ? out : nullptr, treecodeFlags, 0, nullptr));
       PointT r;
       r.x = out[0];
       r.y = out[1];
@@ -269,6 +324,7 @@ public:
       check(fmm_build_tree(this->_plan.get(), nullptr));
       check(fmm_upward(this->_plan.get(), nullptr));
       this->_multipolesAtLeavesAreReady = true;
+      this->_upwardDone = true;
    }
 
    void calcLocalMultipoleExpansions(M2LAlg, Device = Device::CPU)
@@ -282,6 +338,13 @@ public:
    using Base::calcB;
    virtual std::vector<std::pair<PointT, PointT>> calcA(real current) { return evaluate(current, 2); }
    virtual std::vector<std::pair<PointT, PointT>> calcB(real current) { return evaluate(current, 1); }
+   /* calcBEM(current) (fast_multipole_solver.cpp:233-250): the BEM integral at the points, no current factor */
+   virtual std::vector<std::pair<PointT, PointT>> calcBEM(real current)
+   {
+      if(this->_problem != Problem::BEM) throw std::invalid_argument("fmm facade: calcBEM needs Problem::BEM");
+      (void)current;
+      return evaluate(real(1), 2);
+   }
 
 private:
    void upload()
@@ -418,6 +481,9 @@ inline void translateAllCPUMatrix(std::vector<Complex>& result, const std::vecto
 }  // namespace kernels
 
 #ifndef FMM_FACADE_NO_GLOBAL_NAMES
+using fmm::BasicFastMultipoleSolver;
+using fmm::BasicMultipoleSolver;
+using fmm::BEMQuadrature;
 using fmm::FastMultipoleSolver;
 using fmm::M2LAlg;
 using fmm::M2MAlg;

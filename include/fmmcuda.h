@@ -105,6 +105,19 @@ fmm_status fmm_plan_destroy(fmm_plan* plan);
  * copied; the caller's buffers may be released after the call returns. */
 fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const void* J, int64_t n,
                            int on_device, void* stream);
+/* BEM sources (the reference's Problem::BEM, FMM/FMMGPU/multipole_solver_enums.hpp:26-30, BEMQuadrature
+ * bem_quadrature.hpp): points xyz[3n], weights w[n], field values B[3n] and surface normals normal[3n]. The
+ * plan then computes the reference's BEM integral (math::calcBEMIntegral, integration.cpp:191-215)
+ *   F(x) = 1/(4 PI) sum_q w_q [(B_q . n_q) d + d x (B_q x n_q)] / |d|^3,  d = q - x,
+ * by fmm_solve / fmm_evaluate (FastMultipoleSolver::calcBEM, fast_multipole_solver.cpp:233-250; the
+ * multipoles are those of math::calcBEMIntegralContribution, integration.cpp:295-353, from the analytic
+ * gradient of the regular harmonics; close boxes are summed directly) and fmm_direct, always with want = 2,
+ * the result in out_A and no current factor, as there; fmm_treecode (want = 2) scales it by `current` as
+ * MultipoleSolver::calcA does. Not available with fmm_adjoint, fmm_update_sources or batches.
+ * fmm_set_sources returns the plan to the Biot-Savart problem. */
+fmm_status fmm_set_bem_sources(fmm_plan* plan, const void* xyz, const void* w, const void* B, const void* normal,
+                               int64_t n, int on_device, void* stream);
+
 /* Targets xyz[3m] (FastMultipoleSolver's `points`, fast_multipole_solver.hpp:16). */
 fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_device, void* stream);
 /* Targets = the current source points, in source input order (no counterpart in the reference, whose
@@ -130,6 +143,22 @@ fmm_status fmm_evaluate(fmm_plan* plan, double current, int want, void* out_B, v
 /* All phases in order. */
 fmm_status fmm_solve(fmm_plan* plan, double current, int want, void* out_B, void* out_A, int on_device,
                      void* stream);
+
+/* Treecode point queries (MultipoleSolver::calcA / calcB(current, point), FMM/FMMGPU/multipole_solver.cpp:686-700,
+ * with QuadratureOctreeNode::calcA / calcRot, quadrature_octree.cpp:171-258): B and/or A at pts[3m] from the
+ * plan's source tree and multipoles (call fmm_build_tree and fmm_upward first; the plan's own targets play no
+ * part, and a plan without targets has the reference's source-only tree). For each point the tree is walked
+ * from the root: a box of half-diagonal r at distance d from the point contributes its multipole when
+ * 4 r^2 < d^2, otherwise its children do; a leaf that fails the test is summed directly, and B comes from the
+ * analytic gradient of the irregular harmonics. Flags reproduce the reference's choices instead:
+ * FMM_TREECODE_REFERENCE_NEAR drops such leaves (they contribute nothing there), FMM_TREECODE_FD_CURL takes B
+ * by central differences of A with step 1e-3. The reference's tree uses root centre 0 and half-width 3 and
+ * splits a box holding `cap` points: configure root_center / root_half_width and leaf_capacity = cap - 1.
+ * Outputs in point input order, the plan's element type; not available on a batched plan. */
+#define FMM_TREECODE_REFERENCE_NEAR 1
+#define FMM_TREECODE_FD_CURL 2
+fmm_status fmm_treecode(fmm_plan* plan, double current, int want, const void* pts, int64_t m, void* out_B, void* out_A,
+                        int flags, int on_device, void* stream);
 
 /* Direct O(N M) sums on the device in the plan's precision, over the plan's current
  * sources and targets (math::calcBioSavartLaplace, FMM/FMMGPU/integration.cpp:101-111). */

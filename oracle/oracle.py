@@ -136,70 +136,87 @@ REF_MU0 = 1.2566370614e-6   # the reference's math::MU0
 _OCTANTS = ((-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1), (-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1))
 
 
-def _tc_build(xyz, idx, c, h, cap):
+def _tc_build(xyz, idx, c, h, cap, float_centres=True):
     """Node of the reference's quadrature octree (quadrature_octree.cpp:23-97): a box with cap or more
-    points is split into 8 children whose centres and half-widths are computed in float; points are
-    assigned by the half-open box test (box.cpp:13-24), keeping their input order."""
+    points is split into 8 children whose centres and half-widths are computed in float (float_centres;
+    exact halving otherwise); points are assigned by the half-open box test (box.cpp:13-24), keeping their
+    input order."""
     node = {"c": c, "h": h, "idx": idx, "children": []}
     if len(idx) >= cap:
-        fc = np.float32(c)
-        fh = np.float32(h)
-        ch = (fh / np.float32(2)).astype(np.float64)
-        for sgn in _OCTANTS:
-            cc = np.array([fc[a] + np.float32(sgn[a]) * (fh[a] / np.float32(2)) for a in range(3)],
-                          dtype=np.float32).astype(np.float64)
+        if float_centres:
+            fc = np.float32(c)
+            fh = np.float32(h)
+            ch = (fh / np.float32(2)).astype(np.float64)
+            centres = [np.array([fc[a] + np.float32(sgn[a]) * (fh[a] / np.float32(2)) for a in range(3)],
+                                dtype=np.float32).astype(np.float64) for sgn in _OCTANTS]
+        else:
+            ch = h / 2
+            centres = [c + np.array(sgn, dtype=np.float64) * ch for sgn in _OCTANTS]
+        for cc in centres:
             p = xyz[idx]
             inside = np.all((cc - ch <= p) & (p < cc + ch), axis=1)
-            node["children"].append(_tc_build(xyz, idx[inside], cc, ch, cap))
+            node["children"].append(_tc_build(xyz, idx[inside], cc, ch, cap, float_centres))
         node["idx"] = idx[:0]
     return node
 
 
-def _tc_upward(node, p, xyz, w):
+def _tc_upward(node, p, xyz, w, J, compat):
     if len(node["idx"]) > 0:   # a leaf with points: P2M (integration.cpp:137-161)
-        node["M"] = p2m(p, xyz[node["idx"]], w[node["idx"]], None, node["c"], compat=True)
+        node["M"] = p2m(p, xyz[node["idx"]], w[node["idx"]], None if J is None else J[node["idx"]], node["c"],
+                        compat=compat)
         return
     node["M"] = np.zeros((nharm(p), 3))
     for ch in node["children"]:
-        _tc_upward(ch, p, xyz, w)
+        _tc_upward(ch, p, xyz, w, J, compat)
     for ch in node["children"]:   # non-empty leaves and subdivided nodes (quadrature_octree.cpp:116-135)
         if len(ch["idx"]) > 0 or ch["children"]:
-            node["M"] += m2m(p, ch["M"], ch["c"] - node["c"], compat=True)
+            node["M"] += m2m(p, ch["M"], ch["c"] - node["c"], compat=compat)
 
 
-def _tc_rot(node, p, x, eps):
+def _tc_rot(node, p, x, eps, compat):
     d2 = float(np.sum((x - node["c"]) ** 2))
     r2 = float(np.sum(node["h"] ** 2))
     if 4 * r2 < d2:
         v = x - node["c"]
-        hd = []
-        for a in range(3):
-            e = np.zeros(3)
-            e[a] = eps
-            hd.append(solid_harmonics(p, v + e, False, True) - solid_harmonics(p, v - e, False, True))
+        if eps is None:   # analytic gradient of the irregular harmonics
+            g = solid_harmonics_grad2(p, v, False, compat)
+            hd = [g[:, a] for a in range(3)]
+            scale = 1.0
+        else:
+            hd = []
+            for a in range(3):
+                e = np.zeros(3)
+                e[a] = eps
+                hd.append(solid_harmonics(p, v + e, False, compat) - solid_harmonics(p, v - e, False, compat))
+            scale = 1.0 / (2 * eps)
         M = node["M"]
         t = np.array([np.dot(M[:, 2], hd[1]) - np.dot(M[:, 1], hd[2]),
                       np.dot(M[:, 0], hd[2]) - np.dot(M[:, 2], hd[0]),
                       np.dot(M[:, 1], hd[0]) - np.dot(M[:, 0], hd[1])])
-        return t / (2 * eps)
+        return t * scale
     out = np.zeros(3)
     for ch in node["children"]:
-        out += _tc_rot(ch, p, x, eps)
+        out += _tc_rot(ch, p, x, eps, compat)
     return out
 
 
-def treecode_B(p, cap, xyz, w, pts, current=1.0, half=3.0, eps=1e-3):
+def treecode_B(p, cap, xyz, w, pts, current=1.0, half=3.0, eps=1e-3, compat=True, J=None):
     """B at pts by the reference's treecode, FP64 (root: centre 0, half-width `half`; points outside it
-    are not inserted). Returns [m, 3]."""
+    are not inserted). Returns [m, 3]. compat=True reproduces the reference (its harmonic conventions and
+    float box centres); compat=False keeps its tree rule, acceptance test, dropped close leaves and
+    central-difference curl but uses the standard harmonics and exact box centres, the definition the
+    device treecode's reference mode implements. J: current directions (None: the azimuthal direction).
+    eps=None takes the curl from the analytic gradient of the irregular harmonics instead."""
     xyz = _c64(xyz).reshape(-1, 3)
     w = _c64(w)
     pts = _c64(pts).reshape(-1, 3)
+    Jc = None if J is None else _c64(J).reshape(-1, 3)
     c0 = np.zeros(3)
     h0 = np.full(3, float(half))
     inside = np.all((c0 - h0 <= xyz) & (xyz < c0 + h0), axis=1)
-    root = _tc_build(xyz, np.nonzero(inside)[0], c0, h0, cap)
-    _tc_upward(root, p, xyz, w)
-    out = np.stack([_tc_rot(root, p, x, eps) for x in pts])
+    root = _tc_build(xyz, np.nonzero(inside)[0], c0, h0, cap, float_centres=compat)
+    _tc_upward(root, p, xyz, w, Jc, compat)
+    out = np.stack([_tc_rot(root, p, x, eps, compat) for x in pts])
     return out / (4.0 * REF_PI) * current * REF_MU0
 
 

@@ -4,8 +4,11 @@
 //   <dir>/points.bin  m x 3 reals
 //   <dir>/seam.bin    count, order, then count x L harmonics and count x L x 3 expansions (reals)
 // and writes <dir>/fmm_B.bin (m x 3), <dir>/direct_B.bin (first 4 points x 3), <dir>/seam_out.bin
-// (count x L x 3) and <dir>/matrix_out.bin (3 x count x L for b = the identity plus 1 on the
-// diagonal's neighbour). Exit status 0 only when every call and every call-order check behaved.
+// (count x L x 3), <dir>/matrix_out.bin (3 x count x L for b = the identity plus 1 on the
+// diagonal's neighbour), <dir>/tree_B.bin (MultipoleSolver::calcB(current, point), the treecode, at the
+// first 8 points x 3) and <dir>/bem.bin (a BEM FastMultipoleSolver's calcBEM at the points, sources
+// built from quads with field B = (1, 2, 3) and normal (0, 0, 1)). Exit status 0 only when every call
+// and every call-order check behaved.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -107,6 +110,38 @@ int main(int argc, char** argv)
    std::vector<real> flat;
    for(auto& v : prod) flat.insert(flat.end(), v.begin(), v.end());
    writeAll(dir + "/matrix_out.bin", flat.data(), flat.size());
+
+   // the reference's treecode point queries (multipole_solver.cpp:686-700)
+   MultipoleSolver tree(quads, Problem::BioSavartLaplace, 33, 10);
+   tree.calcMultipoleExpansionsAtLeaves();
+   tree.calclMultipoleExpansions(M2MAlg::Matrices, Device::GPU);
+   std::vector<real> TB;
+   for(size_t i = 0; i < 8 && i < points.size(); i++)
+   {
+      Vector3 b = tree.calcB(real(2), points[i]);
+      TB.push_back(b.x);
+      TB.push_back(b.y);
+      TB.push_back(b.z);
+   }
+   writeAll(dir + "/tree_B.bin", TB.data(), TB.size());
+
+   // the BEM problem (Problem::BEM, calcBEM)
+   std::vector<BEMQuadrature> bq(quads.size());
+   for(size_t i = 0; i < quads.size(); i++)
+      bq[i] = BEMQuadrature(quads[i], real(1), quads[i].weight, Vector3(1, 2, 3), Vector3(0, 0, 1));
+   BasicFastMultipoleSolver<BEMQuadrature> bem(bq, points, Problem::BEM, 33, 33, 10);
+   bem.calcMultipoleExpansionsAtLeaves();
+   bem.calclMultipoleExpansions(M2MAlg::Matrices, Device::GPU);
+   bem.calcLocalMultipoleExpansions(M2LAlg::ComplexTranslation, Device::GPU);
+   auto bres = bem.calcBEM(real(1));
+   std::vector<real> BF;
+   for(auto& r : bres)
+   {
+      BF.push_back(r.second.x);
+      BF.push_back(r.second.y);
+      BF.push_back(r.second.z);
+   }
+   writeAll(dir + "/bem.bin", BF.data(), BF.size());
 
    auto sum = kernels::addVectors({1, 2, 3}, {10, 20, 30});
    if(sum.size() != 3 || sum[2] != real(33)) return 5;

@@ -69,3 +69,20 @@ def test_facade_matches_python_mirror(tmp_path, double):
     ref = np.stack([O.translate_all_matrix(expn[:, :, c], bmat) for c in range(3)])
     assert np.linalg.norm(mat - ref) / np.linalg.norm(ref) < (1e-14 if double else 1e-6)
     plan.close()
+    # MultipoleSolver::calcB(current, point): the treecode on the source tree (standard mode), current 2
+    TB = np.fromfile(tmp_path / "tree_B.bin", dtype=dt).reshape(-1, 3)
+    tp = Plan(order=10, leaf_capacity=32, precision="fp64" if double else "fp32")
+    tp.set_sources(xyz.astype(dt), w.astype(dt), None)
+    tp.build_tree()
+    tp.upward()
+    Tref, _ = tp.treecode(pts[:8].astype(dt), 2.0, 1)
+    assert np.array_equal(TB, Tref)
+    Td = O.direct(xyz, w, None, pts[:8], current=2.0)
+    assert np.linalg.norm(TB - Td) / np.linalg.norm(Td) < 1e-4
+    tp.close()
+    # calcBEM: sources = the quadratures with B = (1, 2, 3) and normal = z
+    BF = np.fromfile(tmp_path / "bem.bin", dtype=dt).reshape(-1, 3)
+    Bq = np.tile([1.0, 2.0, 3.0], (len(w), 1))
+    Nq = np.tile([0.0, 0.0, 1.0], (len(w), 1))
+    Fd = O.bem_direct(xyz, w, Bq, Nq, pts)
+    assert np.linalg.norm(BF - Fd) / np.linalg.norm(Fd) < (1e-5 if double else 3e-5)
