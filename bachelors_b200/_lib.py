@@ -23,9 +23,9 @@ EXPORTS = [
     "fmm_set_targets_to_sources",
     "fmm_build_tree", "fmm_upward", "fmm_downward", "fmm_evaluate", "fmm_solve", "fmm_direct",
     "fmm_direct_fp64_subset", "fmm_treecode", "fmm_adjoint", "fmm_adjoint_direct", "fmm_autotune", "fmm_get_tuning",
-    "fmm_set_tuning", "fmm_batch_set_coils", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
+    "fmm_set_tuning", "fmm_batch_set_coils", "fmm_batch_partition", "fmm_update_sources", "fmm_graph_capture", "fmm_graph_launch",
     "fmm_set_wait_limit", "fmm_get_stats", "fmm_get_operator", "fmm_direct_B_noalloc", "fmm_translate_all", "fmm_translate_all_matrix",
-    "fmm_translate_all_matrix_complex", "fmm_add_vectors",
+    "fmm_translate_all_matrix_complex", "fmm_torus_quadratures", "fmm_add_vectors",
     "fmm_last_error_string", "fmm_version",
 ]
 
@@ -101,6 +101,7 @@ def load():
         "fmm_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(FmmTuning)]),
         "fmm_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(FmmTuning)]),
         "fmm_batch_set_coils": (ctypes.c_int, [vp, i64, vp, vp]),
+        "fmm_batch_partition": (ctypes.c_int, [i64, vp, vp, ctypes.c_int, vp]),
         "fmm_update_sources": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
         "fmm_graph_capture": (ctypes.c_int, [vp, ctypes.c_int, vp]),
         "fmm_graph_launch": (ctypes.c_int, [vp, dbl, vp, vp, ctypes.c_int, vp]),
@@ -113,6 +114,8 @@ def load():
                                                     vp]),
         "fmm_translate_all_matrix_complex": (ctypes.c_int, [vp, vp, vp, i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                             vp]),
+        "fmm_torus_quadratures": (ctypes.c_int, [dbl, dbl, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int,
+                                                 ctypes.c_int, vp, vp, ctypes.c_int, vp]),
         "fmm_add_vectors": (ctypes.c_int, [vp, vp, vp, i64]),
         "fmm_last_error_string": (ctypes.c_char_p, []),
         "fmm_version": (ctypes.c_char_p, []),

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfmmcuda.so")
 SOURCES = ["fmm_api.cu", "fmm_tree.cu", "fmm_kernels.cu", "fmm_m2l_tc.cu", "fmm_adjoint.cu", "fmm_noalloc.cu", "fmm_seam.cu",
-           "fmm_treecode.cu", "fmm_bem.cu"]
+           "fmm_treecode.cu", "fmm_bem.cu", "fmm_geometry.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -844,6 +844,32 @@ fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* sr
    return FMM_OK;
 }
 
+fmm_status fmm_batch_partition(int64_t ncoils, const int64_t* src_offsets, const int64_t* tgt_offsets, int nparts,
+                               int* part)
+{
+   if(ncoils < 0 || ncoils > FMM_MAX_COILS || nparts < 1)
+      return setError(FMM_E_INVALID, "fmm_batch_partition: %lld coils, %d parts", (long long)ncoils, nparts);
+   if(ncoils > 0 && (!src_offsets || !tgt_offsets || !part)) return setError(FMM_E_INVALID, "fmm_batch_partition: null argument");
+   std::vector<std::pair<int64_t, int64_t>> work(static_cast<size_t>(ncoils));   // (-work, coil): decreasing work, then coil
+   for(int64_t c = 0; c < ncoils; c++)
+   {
+      const int64_t ns = src_offsets[c + 1] - src_offsets[c], nt = tgt_offsets[c + 1] - tgt_offsets[c];
+      if(ns < 0 || nt < 0) return setError(FMM_E_INVALID, "fmm_batch_partition: offsets decrease at coil %lld", (long long)c);
+      work[size_t(c)] = {-(ns + nt), c};
+   }
+   std::sort(work.begin(), work.end());
+   std::vector<int64_t> load(static_cast<size_t>(nparts), 0);
+   for(const auto& wc : work)
+   {
+      int best = 0;
+      for(int q = 1; q < nparts; q++)
+         if(load[size_t(q)] < load[size_t(best)]) best = q;
+      part[wc.second] = best;
+      load[size_t(best)] -= wc.first;
+   }
+   return FMM_OK;
+}
+
 fmm_status fmm_update_sources(fmm_plan* plan, const void* w, const void* J, int on_device, void* stream)
 {
    if(!plan) return setError(FMM_E_INVALID, "null plan");

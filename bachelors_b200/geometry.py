@@ -169,3 +169,28 @@ def tetra_quadratures(tets, rule_x, rule_w):
         + (d - a)[:, None, :] * rx[None, :, 2:3]
     w = vol[:, None] * rw[None, :]
     return xyz.reshape(-1, 3), w.reshape(-1)
+
+
+def tetra_torus_quadratures_device(radius, section_width, n_length, n_width, n_height, rule_x, rule_w,
+                                   precision="fp64", device=0):
+    """hex_torus_tetrahedra + tetra_quadratures generated on the GPU (fmm_torus_quadratures): returns
+    (xyz [T K, 3], w [T K]) as CUDA tensors on `device`, tetrahedron-major, ready for Plan.set_sources."""
+    import ctypes
+    import torch
+    from . import _lib
+    rx = np.ascontiguousarray(np.asarray(rule_x, dtype=np.float64).reshape(-1, 3))
+    rw = np.ascontiguousarray(np.asarray(rule_w, dtype=np.float64).reshape(-1))
+    k = len(rw)
+    total = 5 * n_length * n_width * n_height * k
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    xyz = torch.empty((total, 3), dtype=dt, device=f"cuda:{device}")
+    w = torch.empty((total,), dtype=dt, device=f"cuda:{device}")
+    lib = _lib.load()
+    with torch.cuda.device(device):
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(lib.fmm_torus_quadratures(ctypes.c_double(radius), ctypes.c_double(section_width), int(n_length),
+                                             int(n_width), int(n_height), ctypes.c_void_p(rx.ctypes.data),
+                                             ctypes.c_void_p(rw.ctypes.data), k,
+                                             _lib.FMM_FP64 if precision == "fp64" else _lib.FMM_FP32,
+                                             ctypes.c_void_p(xyz.data_ptr()), ctypes.c_void_p(w.data_ptr()), 1, stream))
+    return xyz, w

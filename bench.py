@@ -309,9 +309,12 @@ def extra_batch(local, world, steps):
     # accuracy: 16 seeded targets per coil against the FP64 direct sum over that coil's sources
     rng = np.random.default_rng(20260004)
     pick = np.concatenate([rng.choice(np.arange(to[c], to[c + 1]), size=16, replace=False) for c in range(256)])
+    # the reference sum takes the solver's own FP32 inputs (rounded positions of coils ~17 units from the origin
+    # move by ~1e-6, which is 3e-4 of the point spacing of the densest coils: input rounding, not solver error)
+    r32 = lambda a: a.astype(np.float32).astype(np.float64)
     ref = Plan(order=1, leaf_capacity=1 << 30, precision="fp64", device=local)
-    ref.set_sources(xyz, w, J)
-    ref.set_targets(tgt[pick])
+    ref.set_sources(r32(xyz), r32(w), r32(J))
+    ref.set_targets(r32(tgt[pick]))
     ref.set_coils(so, np.arange(0, 16 * 257, 16))
     Bd, _ = ref.direct(1.0, 1)
     ref.close()
@@ -333,7 +336,8 @@ def extra_batch(local, world, steps):
            "rel_l2_vs_fp64_direct": err, "max_coil_rel_l2": max(per_coil),
            "max_coil_rms_err_over_field_scale": max(per_coil_b0), "field_scale_bar": 1e-4,
            "field_scale": "B0 = MU0 |J| a per coil (a = minor radius)",
-           "error_samples": "16 seeded targets per coil (4096) vs FP64 direct over the coil's sources",
+           "error_samples": "16 seeded targets per coil (4096) vs the FP64 direct sum over the coil's sources, both "
+                            "from the same FP32 inputs",
            "phases_ms": phases, "tree": _tree_stats(plan)}
     plan.close()
     return res
@@ -387,7 +391,34 @@ def extra_c5(local, world, steps):
     return res
 
 
-EXTRAS = {"c1": extra_c1, "c2": extra_c2, "batch": extra_batch, "c5": extra_c5}
+def extra_batch_sharded(local, world, steps):
+    """The 256-coil batch split over the ranks by whole coils (fmm_batch_partition), each rank solving its
+    shard with one batched plan and the fields gathered over NCCL into every rank (strong scaling: the same
+    batch whatever the rank count); time = the slowest rank's, CUDA events around solve + gather."""
+    import torch
+    from bachelors_b200 import geometry as G
+    from bachelors_b200.sharding import gather_fields, partition_coils, Shard, solve_shard_on_gpu
+    xyz, w, J, tgt, so, to = G.torus_batch(256, seed=20260004)
+    part = partition_coils(so, to, world)
+    rank = int(os.environ.get("RANK", "0"))
+    f32 = lambda a: a.astype(np.float32)
+    shard = Shard(f32(xyz), f32(w), f32(J), f32(tgt), so, to, part, rank)
+
+    def step():
+        B = solve_shard_on_gpu(shard, order=8, leaf_capacity=32, precision="fp32", m2l="bf16x3", device=local)
+        return gather_fields(shard, B, len(tgt), rank, world) if world > 1 else B
+    for _ in range(3):
+        step()
+    ms, B = _timed(step, steps, world)
+    work = np.bincount(part, weights=np.diff(so) + np.diff(to), minlength=world)
+    return {"workload": "the 256-coil batch (see batch) split by whole coils over the ranks, fields gathered to "
+                        "every rank", "value": len(tgt) / (ms / 1000), "unit": UNIT, "ms_per_step": ms,
+            "steps": steps, "scaling": "strong", "coils_per_rank": np.bincount(part, minlength=world).tolist(),
+            "work_imbalance": float(work.max() / work.mean()),
+            "note": "includes plan creation and tree build per step (each rank's shard is solved from its points)"}
+
+
+EXTRAS = {"c1": extra_c1, "c2": extra_c2, "batch": extra_batch, "c5": extra_c5, "batch_sharded": extra_batch_sharded}
 
 
 def count_launches(plan):
@@ -631,6 +662,8 @@ def main():
         s.plan.close()
 
     extras = [e for e in args.extra.split(",") if e]
+    if world > 1 and extras and "batch_sharded" not in extras:
+        extras.append("batch_sharded")   # the one workload that shards across ranks
     if extras:
         line["workloads"] = {}
         for e in extras:

@@ -198,6 +198,16 @@ fmm_status fmm_adjoint_direct(fmm_plan* plan, double current, const void* dL_dB,
 #define FMM_MAX_COILS 65536
 fmm_status fmm_batch_set_coils(fmm_plan* plan, int64_t ncoils, const int64_t* src_offsets, const int64_t* tgt_offsets);
 
+/* Sharding a batch of coils over ranks (no counterpart in the reference, which runs on one device): assigns
+ * each of the ncoils coils (offsets as for fmm_batch_set_coils) to one of nparts parts so that the parts'
+ * work (sources + targets of their coils) is balanced: coils by decreasing work, each to the least-loaded
+ * part (ties to the lower part). Host only and deterministic, so every rank computes the same assignment;
+ * each rank then builds a batched plan of its part's coils. No data path crosses ranks except the
+ * gathering of the results, which is the caller's (bachelors_b200/sharding.py does it with
+ * torch.distributed). part[c] receives the part of coil c. */
+fmm_status fmm_batch_partition(int64_t ncoils, const int64_t* src_offsets, const int64_t* tgt_offsets, int nparts,
+                               int* part);
+
 /* Tile choices of the kernels (no counterpart in the reference, whose kernels have fixed shapes).
  * Every choice computes the same result up to rounding; they differ in speed with the order, the
  * leaf sizes and the point distribution. */
@@ -289,6 +299,20 @@ fmm_status fmm_translate_all_matrix(void* result, const void* a, const void* b, 
  * computes what its CPU twin computes (math::multMatricesAsVectors, math.hpp:84-105). */
 fmm_status fmm_translate_all_matrix_complex(void* result, const void* a, const void* b, int64_t count, int order,
                                             int precision, int on_device, void* stream);
+
+/* Quadrature sources from the reference's tetrahedral torus, generated on the current device (the reference
+ * builds them on the host: Torus::buildHexahedra and the split of each hexahedron into five tetrahedra,
+ * FMM/FMMGPU/torus.cpp:52-117, then math::tetrahedraToQuadratures, integration.cpp:34-42,163-187): a torus of
+ * square cross-section (side section_width, centre line of radius `radius`, axis z) cut into
+ * n_length x n_width x n_height hexahedra, five tetrahedra each, and the basis rule rule_x[3k] (points on the
+ * unit tetrahedron), rule_w[k] (k <= 64; the reference reads its Keast rule from files,
+ * basis_quadratures.cpp:12-101) mapped into every tetrahedron: x = a + (b - a) u + (c - a) v + (d - a) w,
+ * weight = volume x w_i. Outputs xyz[3 T k] and w[T k], T = 5 n_length n_width n_height, tetrahedron-major, in
+ * `precision` (FMM_FP32 or FMM_FP64); device pointers with on_device != 0 (the call only queues work on
+ * `stream`: pass them to fmm_set_sources with on_device = 1), host memory otherwise. */
+fmm_status fmm_torus_quadratures(double radius, double section_width, int n_length, int n_width, int n_height,
+                                 const double* rule_x, const double* rule_w, int k, int precision, void* xyz, void* w,
+                                 int on_device, void* stream);
 
 /* kernels::addVectors (FMMCUDADLL/kernel_callers.hpp:7-9): c = a + b for host arrays of n floats. */
 fmm_status fmm_add_vectors(const float* a, const float* b, float* c, int64_t n);

@@ -165,6 +165,8 @@ def test_batch_accuracy_against_each_coils_field_scale():
     MU0 = 1.2566370614e-6
     xyz, w, J, tgt, so, to, prm = G.torus_batch(24, seed=20260014, count_range=(2 ** 11, 2 ** 14),
                                                 targets_per_coil=2 ** 11, params=True)
+    # the reference sum takes the solver's FP32 inputs (positions rounded to FP32 are the solver's input)
+    xyz, w, J, tgt = (a.astype(np.float32).astype(np.float64) for a in (xyz, w, J, tgt))
     plan = Plan(order=8, leaf_capacity=32, precision="fp32", m2l="bf16x3")
     plan.set_sources(xyz.astype(np.float32), w.astype(np.float32), J.astype(np.float32))
     plan.set_targets(tgt.astype(np.float32))

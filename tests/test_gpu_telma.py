@@ -25,3 +25,33 @@ def test_telma_points(precision, kind, tol):
     ref = g["direct_B_current5"]
     assert np.linalg.norm(B - ref) / np.linalg.norm(ref) < tol
     plan.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-14), ("fp32", 1e-6)])
+def test_device_generated_torus_matches_host_generator(precision, tol):
+    """fmm_torus_quadratures builds the same Keast torus on the GPU as the host generator (itself equal to
+    the reference's quadratures, tests/test_oracle_telma.py), and the solver takes it straight from device
+    memory: the Telma-point field equals the solve from host inputs."""
+    g = dict(np.load(GOLDEN))
+    hx, hw = G.tetra_quadratures(G.hex_torus_tetrahedra(2.0, 0.2, 20, 4, 4), g["rule_x"], g["rule_w"])
+    dx, dw = G.tetra_torus_quadratures_device(2.0, 0.2, 20, 4, 4, g["rule_x"], g["rule_w"], precision)
+    assert dx.shape == hx.shape and dw.shape == hw.shape
+    ex = np.abs(dx.cpu().numpy() - hx).max() / np.abs(hx).max()
+    ew = np.abs(dw.cpu().numpy() - hw).max() / np.abs(hw).max()
+    assert ex < tol and ew < tol
+    import torch
+    dt = np.float64 if precision == "fp64" else np.float32
+    plan = Plan(order=12, leaf_capacity=32, precision=precision)
+    plan.set_sources(dx, dw, None)
+    plan.set_targets(torch.tensor(g["telma_points"].astype(dt), device="cuda"))
+    B, _ = plan.direct(5.0, 1)
+    ref = g["direct_B_current5"]
+    assert np.linalg.norm(B.cpu().numpy() - ref) / np.linalg.norm(ref) < (1e-13 if precision == "fp64" else 1e-5)
+    plan.close()
+    # a finer mesh than the reference's (20 x 4 x 4): 16 times the tetrahedra, all on the device
+    fx, fw = G.tetra_torus_quadratures_device(2.0, 0.2, 80, 8, 8, g["rule_x"], g["rule_w"], precision)
+    assert fx.shape[0] == 80 * 8 * 8 * 5 * len(g["rule_w"])
+    vol = 2 * np.pi * 2.0 * 0.2 * 0.2   # the square-section torus's volume; the polygonal mesh is slightly smaller
+    assert abs(fw.sum().item() / vol - 1) < 2e-3
+    with pytest.raises(Exception):
+        G.tetra_torus_quadratures_device(2.0, 0.2, 20, 4, 4, np.zeros((65, 3)), np.zeros(65), precision)
