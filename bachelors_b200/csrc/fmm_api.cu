@@ -105,6 +105,8 @@ fmm_status Plan::init(const fmm_config& c)
    if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(3, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
    if(const char* e = getenv("FMM_L2P_SPLIT")) l2pSplit = atoi(e) != 0;
+   if(const char* e = getenv("FMM_SIMT_TILED")) simtTiled = std::min(2, std::max(0, atoi(e)));
+   if(const char* e = getenv("FMM_SIMT_KC")) simtKc = atoi(e) == 32 ? 32 : 16;
    if(const char* e = getenv("FMM_TC_TRANSLATE")) tcTranslate = atoi(e) & 3;
    if(const char* e = getenv("FMM_TC_TRDRAIN")) tcTrDrainItems = std::max(0, atoi(e));
    if(const char* e = getenv("FMM_L2L_CHILD")) l2lChildMajor = atoi(e) != 0;

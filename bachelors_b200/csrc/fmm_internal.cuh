@@ -217,6 +217,8 @@ struct Plan
    int tcDrainMode = 3;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1,
                                          // 3: as 2 with 32 more columns in the drain threads' registers
    int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length
+   int simtKc = 16;                      // its K chunk (16 or 32)
+   int simtTiled = 1;                    // FP32 CUDA-core M2L: register-tiled kernel (0: the row-broadcast form)
    int l2pSplit = 1;                     // 1: L2P in kL2PWarp, then the near field; 0: both in kL2PNear
    int nearTile = 256;                   // near-field source tile, points (128 or 256)
    int p2mChunk = 0;                     // P2M: 0 one warp per leaf; 16 or 32: one block per leaf, that many

@@ -1050,6 +1050,181 @@ __global__ void __launch_bounds__(256) kM2LSimt(const int* __restrict__ targets,
 }
 
 // ====================================================================================
+// M2L on the CUDA cores in FP32, register-tiled (the plain FP32 form of FP32 plans). The same GEMM
+// sum as kM2LTc: a tile of 42 target boxes = 126 rows (box, component) of a 128-row block, and for each
+// offset present in the tile and each 16-wide K chunk C[128 x 160] += A_o[128 x 16] T_o[16 x 160], with
+// C the block's 160 output columns (two column blocks cover the 304 of p = 16; the second skips the K
+// chunks whose degree cutoff ends below its first column). Thread (ty, tx) of 256 owns rows 8 ty .. + 7
+// and the column pairs 2 tx + 32 j (j < 5): per K element it reads its 8 rows as two 16-byte loads from a
+// transposed copy of A and its 10 columns as five 8-byte loads, for 80 FMAs. A (gathered source rows)
+// and the operator slice arrive by cp.async, double-buffered.
+// ====================================================================================
+constexpr int ST_TT = 42, ST_ROWS = 128, ST_CB = 160, ST_TPAD = ST_ROWS + 4;
+
+template <int KC>
+constexpr size_t simtTiledSmem()
+{
+   return sizeof(float) * (2 * ST_ROWS * KC + KC * ST_TPAD + 2 * KC * ST_CB);
+}
+
+template <int MINB, int ST_KC>
+__global__ void __launch_bounds__(256, MINB) kM2LSimtTiled(const int* __restrict__ targets, int nTargets,
+                                                        const int* __restrict__ vtab, int L, int Lp, int nChunks,
+                                                        const SimtCols cols, const float* __restrict__ opw,
+                                                        const float* __restrict__ M, float* __restrict__ Lc)
+{
+   extern __shared__ __align__(16) float smf[];
+   // gathered rows, row-major (cp.async target) [2][ROWS][KC]; the current item's rows, K-major [KC][TPAD];
+   // the operator slice [2][KC][CB]
+   float (*As)[ST_ROWS][ST_KC] = reinterpret_cast<float (*)[ST_ROWS][ST_KC]>(smf);
+   float (*At)[ST_TPAD] = reinterpret_cast<float (*)[ST_TPAD]>(smf + 2 * ST_ROWS * ST_KC);
+   float (*Bs)[ST_KC][ST_CB] = reinterpret_cast<float (*)[ST_KC][ST_CB]>(smf + 2 * ST_ROWS * ST_KC + ST_KC * ST_TPAD);
+   __shared__ int tileNode[ST_TT];
+   __shared__ uint32_t present[10];
+   __shared__ int offs[316];
+   __shared__ int nOffS;
+   __shared__ int chunkList[32], nChunkS;
+   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+   const int first = blockIdx.x * ST_TT;
+   const int cb = blockIdx.y, col0 = cb * ST_CB;
+   if(tid < ST_TT) tileNode[tid] = first + tid < nTargets ? targets[first + tid] : -1;
+   if(tid < 10) present[tid] = 0;
+   __syncthreads();
+   for(int e = tid; e < ST_TT * 316; e += 256)
+   {
+      const int t = tileNode[e / 316], o = e % 316;
+      if(t >= 0 && vtab[int64_t(t) * 316 + o] >= 0) atomicOr(&present[o >> 5], 1u << (o & 31));
+   }
+   __syncthreads();
+   if(tid == 0)
+   {
+      int k = 0;
+      for(int o = 0; o < 316; o++)
+         if(present[o >> 5] & (1u << (o & 31))) offs[k++] = o;
+      nOffS = k;
+      // the K chunks that reach this column block (the degree cutoff narrows later chunks)
+      int nc = 0;
+      for(int c = 0; c < nChunks; c++)
+         if(cols.n[c] > col0) chunkList[nc++] = c;
+      nChunkS = nc;
+   }
+   __syncthreads();
+   const int nCh = nChunkS, nOff = nOffS, nItems = nOff * nCh;
+   // A: 128 rows x KC floats in 16-byte chunks; thread tid copies chunks (tid & 3) + 4 i of rows tid >> 2
+   // and (tid >> 2) + 64 for every item, so it keeps those rows' source boxes for the current offset and
+   // loads the next offset's one offset ahead (the V table read is off the copies' critical path)
+   const int rA = tid >> 2, qA = tid & 3;
+   int tA[2];
+   for(int h = 0; h < 2; h++)
+   {
+      const int r = rA + 64 * h;
+      tA[h] = r < 3 * ST_TT ? tileNode[r / 3] : -1;
+   }
+   int srcCur[2] = {-1, -1}, srcNxt[2] = {-1, -1};
+   int oiCur = -1;
+   auto loadSrc = [&](int oi, int* out) {
+      const int o = offs[oi];
+      for(int h = 0; h < 2; h++) out[h] = tA[h] >= 0 ? vtab[int64_t(tA[h]) * 316 + o] : -1;
+   };
+   auto issue = [&](int it, int b) {
+      const int oi = it / nCh;
+      const int o = offs[oi], c = chunkList[it - oi * nCh];
+      const int k0 = c * ST_KC;
+      if(oi != oiCur)
+      {
+         if(oi == oiCur + 1 && oiCur >= 0) { srcCur[0] = srcNxt[0]; srcCur[1] = srcNxt[1]; }
+         else loadSrc(oi, srcCur);
+         oiCur = oi;
+         if(oi + 1 < nOff) loadSrc(oi + 1, srcNxt);
+      }
+      for(int h = 0; h < 2; h++)
+#pragma unroll
+         for(int i = 0; i < ST_KC / 16; i++)
+         {
+            const int r = rA + 64 * h, src = srcCur[h];
+            const int q = qA + 4 * i, k = k0 + 4 * q;
+            const bool in = src >= 0 && k < Lp;
+            const float* g = M + (int64_t(in ? src : 0) * 3 + r % 3) * Lp + (in ? k : 0);
+            cpAsync16Simt(&As[b][r][4 * q], g, in ? 16u : 0u);
+         }
+      // B: 16 K rows x 160 columns = 640 chunks
+      const float* op = opw + int64_t(o) * L * Lp;
+      const int nCol = cols.n[c];
+      for(int e = tid; e < ST_KC * (ST_CB / 4); e += 256)
+      {
+         const int kk = e / (ST_CB / 4), q = e % (ST_CB / 4);
+         const int col = col0 + 4 * q, k = k0 + kk;
+         const bool in = k < L && col < nCol;
+         cpAsync16Simt(&Bs[b][kk][4 * q], op + (in ? int64_t(k) * Lp + col : 0), in ? 16u : 0u);
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+   };
+   float acc[8][10];
+#pragma unroll
+   for(int r = 0; r < 8; r++)
+#pragma unroll
+      for(int n = 0; n < 10; n++) acc[r][n] = 0.f;
+   if(nItems > 0) issue(0, 0);
+   for(int it = 0; it < nItems; it++)
+   {
+      const int b = it & 1;
+      if(it + 1 < nItems)
+      {
+         issue(it + 1, b ^ 1);
+         asm volatile("cp.async.wait_group 1;" ::: "memory");
+      }
+      else
+         asm volatile("cp.async.wait_group 0;" ::: "memory");
+      __syncthreads();
+      // transpose this item's rows into At[k][row]
+#pragma unroll
+      for(int q = 0; q < (ST_ROWS * ST_KC) / 256; q++)
+      {
+         const int e = tid + 256 * q;
+         const int r = e / ST_KC, k = e % ST_KC;
+         At[k][r] = As[b][r][k];
+      }
+      __syncthreads();
+#pragma unroll 4
+      for(int k = 0; k < ST_KC; k++)
+      {
+         const float4 a0 = *reinterpret_cast<const float4*>(&At[k][8 * ty]);
+         const float4 a1 = *reinterpret_cast<const float4*>(&At[k][8 * ty + 4]);
+         const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+         float bv[10];
+#pragma unroll
+         for(int j = 0; j < 5; j++)
+         {
+            const float2 v = *reinterpret_cast<const float2*>(&Bs[b][k][2 * tx + 32 * j]);
+            bv[2 * j] = v.x;
+            bv[2 * j + 1] = v.y;
+         }
+#pragma unroll
+         for(int r = 0; r < 8; r++)
+#pragma unroll
+            for(int n = 0; n < 10; n++) acc[r][n] = fmaf(a[r], bv[n], acc[r][n]);
+      }
+      __syncthreads();
+   }
+#pragma unroll
+   for(int r = 0; r < 8; r++)
+   {
+      const int row = 8 * ty + r;
+      if(row >= 3 * ST_TT) continue;
+      const int node = tileNode[row / 3];
+      if(node < 0) continue;
+      float* out = Lc + (int64_t(node) * 3 + row % 3) * Lp;
+#pragma unroll
+      for(int j = 0; j < 5; j++)
+      {
+         const int col = col0 + 2 * tx + 32 * j;
+         if(col < Lp) out[col] = col < L ? acc[r][2 * j] : 0.f;
+         if(col + 1 < Lp) out[col + 1] = col + 1 < L ? acc[r][2 * j + 1] : 0.f;
+      }
+   }
+}
+
+// ====================================================================================
 // L2P + near field: one block per target leaf. The local expansion is turned into the
 // expansion of B = curl A (order p - 1) in shared memory, evaluated per target by the
 // harmonic recurrence, then the direct sum over the leaf's source list is added.
@@ -1790,6 +1965,33 @@ fmm_status m2lSimt(Plan& P, cudaStream_t st)
       while((lmin + 1) * (lmin + 1) <= k) lmin++;
       const int n = cut - lmin >= 0 ? std::min(L, (cut - lmin + 1) * (cut - lmin + 1)) : 0;
       cols.n[g] = std::min(Lp, (n + 3) / 4 * 4);
+   }
+   if(sizeof(T) == 4 && P.simtTiled)
+   {
+      // FP32: the register-tiled kernel, K chunks of 16 (or 32) with the same degree cutoff
+      const int ST_KC = P.simtKc;
+      SimtCols c16{};
+      const int n16 = (L + ST_KC - 1) / ST_KC;
+      if(n16 > 32) return setError(FMM_E_INVALID, "CUDA-core M2L supports p <= 16");
+      for(int g = 0; g < n16; g++)
+      {
+         const int k = ST_KC * g;
+         int lmin = 0;
+         while((lmin + 1) * (lmin + 1) <= k) lmin++;
+         const int n = cut - lmin >= 0 ? std::min(L, (cut - lmin + 1) * (cut - lmin + 1)) : 0;
+         c16.n[g] = std::min(Lp, (n + 3) / 4 * 4);
+      }
+      const dim3 grid((count + ST_TT - 1) / ST_TT, (Lp + ST_CB - 1) / ST_CB);
+      // two blocks per SM (registers capped at 128) or one with all the registers it wants
+      auto kern = P.simtTiled == 2 ? (ST_KC == 32 ? kM2LSimtTiled<1, 32> : kM2LSimtTiled<1, 16>)
+                                   : (ST_KC == 32 ? kM2LSimtTiled<2, 32> : kM2LSimtTiled<2, 16>);
+      const size_t smemT = ST_KC == 32 ? simtTiledSmem<32>() : simtTiledSmem<16>();
+      FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemT)));
+      kern<<<grid, 256, smemT, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, L, Lp, n16, c16,
+                                     (const float*)P.opM2Lw.ptr, (const float*)P.mult.ptr, (float*)P.local.ptr);
+      FMM_TRY(launched(P, "kM2LSimtTiled", st));
+      FMM_CHECK_LAUNCH();
+      return FMM_OK;
    }
    const size_t smem = sizeof(T) * 2 * (size_t(8 * RPT) * KC + size_t(KC) * 32 * SM_NC);
    FMM_CUDA(cudaFuncSetAttribute(kM2LSimt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
