@@ -42,8 +42,9 @@ METRIC = "B evals/s (N=2^24, p=16) split-BF16 vs FP32 FMM at rel err<=1e-6; adjo
 UNIT = "target-evals/s"
 SEED = 20260002
 # DRAM bytes (read + write) per M2L pair of the tensor-core M2L, from an ncu capture of the
-# 128 x 32 x 64 torus at p = 16 (2.129 GB read + 0.189 GB written for 1,271,544 pairs)
-M2L_DRAM_BYTES_PER_PAIR = 2.318e9 / 1271544
+# 128 x 32 x 64 torus at p = 16 (676.9 MB read + 77.4 MB written for 1,271,544 pairs;
+# profiles/m2l_tc_bf16x3_torus2e18_p16.md)
+M2L_DRAM_BYTES_PER_PAIR = 754.32e6 / 1271544
 # bounded CPU samples of the same workload family (torus points, targets = sources): 32 x 8 x 8 = 2,048 for
 # each step of the reference arm (25 steps stay within a few minutes), 32 x 8 x 16 = 4,096 for the main
 # line's cpu_baseline (~15 s)
@@ -529,6 +530,10 @@ def main():
     peak_src = "measured" if "bf16_tflops" in peaks else "fallback"
     bf16_peak = peaks.get("bf16_tflops", 1590.0)
     bf16_sustained = peaks.get("bf16_tflops_sustained", 1400.0)
+    if m2l == "simt":
+        # the CUDA-core form: its peak is the FP32 FMA rate (not measured by the driver; nominal)
+        peak_src = "nominal FP32 FMA (148 SMs x 128 lanes x 2 x max SM clock)"
+        bf16_peak = bf16_sustained = fp32_core_peak_tflops(peaks.get("sm_max_mhz", 1965.0))
     achieved = flops_m2l / (m2l_avg / 1000.0) / 1e12
 
     # accuracy against the FP64 direct sum on 4096 seeded targets
@@ -551,20 +556,21 @@ def main():
                    "m2l": m2l, "order": args.order, "leaf": args.leaf, "n_sources": n, "n_targets": n,
                    "l2_flush": "inputs larger than L2 (2^24 points)", "parallelism": f"replicas x{world}",
                    "measured_terms": terms},
-        "roofline": {"kernel": f"M2L ({m2l})", "bound": "tensor", "achieved": achieved, "peak": bf16_peak,
+        "roofline": {"kernel": f"M2L ({m2l})", "bound": "fp32" if m2l == "simt" else "tensor", "achieved": achieved,
+                     "peak": bf16_peak,
                      "unit": "TFLOP/s", "frac": achieved / bf16_peak,
                      "frac_sustained": achieved / bf16_sustained, "peak_sustained": bf16_sustained,
                      "traffic": M2L_DRAM_BYTES_PER_PAIR * st["v_pairs"] if m2l == "bf16x3" else None,
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the "
-                                       "kernel on the 128x32x64 torus (1.82 KB per M2L pair), scaled by the pairs "
+                                       "kernel on the 128x32x64 torus (593 B per M2L pair), scaled by the pairs "
                                        "of this launch",
                      "flops_per_launch": flops_m2l, "flops_per_pair": per_pair,
                      "dense_equiv_flops_per_launch": flops_dense,
                      "reference_truncation_flops_per_launch": flops_reftrunc,
                      "note": f"algorithmic FLOPs = V pairs x 3 components x 2 x the entries of the executed operator "
                              f"(l + lambda <= p + 8 = {cut}); dense_equiv counts (p+1)^4, reference_truncation "
-                             f"l + lambda <= p; peak = {peak_src} bf16 dense (MEASURED_PEAKS.json): burst for frac, "
-                             f"sustained for frac_sustained; achieved over the M2L phase time (CUDA events)"},
+                             f"l + lambda <= p; peak = {peak_src} (bf16: MEASURED_PEAKS.json dense, burst for frac, "
+                             f"sustained for frac_sustained); achieved over the M2L phase time (CUDA events)"},
         "clocks": clk,
         "tuning": tuning,
         "phases_ms": {k: st[k] for k in ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_near", "ms_total")},
