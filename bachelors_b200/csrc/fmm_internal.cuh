@@ -210,6 +210,7 @@ struct Plan
                                          // with twice the accumulations per offset, drains twice as often)
    int tcProf = 0;                       // FMM_TC_PROF=1: per-role cycle counts of the M2L launch to stderr
    DevBuf tcProfBuf;
+   int tcCorrLam = 5;                    // ... and only in K steps whose lowest input degree is <= this (-1: any)
    int tcAsyncArrive = 1;                // tensor-core pipelines: producers arrive through cp.async.mbarrier
                                          // (0: wait for their copies, then arrive; one item in flight)
    int tcCorrCut = -2;                   // tensor-core M2L: correction products only for l + lambda <= this
