@@ -213,6 +213,8 @@ struct Plan
    int tcCorrLam = 5;                    // ... and only in K steps whose lowest input degree is <= this (-1: any)
    int tcAsyncArrive = 1;                // tensor-core pipelines: producers arrive through cp.async.mbarrier
                                          // (0: wait for their copies, then arrive; one item in flight)
+   int tcPair = 1;                       // tensor-core M2L: K chunks without correction products travel
+                                         // up to NP per pipeline stage (0: one chunk per stage)
    int tcCorrCut = -2;                   // tensor-core M2L: correction products only for l + lambda <= this
                                          // (-1: every term the degree cutoff keeps; -2: 10)
    int tcDrainMode = 3;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1,

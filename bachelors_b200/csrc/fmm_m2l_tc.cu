@@ -356,10 +356,18 @@ __global__ void kPrepM2LImage(const double* __restrict__ op64, int nOps, int L, 
 // offset), so far beyond degree C the hi*hi product's 2^-9 relative rounding is below the result's
 // accuracy, and those terms need no correction passes.
 constexpr int MAXKSTEPS = 64;   // K steps of one row (38 at p = 16 with 8-element TF32 steps)
+constexpr int MAXITEMS = 16;    // pipeline items of one offset (K chunks: 10 at p = 16 with 32-wide chunks)
+// Pipeline items of one offset: item i carries K chunks first[i] .. first[i] + count[i] - 1. A chunk with
+// correction products travels alone, its NP pieces in the stage's NP slots; chunks without any (their
+// first, widest K step has none) travel up to NP per stage, chunk first + j's leading piece in slot j.
+// The chunks stay in increasing K order, so an accumulation still starts with chunk 0's full-width MMA.
 struct M2LCols
 {
    int n[MAXKSTEPS];    // output columns of the leading product (hi * hi)
    int nc[MAXKSTEPS];   // output columns of the correction products, <= n
+   int first[MAXITEMS];
+   int count[MAXITEMS];
+   int nItems;          // items per offset
 };
 
 template <int NP, bool TF32>
@@ -416,14 +424,14 @@ struct DrainSchedule
 };
 
 // Position in the pipeline kept by increments (no divisions in the loops): the stage s and the parity
-// of its current use, the K chunk c of the current offset and the offset's index oi.
+// of its current use, the item c of the current offset and the offset's index oi.
 struct PipeCursor
 {
    int s = 0, ph = 0, c = 0, oi = 0;
-   __device__ __forceinline__ void next(int NS, int nChunks)
+   __device__ __forceinline__ void next(int NS, int nPer)
    {
       if(++s == NS) { s = 0; ph ^= 1; }
-      if(++c == nChunks) { c = 0; ++oi; }
+      if(++c == nPer) { c = 0; ++oi; }
    }
 };
 
@@ -467,6 +475,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
    int* colTab = tileNode + 64;                                 // output columns per K step [MAXKSTEPS]
    int* corTab = colTab + MAXKSTEPS;                            // ... of the correction products [MAXKSTEPS]
+   int* itemTab = corTab + MAXKSTEPS;                           // per item: first chunk, chunks [2 MAXITEMS]
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
@@ -485,6 +494,12 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       {
          colTab[g] = cols.n[g];
          corTab[g] = cols.nc[g];
+      }
+#pragma unroll
+      for(int i = 0; i < MAXITEMS; i++)
+      {
+         itemTab[2 * i] = cols.first[i];
+         itemTab[2 * i + 1] = cols.count[i];
       }
    }
    if(tid == 0)
@@ -528,16 +543,17 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          if(present[o >> 5] & (1u << (o & 31))) itemOffset[k++] = o;
       }
       itemOffset[316] = k;
-      // work accounting: pipeline items (offset x K chunk) and tile-offset pairs
+      // work accounting: pipeline items and tile-offset pairs
       if(counters)
       {
-         atomicAdd(counters, (unsigned long long)(k * nChunks));
+         atomicAdd(counters, (unsigned long long)(k * cols.nItems));
          atomicAdd(counters + 1, (unsigned long long)k);
       }
    }
    __syncthreads();
    const int nOff = itemOffset[316];
-   const int nItems = nOff * nChunks;
+   const int nPer = cols.nItems;                       // items per offset
+   const int nItems = nOff * nPer;
    const uint32_t tmem = *tmemBase;
    if(prof && tid == 0)
    {
@@ -557,17 +573,19 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          DrainSchedule sched(nOff, drainEvery, drainFar);
          PipeCursor cur;
          int sinceDrain = 0;
-         for(int it = 0; it < nItems; it++, cur.next(NS, nChunks))
+         for(int it = 0; it < nItems; it++, cur.next(NS, nPer))
          {
             const int s = cur.s;
-            // this chunk's output widths per K step, read before the wait
-            int nColK[KCH / KS], nCorK[KCH / KS];
+            // the item's chunks and their output widths per K step, read before the wait
+            const int c0 = itemTab[2 * cur.c], m = itemTab[2 * cur.c + 1];
+            int nColK[NP][KCH / KS], nCorK[KCH / KS];
 #pragma unroll
-            for(int ks = 0; ks < KCH / KS; ks++)
-            {
-               nColK[ks] = colTab[cur.c * (KCH / KS) + ks];
-               nCorK[ks] = corTab[cur.c * (KCH / KS) + ks];
-            }
+            for(int j = 0; j < NP; j++)
+#pragma unroll
+               for(int ks = 0; ks < KCH / KS; ks++)
+                  nColK[j][ks] = j < m ? colTab[(c0 + j) * (KCH / KS) + ks] : 0;
+#pragma unroll
+            for(int ks = 0; ks < KCH / KS; ks++) nCorK[ks] = m == 1 ? corTab[c0 * (KCH / KS) + ks] : 0;
             long long t0 = prof ? clock64() : 0;
             if(!mbarWait(fullBar0 + 8 * s, cur.ph, err, abortFlag, waitNs)) break;
             long long t1 = prof ? clock64() : 0;
@@ -585,47 +603,51 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             fenceAfterSync();
             const uint32_t st = base + s * stageBytes;
             const uint32_t aSt = st, bSt = st + NP * aBytes;
-            // K steps of 16 that reach a coefficient < L (the last chunk is partly padding); chunks run
-            // in increasing K, so an accumulation always starts with a full-width MMA
-            const int cItem = cur.c;
-            const int kSteps = min(KCH / KS, (L - cItem * KCH + KS - 1) / KS);
-            // descriptors of the stage's pieces; an MMA's operand is the piece's descriptor plus its
+            // descriptors of the stage's slots; an MMA's operand is the slot's descriptor plus its
             // byte offset / 16 (the start-address field, bits 0-13, holds every address of the stage)
             const uint64_t dA = smemDescT<Lay>(aSt), dB = smemDescT<Lay>(bSt);
 #pragma unroll
-            for(int ks = 0; ks < KCH / KS; ks++)
+            for(int j = 0; j < NP; j++)
             {
-               if(ks >= kSteps) break;
-               const uint32_t koff = ks * 32;
-               // this K step's output columns in one MMA (<= 256) or two (256 + the rest); the
-               // correction products over the first nCor of them
-               const int nCol = nColK[ks];
-               if(nCol == 0) break;
-               const int nCor = nCorK[ks];
+               if(j >= m) break;
+               // K steps of 16 that reach a coefficient < L (the last chunk is partly padding)
+               const int kSteps = min(KCH / KS, (L - (c0 + j) * KCH + KS - 1) / KS);
 #pragma unroll
-               for(int pass = 0; pass < NPASS; pass++)
+               for(int ks = 0; ks < KCH / KS; ks++)
                {
-                  const int w = pass == 0 ? nCol : nCor;
-                  if(w == 0) break;
-                  const int nA = min(w, 256), nB = w - nA;
-                  const uint32_t idA = Lay::TF32 ? instrDescTf32(ROWS, nA) : instrDescBf16(ROWS, nA);
-                  const uint32_t idB = Lay::TF32 ? instrDescTf32(ROWS, nB > 0 ? nB : 16) : instrDescBf16(ROWS, nB > 0 ? nB : 16);
-                  const int pa = NP == 1 ? 0 : (NP == 2 ? PA2[pass] : PA[pass]);
-                  const int pb = NP == 1 ? 0 : (NP == 2 ? PB2[pass] : PB[pass]);
-                  const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
-                  const uint64_t db = dB + ((pb * bBytes + koff) >> 4);
-                  const uint32_t acc = firstMma ? 0u : 1u;
-                  if constexpr(Lay::TF32)
+                  if(ks >= kSteps) break;
+                  const uint32_t koff = ks * 32;
+                  // this K step's output columns in one MMA (<= 256) or two (256 + the rest); the
+                  // correction products over the first nCor of them (a chunk alone in its item: j = 0)
+                  const int nCol = nColK[j][ks];
+                  if(nCol == 0) break;
+                  const int nCor = nCorK[ks];
+#pragma unroll
+                  for(int pass = 0; pass < NPASS; pass++)
                   {
-                     mmaTf32(tmem, da, db, idA, acc);
-                     if(nB > 0) mmaTf32(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                     const int w = pass == 0 ? nCol : nCor;
+                     if(w == 0) break;
+                     const int nA = min(w, 256), nB = w - nA;
+                     const uint32_t idA = Lay::TF32 ? instrDescTf32(ROWS, nA) : instrDescBf16(ROWS, nA);
+                     const uint32_t idB = Lay::TF32 ? instrDescTf32(ROWS, nB > 0 ? nB : 16) : instrDescBf16(ROWS, nB > 0 ? nB : 16);
+                     // piece slots: pa, pb for a chunk alone, slot j (pass 0 only) for a shared stage
+                     const int pa = j + (NP == 1 ? 0 : (NP == 2 ? PA2[pass] : PA[pass]));
+                     const int pb = j + (NP == 1 ? 0 : (NP == 2 ? PB2[pass] : PB[pass]));
+                     const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
+                     const uint64_t db = dB + ((pb * bBytes + koff) >> 4);
+                     const uint32_t acc = firstMma ? 0u : 1u;
+                     if constexpr(Lay::TF32)
+                     {
+                        mmaTf32(tmem, da, db, idA, acc);
+                        if(nB > 0) mmaTf32(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                     }
+                     else
+                     {
+                        mmaBf16(tmem, da, db, idA, acc);
+                        if(nB > 0) mmaBf16(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                     }
+                     firstMma = false;
                   }
-                  else
-                  {
-                     mmaBf16(tmem, da, db, idA, acc);
-                     if(nB > 0) mmaBf16(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
-                  }
-                  firstMma = false;
                }
             }
             mmaCommit(emptyBar0 + 8 * s);
@@ -642,7 +664,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                if(drainNow) sinceDrain = 0;
             }
             else
-               drainNow = cur.c == nChunks - 1 && sched.after(cur.oi);
+               drainNow = cur.c == nPer - 1 && sched.after(cur.oi);
             {
                if(drainNow)
                {
@@ -678,25 +700,36 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          int issued = 0;
          long long twe = 0;
          PipeCursor cur;
-         for(int it = 0; it < nItems; it++, cur.next(NS, nChunks))
+         for(int it = 0; it < nItems; it++, cur.next(NS, nPer))
          {
             const int s = cur.s;
             const long long t0 = prof ? clock64() : 0;
             // the stage's previous use (parity ph ^ 1) must have been consumed
             if(it >= NS && !mbarWait(emptyBar0 + 8 * s, cur.ph ^ 1, err, abortFlag, waitNs)) break;
             if(prof) twe += clock64() - t0;
-            const int o = itemOffset[cur.oi], c = cur.c;
-            const uint8_t* src = img + (int64_t(o) * nChunks + c) * NP * bBytes;
+            const int o = itemOffset[cur.oi], c0 = itemTab[2 * cur.c], m = itemTab[2 * cur.c + 1];
             const uint32_t dst = base + s * stageBytes + NP * aBytes;
-            // only the operator rows (output columns) this chunk's widest K step uses: of the leading
-            // piece for the hi * hi product, of the others for the correction products
-            const uint32_t rowBytes = uint32_t(colTab[c * (KCH / KS)]) * Lay::RB;
-            const uint32_t corBytes = uint32_t(corTab[c * (KCH / KS)]) * Lay::RB;
-            mbarArriveExpectTx(opBar0 + 8 * s, rowBytes + (NP - 1) * corBytes);
-            bulkLoad(dst, src, rowBytes, opBar0 + 8 * s);
+            // only the operator rows (output columns) a chunk's widest K step uses: of the leading
+            // piece for the hi * hi product, of the others for the correction products. A chunk alone
+            // fills the slots with its pieces, chunks sharing the stage their leading pieces.
+            uint32_t bytes[NP];
+            uint32_t tx = 0;
 #pragma unroll
-            for(int j = 1; j < NP; j++)
-               if(corBytes) bulkLoad(dst + j * bBytes, src + j * bBytes, corBytes, opBar0 + 8 * s);
+            for(int j = 0; j < NP; j++)
+            {
+               const int g = (m == 1 ? c0 : c0 + j) * (KCH / KS);
+               bytes[j] = m == 1 ? uint32_t(j == 0 ? colTab[g] : corTab[g]) * Lay::RB
+                                 : (j < m ? uint32_t(colTab[g]) * Lay::RB : 0u);
+               tx += bytes[j];
+            }
+            mbarArriveExpectTx(opBar0 + 8 * s, tx);
+#pragma unroll
+            for(int j = 0; j < NP; j++)
+            {
+               const uint8_t* src = m == 1 ? img + ((int64_t(o) * nChunks + c0) * NP + j) * bBytes
+                                           : img + (int64_t(o) * nChunks + c0 + j) * NP * bBytes;
+               if(bytes[j]) bulkLoad(dst + j * bBytes, src, bytes[j], opBar0 + 8 * s);
+            }
             issued = it + 1;
          }
          // the copies in flight write this CTA's shared memory: wait for them before it can exit. A stage
@@ -880,7 +913,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       long long twp = 0;
       const long long tpl = prof ? clock64() : 0;
       PipeCursor cur;
-      for(int it = 0; it < nItems; it++, cur.next(NS, nChunks))
+      for(int it = 0; it < nItems; it++, cur.next(NS, nPer))
       {
          const int s = cur.s;
          const int oi = cur.oi, c = cur.c;
@@ -898,21 +931,25 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          if(it >= NS && !mbarWait(emptyBar0 + 8 * s, cur.ph ^ 1, err, abortFlag, waitNs)) break;
          if(prof) twp += clock64() - t0;
          const uint32_t aSt = base + s * stageBytes;
-         const int k0 = c * KCH + half * PER;
+         const int c0 = itemTab[2 * c], m = itemTab[2 * c + 1];
          const uint8_t* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp * Lay::ES;
-         // the pieces after the leading one feed only the correction products: none in this chunk when
-         // its first (widest) K step has none
-         const int npc = corTab[c * (KCH / Lay::KSTEP)] > 0 ? NP : 1;
+         // a chunk alone: its pieces into the slots, the ones after the leading piece only when its first
+         // (widest) K step has correction products; chunks sharing the stage: chunk c0 + j's leading
+         // piece into slot j
+         const int nSlots = m == 1 ? (corTab[c0 * (KCH / Lay::KSTEP)] > 0 ? NP : 1) : m;
 #pragma unroll
          for(int q = 0; q < PER / EPC; q++)
          {
-            const int k = k0 + EPC * q;
-            const uint32_t bytes = (src >= 0 && k < Lp) ? 16u : 0u;
             const uint32_t off = Lay::off(uint32_t(row), uint32_t(half * PER + EPC * q));
 #pragma unroll
             for(int j = 0; j < NP; j++)
-               if(j < npc)
-                  cpAsync16(aSt + j * aBytes + off, rowp + (int64_t(j) * Lp + (bytes ? k : 0)) * Lay::ES, bytes);
+            {
+               if(j >= nSlots) break;
+               const int k = (m == 1 ? c0 : c0 + j) * KCH + half * PER + EPC * q;
+               const int piece = m == 1 ? j : 0;
+               const uint32_t bytes = (src >= 0 && k < Lp) ? 16u : 0u;
+               cpAsync16(aSt + j * aBytes + off, rowp + (int64_t(piece) * Lp + (bytes ? k : 0)) * Lay::ES, bytes);
+            }
          }
          if(asyncArrive)
             // the barrier completes when every producer's copies of this item have landed, while the
@@ -923,7 +960,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             cpAsyncCommit();
             pending = s;
          }
-         if(c == nChunks - 1) src = srcNext;
+         if(c == nPer - 1) src = srcNext;
       }
       cpAsyncWaitAll();
       if(pending >= 0 && !*abortFlag)
@@ -949,6 +986,31 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
    }
    if(prof && tid == 0) atomicAdd(prof + 9, (unsigned long long)(clock64() - tStart));
+}
+
+// The pipeline items of one offset (M2LCols): a K chunk with correction products travels alone; with
+// share, runs of chunks without any travel up to NP per stage.
+static fmm_status planItems(M2LCols& cols, int nChunks, int stepsPerChunk, int NP, bool share)
+{
+   if(nChunks > MAXITEMS) return setError(FMM_E_INVALID, "tensor-core pipeline: %d K chunks exceed the item table", nChunks);
+   auto hiOnly = [&](int c) {
+      for(int ks = 0; ks < stepsPerChunk; ks++)
+         if(cols.nc[c * stepsPerChunk + ks] > 0) return false;
+      return true;
+   };
+   int n = 0;
+   for(int c = 0; c < nChunks;)
+   {
+      int m = 1;
+      if(share && hiOnly(c))
+         while(m < NP && c + m < nChunks && hiOnly(c + m)) m++;
+      cols.first[n] = c;
+      cols.count[n] = m;
+      n++;
+      c += m;
+   }
+   cols.nItems = n;
+   return FMM_OK;
 }
 
 template <int NP, class Lay>
@@ -999,8 +1061,9 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
       nc = std::min(Lp, (nc + 15) / 16 * 16);
       cols.nc[g] = corr < 0 ? cols.n[g] : std::min(cols.n[g], nc);
    }
+   FMM_TRY(planItems(cols, nChunks, Lay::KC / Lay::KSTEP, NP, P.tcPair != 0));
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS);
+   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS + 2 * MAXITEMS);
    const size_t budget = 232448;
    const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
@@ -1040,8 +1103,8 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
               "| producer: loop %.0f, wait stage %.0f | drain: loop %.0f, wait accumulator %.0f\n",
               blocks, it, h[9] / b, h[10] / b, h[3] / b, h[0] / b, h[1] / b, h[2] / b, h[4] / b, h[6] / b, h[5] / b,
               h[8] / b, h[7] / b);
-      fprintf(stderr, "kM2LTc profile, MMA thread cycles per item from the stage's arrival to its commit, by K chunk:");
-      for(int c = 0; c < std::min(nChunks, 6); c++) fprintf(stderr, " %.0f", h[16 + c] * double(nChunks) / double(h[11]));
+      fprintf(stderr, "kM2LTc profile, MMA thread cycles per item from the stage's arrival to its commit, by item:");
+      for(int c = 0; c < std::min(cols.nItems, 6); c++) fprintf(stderr, " %.0f", h[16 + c] * double(cols.nItems) / double(h[11]));
       fprintf(stderr, "\n");
    }
    // a timed-out wait raises the pipeline error word, which the calling phase reads once at its end
@@ -1079,8 +1142,10 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
    const int nSteps = nChunks * (Lay::KC / Lay::KSTEP);
    if(nSteps > MAXKSTEPS) return setError(FMM_E_INVALID, "tensor-core translation: %d K steps exceed the column table", nSteps);
    for(int g = 0; g < nSteps; g++) cols.n[g] = cols.nc[g] = Lay::KSTEP * g < L ? Lp : 0;
+   // every chunk alone in its stage: the drains every drainItems items need full-width chunks
+   FMM_TRY(planItems(cols, nChunks, Lay::KC / Lay::KSTEP, NP, false));
    const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS);
+   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS + 2 * MAXITEMS);
    const size_t budget = 232448;
    const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
    if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core translation: %zu-byte stages do not fit twice", stageBytes);
