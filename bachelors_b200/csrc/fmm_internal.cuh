@@ -211,8 +211,11 @@ struct Plan
    int tcProf = 0;                       // FMM_TC_PROF=1: per-role cycle counts of the M2L launch to stderr
    DevBuf tcProfBuf;
    int tcCorrLam = 5;                    // ... and only in K steps whose lowest input degree is <= this (-1: any)
-   int tcAsyncArrive = 1;                // tensor-core pipelines: producers arrive through cp.async.mbarrier
-                                         // (0: wait for their copies, then arrive; one item in flight)
+   int tcAsyncArrive = 0;                // tensor-core pipelines: 0: each producer waits for its copies, fences
+                                         // and arrives; 1: producers arrive through cp.async.mbarrier and
+                                         // the MMA thread fences (up to NS items in flight, but the MMA
+                                         // thread loses ~400-600 cycles per item after such a barrier:
+                                         // M2L 159 ms against 137 ms at 2^24)
    int tcPair = 1;                       // tensor-core M2L: K chunks without correction products travel
                                          // up to NP per pipeline stage (0: one chunk per stage)
    int tcCorrCut = -2;                   // tensor-core M2L: correction products only for l + lambda <= this

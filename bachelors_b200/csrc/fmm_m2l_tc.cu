@@ -567,7 +567,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       {
          bool firstMma = true;
          int drains = 0;
-         long long tw0 = 0, tw1 = 0, tw2 = 0;
+         long long tw0 = 0, tw1 = 0, tw2 = 0, tFence = 0, tGap = 0, tEnd = 0;
          long long tIssue[6] = {0, 0, 0, 0, 0, 0};   // per K chunk: from the stage's arrival to the commit
          const long long tl = prof ? clock64() : 0;
          DrainSchedule sched(nOff, drainEvery, drainFar);
@@ -587,6 +587,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
 #pragma unroll
             for(int ks = 0; ks < KCH / KS; ks++) nCorK[ks] = m == 1 ? corTab[c0 * (KCH / KS) + ks] : 0;
             long long t0 = prof ? clock64() : 0;
+            if(prof && it > 0) tGap += t0 - tEnd;
             if(!mbarWait(fullBar0 + 8 * s, cur.ph, err, abortFlag, waitNs)) break;
             long long t1 = prof ? clock64() : 0;
             if(!mbarWait(opBar0 + 8 * s, cur.ph, err, abortFlag, waitNs)) break;
@@ -601,6 +602,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             // the tensor core reads the stage (async proxy)
             if(asyncArrive) fenceProxyAsync();
             fenceAfterSync();
+            if(prof) tFence += clock64() - t2;
             const uint32_t st = base + s * stageBytes;
             const uint32_t aSt = st, bSt = st + NP * aBytes;
             // descriptors of the stage's slots; an MMA's operand is the slot's descriptor plus its
@@ -680,10 +682,13 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                   firstMma = true;
                }
             }
+            if(prof) tEnd = clock64();
          }
          mmaCommit(doneBar);
          if(prof)
          {
+            atomicAdd(prof + 12, (unsigned long long)tFence);
+            atomicAdd(prof + 13, (unsigned long long)tGap);
             atomicAdd(prof + 0, (unsigned long long)tw0);
             atomicAdd(prof + 1, (unsigned long long)tw1);
             atomicAdd(prof + 2, (unsigned long long)tw2);
@@ -1103,6 +1108,8 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
               "| producer: loop %.0f, wait stage %.0f | drain: loop %.0f, wait accumulator %.0f\n",
               blocks, it, h[9] / b, h[10] / b, h[3] / b, h[0] / b, h[1] / b, h[2] / b, h[4] / b, h[6] / b, h[5] / b,
               h[8] / b, h[7] / b);
+      fprintf(stderr, "kM2LTc profile, MMA thread cycles per item: fences after the stage's arrival %.0f, from one item's "
+              "end to the next's wait %.0f\n", double(h[12]) / double(h[11]), double(h[13]) / double(h[11]));
       fprintf(stderr, "kM2LTc profile, MMA thread cycles per item from the stage's arrival to its commit, by item:");
       for(int c = 0; c < std::min(cols.nItems, 6); c++) fprintf(stderr, " %.0f", h[16 + c] * double(cols.nItems) / double(h[11]));
       fprintf(stderr, "\n");
