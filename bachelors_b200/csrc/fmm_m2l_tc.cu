@@ -367,8 +367,14 @@ struct M2LCols
    int nc[MAXKSTEPS];   // output columns of the correction products, <= n
    int first[MAXITEMS];
    int count[MAXITEMS];
-   int nItems;          // items per offset
+   int bOff[MAXITEMS][3];   // byte offsets / 16 of the item's operator slots in its B stage
+   int nItems;              // items per offset
 };
+
+// Control area after the stages: barriers, the accumulator's address, the abort flag, the offsets present,
+// then the per-tile tables (16-bit where they fit, so that a third A stage fits at p = 16)
+constexpr int CTRL_HEAD = 256;
+constexpr int CTRL_BYTES = CTRL_HEAD + 2 * 320 + 4 * 64 + 2 * (2 * MAXKSTEPS + 5 * MAXITEMS);
 
 template <int NP, bool TF32>
 __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int Lp, uint8_t* __restrict__ Mout)
@@ -423,14 +429,15 @@ struct DrainSchedule
    }
 };
 
-// Position in the pipeline kept by increments (no divisions in the loops): the stage s and the parity
-// of its current use, the item c of the current offset and the offset's index oi.
+// Position in the pipeline kept by increments (no divisions in the loops): the A stage sa and the B stage
+// sb with the parities of their current uses, the item c of the current offset and the offset's index oi.
 struct PipeCursor
 {
-   int s = 0, ph = 0, c = 0, oi = 0;
-   __device__ __forceinline__ void next(int NS, int nPer)
+   int sa = 0, pha = 0, sb = 0, phb = 0, c = 0, oi = 0;
+   __device__ __forceinline__ void next(int NA, int NB, int nPer)
    {
-      if(++s == NS) { s = 0; ph ^= 1; }
+      if(++sa == NA) { sa = 0; pha ^= 1; }
+      if(++sb == NB) { sb = 0; phb ^= 1; }
       if(++c == nPer) { c = 0; ++oi; }
    }
 };
@@ -441,7 +448,8 @@ template <int NP, class Lay, bool PIECES = false>
 __global__ void __maxnreg__(96)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int nOps, int L, int Lp,
        int nChunks, const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc,
-       int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainFar, int drainItems, int nStages, int drainMode,
+       int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainFar, int drainItems, int nStagesA, int nStagesB,
+       uint32_t bStage, int drainMode,
        const M2LCols cols, unsigned long long* counters, int* err, uint64_t waitNs, int asyncArrive,
        unsigned long long* prof)
 {
@@ -459,31 +467,34 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    extern __shared__ uint8_t smraw[];
    const int N = Lp;                                   // output columns (<= 320)
    const uint32_t aBytes = ROWS * Lay::RB;             // one A piece
-   const uint32_t bBytes = uint32_t(N) * Lay::RB;      // one B piece
-   const uint32_t stageBytes = NP * (aBytes + bBytes);
+   const uint32_t bBytes = uint32_t(N) * Lay::RB;      // one operator block (all N rows of a piece)
+   const uint32_t aStage = NP * aBytes;
    const uint32_t rawAddr = smemAddr(smraw);
    const uint32_t base = (rawAddr + 1023u) & ~1023u;
    uint8_t* sbase = smraw + (base - rawAddr);
-   const int NS = nStages;
-   uint8_t* ctrl = sbase + NS * stageBytes;
-   // full[NS], empty[NS], done, drainFull, drainEmpty, op[NS]: at most 3 MAXSTAGE + 3 = 21 barriers
+   // two rings: NA stages of the gathered multipole pieces (A), NB <= NA stages of operator rows (B)
+   const int NA = nStagesA, NB = nStagesB;
+   const uint32_t bRing = base + NA * aStage;
+   uint8_t* ctrl = sbase + NA * aStage + NB * bStage;
+   // full[NA], empty[NA], done, drainFull, drainEmpty, op[NB]: at most 3 MAXSTAGE + 3 = 21 barriers
    uint64_t* bars = reinterpret_cast<uint64_t*>(ctrl);
    uint32_t* tmemBase = reinterpret_cast<uint32_t*>(ctrl + 192);
    volatile int* abortFlag = reinterpret_cast<volatile int*>(ctrl + 196);
    uint32_t* present = reinterpret_cast<uint32_t*>(ctrl + 200); // 10 words: offsets present in the tile
-   int* itemOffset = reinterpret_cast<int*>(ctrl + 256);        // compacted present offsets [316] + count
-   int* tileNode = itemOffset + 320;                            // the tile's target boxes [TT]
-   int* colTab = tileNode + 64;                                 // output columns per K step [MAXKSTEPS]
-   int* corTab = colTab + MAXKSTEPS;                            // ... of the correction products [MAXKSTEPS]
-   int* itemTab = corTab + MAXKSTEPS;                           // per item: first chunk, chunks [2 MAXITEMS]
+   int* offCount = reinterpret_cast<int*>(ctrl + 240);          // offsets present
+   uint16_t* itemOffset = reinterpret_cast<uint16_t*>(ctrl + CTRL_HEAD); // compacted present offsets [316]
+   int* tileNode = reinterpret_cast<int*>(ctrl + CTRL_HEAD + 2 * 320);    // the tile's target boxes [TT]
+   int16_t* colTab = reinterpret_cast<int16_t*>(tileNode + 64);          // output columns per K step
+   int16_t* corTab = colTab + MAXKSTEPS;                                  // ... of the correction products
+   int16_t* itemTab = corTab + MAXKSTEPS;  // per item: first chunk, chunks, B slot offsets / 16 [5 MAXITEMS]
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
    const int first = blockIdx.x * TT;
    const int nTile = min(TT, nTargets - first);
-   const uint32_t fullBar0 = smemAddr(&bars[0]), emptyBar0 = smemAddr(&bars[NS]), doneBar = smemAddr(&bars[2 * NS]);
-   const uint32_t drainFull = smemAddr(&bars[2 * NS + 1]), drainEmpty = smemAddr(&bars[2 * NS + 2]);
-   const uint32_t opBar0 = smemAddr(&bars[2 * NS + 3]);
+   const uint32_t fullBar0 = smemAddr(&bars[0]), emptyBar0 = smemAddr(&bars[NA]), doneBar = smemAddr(&bars[2 * NA]);
+   const uint32_t drainFull = smemAddr(&bars[2 * NA + 1]), drainEmpty = smemAddr(&bars[2 * NA + 2]);
+   const uint32_t opBar0 = smemAddr(&bars[2 * NA + 3]);
 
    if(tid < 10) present[tid] = 0;
    if(tid < TT) tileNode[tid] = tid < nTile ? targets[first + tid] : -1;
@@ -492,25 +503,27 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
 #pragma unroll
       for(int g = 0; g < MAXKSTEPS; g++)
       {
-         colTab[g] = cols.n[g];
-         corTab[g] = cols.nc[g];
+         colTab[g] = int16_t(cols.n[g]);
+         corTab[g] = int16_t(cols.nc[g]);
       }
 #pragma unroll
       for(int i = 0; i < MAXITEMS; i++)
       {
-         itemTab[2 * i] = cols.first[i];
-         itemTab[2 * i + 1] = cols.count[i];
+         itemTab[5 * i] = int16_t(cols.first[i]);
+         itemTab[5 * i + 1] = int16_t(cols.count[i]);
+#pragma unroll
+         for(int j = 0; j < 3; j++) itemTab[5 * i + 2 + j] = int16_t(cols.bOff[i][j]);
       }
    }
    if(tid == 0)
    {
       *abortFlag = 0;
-      for(int s = 0; s < NS; s++)
+      for(int s = 0; s < NA; s++)
       {
          mbarInit(fullBar0 + 8 * s, NPROD);
          mbarInit(emptyBar0 + 8 * s, 1);
-         mbarInit(opBar0 + 8 * s, 1);
       }
+      for(int s = 0; s < NB; s++) mbarInit(opBar0 + 8 * s, 1);
       mbarInit(doneBar, 1);
       mbarInit(drainFull, 1);
       mbarInit(drainEmpty, 256);
@@ -540,9 +553,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       for(int i = 0; i < nOps; i++)
       {
          const int o = nOps == 316 ? d_m2lFarFirst[i] : i;
-         if(present[o >> 5] & (1u << (o & 31))) itemOffset[k++] = o;
+         if(present[o >> 5] & (1u << (o & 31))) itemOffset[k++] = uint16_t(o);
       }
-      itemOffset[316] = k;
+      *offCount = k;
       // work accounting: pipeline items and tile-offset pairs
       if(counters)
       {
@@ -551,7 +564,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       }
    }
    __syncthreads();
-   const int nOff = itemOffset[316];
+   const int nOff = *offCount;
    const int nPer = cols.nItems;                       // items per offset
    const int nItems = nOff * nPer;
    const uint32_t tmem = *tmemBase;
@@ -573,11 +586,13 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          DrainSchedule sched(nOff, drainEvery, drainFar);
          PipeCursor cur;
          int sinceDrain = 0;
-         for(int it = 0; it < nItems; it++, cur.next(NS, nPer))
+         for(int it = 0; it < nItems; it++, cur.next(NA, NB, nPer))
          {
-            const int s = cur.s;
-            // the item's chunks and their output widths per K step, read before the wait
-            const int c0 = itemTab[2 * cur.c], m = itemTab[2 * cur.c + 1];
+            // the item's chunks, its operator slots and their output widths per K step, read before the wait
+            const int c0 = itemTab[5 * cur.c], m = itemTab[5 * cur.c + 1];
+            int bo[NP];
+#pragma unroll
+            for(int j = 0; j < NP; j++) bo[j] = itemTab[5 * cur.c + 2 + j];
             int nColK[NP][KCH / KS], nCorK[KCH / KS];
 #pragma unroll
             for(int j = 0; j < NP; j++)
@@ -588,9 +603,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             for(int ks = 0; ks < KCH / KS; ks++) nCorK[ks] = m == 1 ? corTab[c0 * (KCH / KS) + ks] : 0;
             long long t0 = prof ? clock64() : 0;
             if(prof && it > 0) tGap += t0 - tEnd;
-            if(!mbarWait(fullBar0 + 8 * s, cur.ph, err, abortFlag, waitNs)) break;
+            if(!mbarWait(fullBar0 + 8 * cur.sa, cur.pha, err, abortFlag, waitNs)) break;
             long long t1 = prof ? clock64() : 0;
-            if(!mbarWait(opBar0 + 8 * s, cur.ph, err, abortFlag, waitNs)) break;
+            if(!mbarWait(opBar0 + 8 * cur.sb, cur.phb, err, abortFlag, waitNs)) break;
             long long t2 = 0;
             if(prof)
             {
@@ -603,10 +618,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             if(asyncArrive) fenceProxyAsync();
             fenceAfterSync();
             if(prof) tFence += clock64() - t2;
-            const uint32_t st = base + s * stageBytes;
-            const uint32_t aSt = st, bSt = st + NP * aBytes;
-            // descriptors of the stage's slots; an MMA's operand is the slot's descriptor plus its
-            // byte offset / 16 (the start-address field, bits 0-13, holds every address of the stage)
+            const uint32_t aSt = base + cur.sa * aStage, bSt = bRing + cur.sb * bStage;
+            // descriptors of the stages; an MMA's operand is the stage's descriptor plus the slot's
+            // byte offset / 16 (the start-address field, bits 0-13, holds every shared-memory address)
             const uint64_t dA = smemDescT<Lay>(aSt), dB = smemDescT<Lay>(bSt);
 #pragma unroll
             for(int j = 0; j < NP; j++)
@@ -636,7 +650,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                      const int pa = j + (NP == 1 ? 0 : (NP == 2 ? PA2[pass] : PA[pass]));
                      const int pb = j + (NP == 1 ? 0 : (NP == 2 ? PB2[pass] : PB[pass]));
                      const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
-                     const uint64_t db = dB + ((pb * bBytes + koff) >> 4);
+                     const uint64_t db = dB + uint64_t(bo[pb]) + (koff >> 4);
                      const uint32_t acc = firstMma ? 0u : 1u;
                      if constexpr(Lay::TF32)
                      {
@@ -652,7 +666,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                   }
                }
             }
-            mmaCommit(emptyBar0 + 8 * s);
+            mmaCommit(emptyBar0 + 8 * cur.sa);
             if(prof && cur.c < 6) tIssue[cur.c] += clock64() - t2;
             // every drainEvery offsets (and after the last) hand the accumulator to the drain warps
             // and start a fresh one: the tensor cores' FP32 accumulation truncates, so long chains
@@ -705,15 +719,21 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          int issued = 0;
          long long twe = 0;
          PipeCursor cur;
-         for(int it = 0; it < nItems; it++, cur.next(NS, nPer))
+         for(int it = 0; it < nItems; it++, cur.next(NA, NB, nPer))
          {
-            const int s = cur.s;
+            const int s = cur.sb;
             const long long t0 = prof ? clock64() : 0;
-            // the stage's previous use (parity ph ^ 1) must have been consumed
-            if(it >= NS && !mbarWait(emptyBar0 + 8 * s, cur.ph ^ 1, err, abortFlag, waitNs)) break;
+            // the B stage's previous use, item it - NB, must have been consumed: its MMAs completed when
+            // the empty barrier of its A stage completed its use (it - NB) / NA. (That barrier cannot
+            // complete a later use first: item it - NB + NA >= it needs this item's operator rows.)
+            if(it >= NB)
+            {
+               const int prev = it - NB;
+               if(!mbarWait(emptyBar0 + 8 * (prev % NA), (prev / NA) & 1, err, abortFlag, waitNs)) break;
+            }
             if(prof) twe += clock64() - t0;
-            const int o = itemOffset[cur.oi], c0 = itemTab[2 * cur.c], m = itemTab[2 * cur.c + 1];
-            const uint32_t dst = base + s * stageBytes + NP * aBytes;
+            const int o = itemOffset[cur.oi], c0 = itemTab[5 * cur.c], m = itemTab[5 * cur.c + 1];
+            const uint32_t dst = bRing + s * bStage;
             // only the operator rows (output columns) a chunk's widest K step uses: of the leading
             // piece for the hi * hi product, of the others for the correction products. A chunk alone
             // fills the slots with its pieces, chunks sharing the stage their leading pieces.
@@ -733,17 +753,17 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             {
                const uint8_t* src = m == 1 ? img + ((int64_t(o) * nChunks + c0) * NP + j) * bBytes
                                            : img + (int64_t(o) * nChunks + c0 + j) * NP * bBytes;
-               if(bytes[j]) bulkLoad(dst + j * bBytes, src, bytes[j], opBar0 + 8 * s);
+               if(bytes[j]) bulkLoad(dst + 16u * uint32_t(itemTab[5 * cur.c + 2 + j]), src, bytes[j], opBar0 + 8 * s);
             }
             issued = it + 1;
          }
          // the copies in flight write this CTA's shared memory: wait for them before it can exit. A stage
          // is reused only after the MMAs consumed its previous item, which waited for that item's copy, so
          // only the last item issued on each stage can still be in flight.
-         for(int s = 0; s < NS && s < issued; s++)
+         for(int s = 0; s < NB && s < issued; s++)
          {
-            const int last = s + ((issued - 1 - s) / NS) * NS;
-            mbarWaitIssued(opBar0 + 8 * s, (last / NS) & 1, err);
+            const int last = s + ((issued - 1 - s) / NB) * NB;
+            mbarWaitIssued(opBar0 + 8 * s, (last / NB) & 1, err);
          }
          if(prof) atomicAdd(prof + 4, (unsigned long long)twe);
       }
@@ -918,9 +938,9 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       long long twp = 0;
       const long long tpl = prof ? clock64() : 0;
       PipeCursor cur;
-      for(int it = 0; it < nItems; it++, cur.next(NS, nPer))
+      for(int it = 0; it < nItems; it++, cur.next(NA, NB, nPer))
       {
-         const int s = cur.s;
+         const int s = cur.sa;
          const int oi = cur.oi, c = cur.c;
          if(c == 0 && oi + 1 < nOff)
             srcNext = tgt >= 0 ? vtab[int64_t(tgt) * nOps + itemOffset[oi + 1]] : -1;
@@ -933,10 +953,10 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             pending = -1;
          }
          const long long t0 = prof ? clock64() : 0;
-         if(it >= NS && !mbarWait(emptyBar0 + 8 * s, cur.ph ^ 1, err, abortFlag, waitNs)) break;
+         if(it >= NA && !mbarWait(emptyBar0 + 8 * s, cur.pha ^ 1, err, abortFlag, waitNs)) break;
          if(prof) twp += clock64() - t0;
-         const uint32_t aSt = base + s * stageBytes;
-         const int c0 = itemTab[2 * c], m = itemTab[2 * c + 1];
+         const uint32_t aSt = base + s * aStage;
+         const int c0 = itemTab[5 * c], m = itemTab[5 * c + 1];
          const uint8_t* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp * Lay::ES;
          // a chunk alone: its pieces into the slots, the ones after the leading piece only when its first
          // (widest) K step has correction products; chunks sharing the stage: chunk c0 + j's leading
@@ -958,7 +978,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          }
          if(asyncArrive)
             // the barrier completes when every producer's copies of this item have landed, while the
-            // thread goes on with the next free stage: up to NS items in flight
+            // thread goes on with the next free stage: up to NA items in flight
             cpAsyncArriveNoinc(fullBar0 + 8 * s);
          else
          {
@@ -1018,6 +1038,47 @@ static fmm_status planItems(M2LCols& cols, int nChunks, int stepsPerChunk, int N
    return FMM_OK;
 }
 
+// The operator slots of every item in its B stage (M2LCols::bOff), the B stage size, and the stage counts of
+// the two rings within the shared memory: two B stages (more while A stages outnumber them) and as many A
+// stages as the rest holds.
+struct StagePlan
+{
+   int na, nb;
+   uint32_t bStage;
+   size_t smem;
+};
+static constexpr size_t SMEM_BUDGET = 232448;   // the opt-in dynamic shared memory of one block
+
+static fmm_status planStages(M2LCols& cols, int NP, int stepsPerChunk, int rowBytes, const char* what, StagePlan& sp)
+{
+   uint32_t bStage = 1024;
+   for(int i = 0; i < cols.nItems; i++)
+   {
+      const int c0 = cols.first[i], m = cols.count[i];
+      uint32_t off = 0;
+      for(int j = 0; j < 3; j++) cols.bOff[i][j] = 0;
+      for(int j = 0; j < NP; j++)
+      {
+         cols.bOff[i][j] = int(off / 16);
+         int rows = 0;
+         if(m == 1) rows = j == 0 ? cols.n[c0 * stepsPerChunk] : cols.nc[c0 * stepsPerChunk];
+         else if(j < m) rows = cols.n[(c0 + j) * stepsPerChunk];
+         off += uint32_t(rows) * uint32_t(rowBytes);
+      }
+      bStage = std::max(bStage, off);
+   }
+   bStage = (bStage + 1023u) & ~1023u;
+   const size_t aStage = size_t(NP) * tc::ROWS * rowBytes;
+   const size_t fixed = 1024 + CTRL_BYTES;
+   if(fixed + 2 * (aStage + bStage) > SMEM_BUDGET)
+      return setError(FMM_E_INVALID, "%s: stages of %zu + %u bytes do not fit twice", what, aStage, bStage);
+   int nb = 2;
+   const int na = int(std::min<size_t>(tc::MAXSTAGE, (SMEM_BUDGET - fixed - nb * size_t(bStage)) / aStage));
+   while(nb < na && fixed + na * aStage + (nb + 1) * size_t(bStage) <= SMEM_BUDGET) nb++;
+   sp = {na, nb, bStage, fixed + na * aStage + nb * size_t(bStage)};
+   return FMM_OK;
+}
+
 template <int NP, class Lay>
 static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
 {
@@ -1067,13 +1128,11 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
       cols.nc[g] = corr < 0 ? cols.n[g] : std::min(cols.n[g], nc);
    }
    FMM_TRY(planItems(cols, nChunks, Lay::KC / Lay::KSTEP, NP, P.tcPair != 0));
-   const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS + 2 * MAXITEMS);
-   const size_t budget = 232448;
-   const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
-   if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core M2L: %zu-byte stages do not fit twice", stageBytes);
-   const size_t smem = fixed + nStages * stageBytes;
-   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   StagePlan sp;
+   FMM_TRY(planStages(cols, NP, Lay::KC / Lay::KSTEP, Lay::RB, "tensor-core M2L", sp));
+   // (the attribute is the budget, not this launch's size: the translations share the kernel and a graph
+   // replays every launch with its own size)
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_BUDGET)));
    const int64_t rows = P.tree.nNodes * 3;
    // developer switch FMM_TC_PROF=1: per-role SM cycles of this launch, printed to stderr
    unsigned long long* prof = nullptr;
@@ -1090,10 +1149,10 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
       kSplitMultipoles<NP, Lay::TF32><<<148 * 16, 256, 0, st>>>((const float*)P.mult.ptr, rows, Lp, (uint8_t*)P.multBf.ptr);
       FMM_TRY(launched(P, "kSplitMultipoles", st));
    }
-   kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
+   kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, sp.smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
                                                       nChunks, (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
                                                       (float*)P.local.ptr, 0, nullptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
-                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, nStages, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive,
+                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, sp.na, sp.nb, sp.bStage, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive,
                                                       prof);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(prof)
@@ -1151,14 +1210,11 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
    for(int g = 0; g < nSteps; g++) cols.n[g] = cols.nc[g] = Lay::KSTEP * g < L ? Lp : 0;
    // every chunk alone in its stage: the drains every drainItems items need full-width chunks
    FMM_TRY(planItems(cols, nChunks, Lay::KC / Lay::KSTEP, NP, false));
-   const size_t stageBytes = NP * (size_t(tc::ROWS) + size_t(Lp)) * Lay::RB;
-   const size_t fixed = 1024 + 256 + 4 * (320 + 64 + 2 * MAXKSTEPS + 2 * MAXITEMS);
-   const size_t budget = 232448;
-   const int nStages = int(std::min<size_t>(tc::MAXSTAGE, (budget - fixed) / stageBytes));
-   if(nStages < 2) return setError(FMM_E_INVALID, "tensor-core translation: %zu-byte stages do not fit twice", stageBytes);
-   const size_t smem = fixed + nStages * stageBytes;
-   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+   StagePlan sp;
+   FMM_TRY(planStages(cols, NP, Lay::KC / Lay::KSTEP, Lay::RB, "tensor-core translation", sp));
+   const size_t smem = sp.smem;
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_BUDGET)));
+   FMM_CUDA(cudaFuncSetAttribute(kM2LTc<NP, Lay, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_BUDGET)));
    const int64_t rows = P.tree.nNodes * 3;
    FMM_TRY(P.multBf.reserve(size_t(Lay::ES) * rows * NP * Lp));
    const int drainEvery = NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2);
@@ -1186,7 +1242,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          kern<<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.parList.ptr + a, b - a, (const int*)P.vtabUp.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0,
-            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, nStages, P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
+            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, sp.na, sp.nb, sp.bStage, P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
          FMM_TRY(launched(P, "kM2LTc<M2M>", st));
       }
       P.multBfTag = NP * 2 + (Lay::TF32 ? 1 : 0);
@@ -1201,7 +1257,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          kM2LTc<NP, Lay><<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.l2lTargets.ptr + a, b - a, (const int*)P.vtabDn.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, nullptr, drainEvery, drainEvery,
-            P.tcTrDrainItems, nStages,
+            P.tcTrDrainItems, sp.na, sp.nb, sp.bStage,
             P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
          FMM_TRY(launched(P, "kM2LTc<L2L>", st));
       }
