@@ -216,6 +216,8 @@ struct Plan
                                          // the MMA thread fences (up to NS items in flight, but the MMA
                                          // thread loses ~400-600 cycles per item after such a barrier:
                                          // M2L 159 ms against 137 ms at 2^24)
+   int tcKeepTail = 1;                   // tensor-core M2L: accumulator columns >= 256 (the top degrees) are
+                                         // drained once per tile, not with the others
    int tcPair = 1;                       // tensor-core M2L: K chunks without correction products travel
                                          // up to NP per pipeline stage (0: one chunk per stage)
    int tcCorrCut = -2;                   // tensor-core M2L: correction products only for l + lambda <= this

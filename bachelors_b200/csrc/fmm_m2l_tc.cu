@@ -231,6 +231,13 @@ __device__ __forceinline__ void tmemLd16NoWait(uint32_t addr, uint32_t* r)
       : "r"(addr));
 }
 __device__ __forceinline__ void tmemWaitLd() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// 32 lanes x 8 columns of FP32, no wait
+__device__ __forceinline__ void tmemLd8NoWait(uint32_t addr, uint32_t* r)
+{
+   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                : "r"(addr));
+}
 __device__ __forceinline__ void tmemSt16(uint32_t addr, const uint32_t* r)
 {
    asm volatile(
@@ -401,6 +408,14 @@ __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int 
    }
 }
 
+// First column of the kept tail (keepTail, N > 256): the drains sum the columns that the tensor memory beside the
+// accumulator (512 - N) and 32 registers per row hold; the columns after them, the top degrees, accumulate
+// through the whole tile. Without a tail: N.
+__host__ __device__ constexpr int tailSplit(int keepTail, int N)
+{
+   return !(keepTail && N > 256) ? N : (((512 - N + 32) & ~15) < 256 ? ((512 - N + 32) & ~15) : 256);
+}
+
 // Whether the accumulator is drained after the oi-th of nOff offsets: every dNear offsets, and, when
 // dFar differs, every dFar offsets through the first (far) half of the offsets, which ends with a drain.
 // Offsets run far first, so the first half holds the small contributions: the tensor core's accumulation
@@ -449,7 +464,7 @@ __global__ void __maxnreg__(96)
 kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vtab, int nOps, int L, int Lp,
        int nChunks, const uint8_t* __restrict__ img, const uint8_t* __restrict__ Mbf, float* __restrict__ Lc,
        int addOut, uint8_t* __restrict__ Mout, int drainEvery, int drainFar, int drainItems, int nStagesA, int nStagesB,
-       uint32_t bStage, int drainMode,
+       uint32_t bStage, int drainMode, int keepTail,
        const M2LCols cols, unsigned long long* counters, int* err, uint64_t waitNs, int asyncArrive,
        unsigned long long* prof)
 {
@@ -579,8 +594,12 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       if(lane == 0)
       {
          bool firstMma = true;
+         bool tailFirst = true;   // keepTail: the columns >= split accumulate through the whole tile
+         // an MMA covers at most 256 columns; a wider K step is split at 256, with keepTail where the kept
+         // columns start
+         const int split = keepTail ? tailSplit(1, N) : 256;
          int drains = 0;
-         long long tw0 = 0, tw1 = 0, tw2 = 0, tFence = 0, tGap = 0, tEnd = 0;
+         long long tw0 = 0, tw1 = 0, tw2 = 0;
          long long tIssue[6] = {0, 0, 0, 0, 0, 0};   // per K chunk: from the stage's arrival to the commit
          const long long tl = prof ? clock64() : 0;
          DrainSchedule sched(nOff, drainEvery, drainFar);
@@ -602,7 +621,6 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
 #pragma unroll
             for(int ks = 0; ks < KCH / KS; ks++) nCorK[ks] = m == 1 ? corTab[c0 * (KCH / KS) + ks] : 0;
             long long t0 = prof ? clock64() : 0;
-            if(prof && it > 0) tGap += t0 - tEnd;
             if(!mbarWait(fullBar0 + 8 * cur.sa, cur.pha, err, abortFlag, waitNs)) break;
             long long t1 = prof ? clock64() : 0;
             if(!mbarWait(opBar0 + 8 * cur.sb, cur.phb, err, abortFlag, waitNs)) break;
@@ -617,7 +635,6 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             // the tensor core reads the stage (async proxy)
             if(asyncArrive) fenceProxyAsync();
             fenceAfterSync();
-            if(prof) tFence += clock64() - t2;
             const uint32_t aSt = base + cur.sa * aStage, bSt = bRing + cur.sb * bStage;
             // descriptors of the stages; an MMA's operand is the stage's descriptor plus the slot's
             // byte offset / 16 (the start-address field, bits 0-13, holds every shared-memory address)
@@ -643,7 +660,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                   {
                      const int w = pass == 0 ? nCol : nCor;
                      if(w == 0) break;
-                     const int nA = min(w, 256), nB = w - nA;
+                     const int nA = min(w, split), nB = w - nA;
                      const uint32_t idA = Lay::TF32 ? instrDescTf32(ROWS, nA) : instrDescBf16(ROWS, nA);
                      const uint32_t idB = Lay::TF32 ? instrDescTf32(ROWS, nB > 0 ? nB : 16) : instrDescBf16(ROWS, nB > 0 ? nB : 16);
                      // piece slots: pa, pb for a chunk alone, slot j (pass 0 only) for a shared stage
@@ -652,17 +669,19 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                      const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
                      const uint64_t db = dB + uint64_t(bo[pb]) + (koff >> 4);
                      const uint32_t acc = firstMma ? 0u : 1u;
+                     const uint32_t accT = keepTail ? (tailFirst ? 0u : 1u) : acc;
                      if constexpr(Lay::TF32)
                      {
                         mmaTf32(tmem, da, db, idA, acc);
-                        if(nB > 0) mmaTf32(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                        if(nB > 0) mmaTf32(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, accT);
                      }
                      else
                      {
                         mmaBf16(tmem, da, db, idA, acc);
-                        if(nB > 0) mmaBf16(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, acc);
+                        if(nB > 0) mmaBf16(tmem + nA, da, db + ((nA * Lay::RB) >> 4), idB, accT);
                      }
                      firstMma = false;
+                     if(nB > 0) tailFirst = false;
                   }
                }
             }
@@ -696,13 +715,10 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                   firstMma = true;
                }
             }
-            if(prof) tEnd = clock64();
          }
          mmaCommit(doneBar);
          if(prof)
          {
-            atomicAdd(prof + 12, (unsigned long long)tFence);
-            atomicAdd(prof + 13, (unsigned long long)tGap);
             atomicAdd(prof + 0, (unsigned long long)tw0);
             atomicAdd(prof + 1, (unsigned long long)tw1);
             atomicAdd(prof + 2, (unsigned long long)tw2);
@@ -788,11 +804,15 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       // deterministic. Its columns live in three parts:
       //   [0, nS)    in the tensor memory the accumulator leaves free (columns N .. 511), drainMode >= 2
       //   [nS, nR)   in this thread's registers (RHALF columns per half), drainMode 3
-      //   [nR, N)    in the local expansions: fire-and-forget vector atomics (drainMode 0) or
+      //   [nR, nT)   in the local expansions: fire-and-forget vector atomics (drainMode 0) or
       //              load-add-store, the first drain storing (drainMode >= 1)
+      // With keepTail the columns [nT, N) (the top degrees, whose terms are the smallest; the columns the
+      // tensor memory and the registers cannot hold) are not drained: their accumulation runs through the
+      // whole tile in tensor memory and the last drain writes it.
       constexpr int RHALF = 16;
-      const int nS = drainMode >= 2 ? (min(N, 512 - N) & ~15) : 0;
-      const int nR = drainMode == 3 ? min(N, nS + 2 * RHALF) : nS;
+      const int nT = tailSplit(keepTail, N);
+      const int nS = drainMode >= 2 ? (min(nT, 512 - N) & ~15) : 0;
+      const int nR = drainMode == 3 ? min(nT, nS + 2 * RHALF) : nS;
       // [a, b) split at a multiple of 16 columns; this warp's half
       auto split = [&](int a, int b, int& lo, int& hi) {
          const int mid = min(b, a + ((((b - a) >> 1) + 15) & ~15));
@@ -803,7 +823,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       split(0, nS, sLo, sHi);
       const int rLo = nS + half * RHALF;
       const int rHi = min(nR, rLo + RHALF);
-      split(nR, N, gLo, gHi);
+      split(nR, nT, gLo, gHi);
       const uint32_t tSum = tAcc + uint32_t(N);
       float rsum[RHALF];
 #pragma unroll
@@ -880,34 +900,41 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                }
             }
          }
-         // global part, 16 columns per step; the running sums load while the accumulator does
-         // with addOut the first drain adds to the values already there as well
-         const bool rmw = drainMode != 0 && (d > 0 || addOut) && et >= 0;
-         for(int c0 = gLo; c0 < gHi; c0 += 16)
+         // global part, 16 columns per step (with addOut the first drain adds to the values already there
+         // as well); the running sums load while the accumulator does. The last drain also writes the
+         // kept columns [nT, N) the same way: their accumulator, plus the values there with addOut.
+         int tLo = 0, tHi = 0;
+         if(last) split(nT, N, tLo, tHi);
+         for(int part = 0; part < 2; part++)
          {
-            uint32_t u[16];
-            float4 old[4];
-            float4* o4 = reinterpret_cast<float4*>(out + c0);
-            tmemLd16NoWait(tAcc + uint32_t(c0), u);
-            if(rmw)
+            const int lo = part ? tLo : gLo, hi = part ? tHi : gHi;
+            const bool rmw = drainMode != 0 && (part ? addOut != 0 : (d > 0 || addOut)) && et >= 0;
+            for(int c0 = lo; c0 < hi; c0 += 16)
             {
-#pragma unroll
-               for(int i = 0; i < 4; i++) old[i] = o4[i];
-            }
-            tmemWaitLd();
-            if(et < 0) continue;
-#pragma unroll
-            for(int i = 0; i < 4; i++)
-            {
-               const float4 v = make_float4(__uint_as_float(u[4 * i]), __uint_as_float(u[4 * i + 1]),
-                                            __uint_as_float(u[4 * i + 2]), __uint_as_float(u[4 * i + 3]));
-               if(drainMode == 0) atomicAdd(o4 + i, v);
-               else
+               uint32_t u[16];
+               float4 old[4];
+               float4* o4 = reinterpret_cast<float4*>(out + c0);
+               tmemLd16NoWait(tAcc + uint32_t(c0), u);
+               if(rmw)
                {
-                  const float4 f = rmw ? make_float4(old[i].x + v.x, old[i].y + v.y, old[i].z + v.z, old[i].w + v.w) : v;
-                  o4[i] = f;
-                  // (Mout is only given with drainMode != 0: atomics leave the final value unknown here)
-                  if(PIECES && last) storePieces4(Mout, int64_t(et) * 3 + ec, c0 + 4 * i, Lp, Lay::TF32 ? 1 : NP, f);
+#pragma unroll
+                  for(int i = 0; i < 4; i++) old[i] = o4[i];
+               }
+               tmemWaitLd();
+               if(et < 0) continue;
+#pragma unroll
+               for(int i = 0; i < 4; i++)
+               {
+                  const float4 v = make_float4(__uint_as_float(u[4 * i]), __uint_as_float(u[4 * i + 1]),
+                                               __uint_as_float(u[4 * i + 2]), __uint_as_float(u[4 * i + 3]));
+                  if(drainMode == 0) atomicAdd(o4 + i, v);
+                  else
+                  {
+                     const float4 f = rmw ? make_float4(old[i].x + v.x, old[i].y + v.y, old[i].z + v.z, old[i].w + v.w) : v;
+                     o4[i] = f;
+                     // (Mout is only given with drainMode != 0: atomics leave the final value unknown here)
+                     if(PIECES && last) storePieces4(Mout, int64_t(et) * 3 + ec, c0 + 4 * i, Lp, Lay::TF32 ? 1 : NP, f);
+                  }
                }
             }
          }
@@ -916,6 +943,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
       }
       if(prof && warp == 10 && lane == 0)
       {
+         atomicAdd(prof + 23, (unsigned long long)nDrains);
          atomicAdd(prof + 7, (unsigned long long)twd);
          atomicAdd(prof + 8, (unsigned long long)(clock64() - tdl));
       }
@@ -1152,7 +1180,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
    kM2LTc<NP, Lay><<<blocks, tc::NTHREADS, sp.smem, st>>>((const int*)P.m2lTargets.ptr, count, P.lists.vtab, 316, L, Lp,
                                                       nChunks, (const uint8_t*)P.opM2Lbf.ptr, (const uint8_t*)P.multBf.ptr,
                                                       (float*)P.local.ptr, 0, nullptr, (NP == 2 ? P.tcDrainEvery : std::max(1, P.tcDrainEvery / 2)),
-                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, sp.na, sp.nb, sp.bStage, P.tcDrainMode, cols, (unsigned long long*)P.tcCounters.ptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive,
+                                                      (NP == 2 ? P.tcDrainFar : std::max(1, P.tcDrainFar / 2)), 0, sp.na, sp.nb, sp.bStage, P.tcDrainMode, P.tcKeepTail, cols, (unsigned long long*)P.tcCounters.ptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive,
                                                       prof);
    FMM_TRY(launched(P, "kM2LTc", st));
    if(prof)
@@ -1167,8 +1195,7 @@ static fmm_status launchM2LTc(Plan& P, cudaStream_t st)
               "| producer: loop %.0f, wait stage %.0f | drain: loop %.0f, wait accumulator %.0f\n",
               blocks, it, h[9] / b, h[10] / b, h[3] / b, h[0] / b, h[1] / b, h[2] / b, h[4] / b, h[6] / b, h[5] / b,
               h[8] / b, h[7] / b);
-      fprintf(stderr, "kM2LTc profile, MMA thread cycles per item: fences after the stage's arrival %.0f, from one item's "
-              "end to the next's wait %.0f\n", double(h[12]) / double(h[11]), double(h[13]) / double(h[11]));
+      fprintf(stderr, "kM2LTc profile, drains per CTA %.1f\n", double(h[23]) / b);
       fprintf(stderr, "kM2LTc profile, MMA thread cycles per item from the stage's arrival to its commit, by item:");
       for(int c = 0; c < std::min(cols.nItems, 6); c++) fprintf(stderr, " %.0f", h[16 + c] * double(cols.nItems) / double(h[11]));
       fprintf(stderr, "\n");
@@ -1242,7 +1269,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
          kern<<<(b - a + tc::TT - 1) / tc::TT, tc::NTHREADS, smem, st>>>(
             (const int*)P.parList.ptr + a, b - a, (const int*)P.vtabUp.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opM2Mbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.mult.ptr, 0,
-            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, sp.na, sp.nb, sp.bStage, P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
+            (uint8_t*)P.multBf.ptr, drainEvery, drainEvery, P.tcTrDrainItems, sp.na, sp.nb, sp.bStage, P.tcDrainMode, 0, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
          FMM_TRY(launched(P, "kM2LTc<M2M>", st));
       }
       P.multBfTag = NP * 2 + (Lay::TF32 ? 1 : 0);
@@ -1258,7 +1285,7 @@ static fmm_status translateTc(Plan& P, cudaStream_t st, bool up)
             (const int*)P.l2lTargets.ptr + a, b - a, (const int*)P.vtabDn.ptr, 8, L, Lp, nChunks,
             (const uint8_t*)P.opL2Lbf.ptr, (const uint8_t*)P.multBf.ptr, (float*)P.local.ptr, 1, nullptr, drainEvery, drainEvery,
             P.tcTrDrainItems, sp.na, sp.nb, sp.bStage,
-            P.tcDrainMode, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
+            P.tcDrainMode, 0, cols, nullptr, P.pipeErr, P.tcWaitNs, P.tcAsyncArrive, nullptr);
          FMM_TRY(launched(P, "kM2LTc<L2L>", st));
       }
       P.multBfTag = -1;
