@@ -381,7 +381,34 @@ struct M2LCols
 // Control area after the stages: barriers, the accumulator's address, the abort flag, the offsets present,
 // then the per-tile tables (16-bit where they fit, so that a third A stage fits at p = 16)
 constexpr int CTRL_HEAD = 256;
-constexpr int CTRL_BYTES = CTRL_HEAD + 2 * 320 + 4 * 64 + 2 * (2 * MAXKSTEPS + 5 * MAXITEMS);
+constexpr int REC = 24;   // 16-bit fields per item record (ItemRec), 48 bytes
+constexpr int CTRL_BYTES = CTRL_HEAD + 2 * 320 + 4 * 64 + 2 * REC * MAXITEMS;
+
+// An item's record in shared memory, read with one vector load per 8 fields: first chunk, chunks, the B
+// slots' offsets / 16 [NP], the output columns of every K step of its chunks [NP][K steps per chunk] (0 beyond
+// the item's chunks and past the last coefficient), the correction products' columns [K steps per chunk] (0
+// unless the item is one chunk).
+template <int NP, int KPC>
+struct ItemRec
+{
+   static constexpr int FIRST = 0, COUNT = 1, BOFF = 2, NCOL = 2 + NP, NCOR = 2 + NP + NP * KPC;
+   static constexpr int WORDS = (NCOR + KPC + 7) / 8;   // 16-byte words read
+   static_assert(WORDS * 8 <= REC, "item record too small");
+   int4 q[WORDS];
+   __device__ __forceinline__ void load(const int4* tab, int item)
+   {
+#pragma unroll
+      for(int w = 0; w < WORDS; w++) q[w] = tab[(REC / 8) * item + w];
+   }
+   // field k (a constant once the callers' loops are unrolled)
+   __device__ __forceinline__ int operator[](int k) const
+   {
+      const int4& v4 = q[k >> 3];
+      const int w = (k >> 1) & 3;
+      const int v = w == 0 ? v4.x : w == 1 ? v4.y : w == 2 ? v4.z : v4.w;
+      return (v >> (16 * (k & 1))) & 0xFFFF;
+   }
+};
 
 template <int NP, bool TF32>
 __global__ void kSplitMultipoles(const float* __restrict__ M, int64_t rows, int Lp, uint8_t* __restrict__ Mout)
@@ -472,7 +499,6 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    const long long tStart = prof ? clock64() : 0;
    using namespace tc;
    constexpr int KCH = Lay::KC;
-   constexpr int KS = Lay::KSTEP;                      // K elements per MMA
    constexpr int NPASS = NP == 1 ? 1 : (NP == 2 ? 3 : 6);
    // (A piece, B piece) of every product kept: hi*hi, hi*lo, lo*hi  /  down to 2^-16 with three pieces
    constexpr int PA[6] = {0, 0, 1, 1, 0, 2};
@@ -499,9 +525,10 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    int* offCount = reinterpret_cast<int*>(ctrl + 240);          // offsets present
    uint16_t* itemOffset = reinterpret_cast<uint16_t*>(ctrl + CTRL_HEAD); // compacted present offsets [316]
    int* tileNode = reinterpret_cast<int*>(ctrl + CTRL_HEAD + 2 * 320);    // the tile's target boxes [TT]
-   int16_t* colTab = reinterpret_cast<int16_t*>(tileNode + 64);          // output columns per K step
-   int16_t* corTab = colTab + MAXKSTEPS;                                  // ... of the correction products
-   int16_t* itemTab = corTab + MAXKSTEPS;  // per item: first chunk, chunks, B slot offsets / 16 [5 MAXITEMS]
+   uint16_t* recTab = reinterpret_cast<uint16_t*>(tileNode + 64);          // item records [MAXITEMS][REC]
+   const int4* rec4 = reinterpret_cast<const int4*>(recTab);
+   constexpr int KPC = Lay::KC / Lay::KSTEP;                               // K steps per chunk
+   using Rec = ItemRec<NP, KPC>;
 
    const int tid = threadIdx.x;
    const int warp = tid >> 5, lane = tid & 31;
@@ -515,19 +542,21 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
    if(tid < TT) tileNode[tid] = tid < nTile ? targets[first + tid] : -1;
    if(tid == 0)
    {
-#pragma unroll
-      for(int g = 0; g < MAXKSTEPS; g++)
+      for(int i = 0; i < cols.nItems; i++)
       {
-         colTab[g] = int16_t(cols.n[g]);
-         corTab[g] = int16_t(cols.nc[g]);
-      }
-#pragma unroll
-      for(int i = 0; i < MAXITEMS; i++)
-      {
-         itemTab[5 * i] = int16_t(cols.first[i]);
-         itemTab[5 * i + 1] = int16_t(cols.count[i]);
-#pragma unroll
-         for(int j = 0; j < 3; j++) itemTab[5 * i + 2 + j] = int16_t(cols.bOff[i][j]);
+         uint16_t* r = recTab + REC * i;
+         const int c0 = cols.first[i], m = cols.count[i];
+         for(int k = 0; k < REC; k++) r[k] = 0;
+         r[Rec::FIRST] = uint16_t(c0);
+         r[Rec::COUNT] = uint16_t(m);
+         for(int j = 0; j < NP; j++)
+         {
+            r[Rec::BOFF + j] = uint16_t(cols.bOff[i][j]);
+            if(j < m)
+               for(int ks = 0; ks < KPC; ks++) r[Rec::NCOL + KPC * j + ks] = uint16_t(cols.n[(c0 + j) * KPC + ks]);
+         }
+         if(m == 1)
+            for(int ks = 0; ks < KPC; ks++) r[Rec::NCOR + ks] = uint16_t(cols.nc[c0 * KPC + ks]);
       }
    }
    if(tid == 0)
@@ -605,21 +634,16 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          DrainSchedule sched(nOff, drainEvery, drainFar);
          PipeCursor cur;
          int sinceDrain = 0;
+         // item records are read one item ahead: the loads land while the thread waits for the stages
+         Rec next;
+         next.load(rec4, 0);
          for(int it = 0; it < nItems; it++, cur.next(NA, NB, nPer))
          {
-            // the item's chunks, its operator slots and their output widths per K step, read before the wait
-            const int c0 = itemTab[5 * cur.c], m = itemTab[5 * cur.c + 1];
-            int bo[NP];
-#pragma unroll
-            for(int j = 0; j < NP; j++) bo[j] = itemTab[5 * cur.c + 2 + j];
-            int nColK[NP][KCH / KS], nCorK[KCH / KS];
-#pragma unroll
-            for(int j = 0; j < NP; j++)
-#pragma unroll
-               for(int ks = 0; ks < KCH / KS; ks++)
-                  nColK[j][ks] = j < m ? colTab[(c0 + j) * (KCH / KS) + ks] : 0;
-#pragma unroll
-            for(int ks = 0; ks < KCH / KS; ks++) nCorK[ks] = m == 1 ? corTab[c0 * (KCH / KS) + ks] : 0;
+            const Rec rc = next;
+            {
+               next.load(rec4, cur.c + 1 == nPer ? 0 : cur.c + 1);
+            }
+            const int m = rc[Rec::COUNT];
             long long t0 = prof ? clock64() : 0;
             if(!mbarWait(fullBar0 + 8 * cur.sa, cur.pha, err, abortFlag, waitNs)) break;
             long long t1 = prof ? clock64() : 0;
@@ -643,18 +667,16 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             for(int j = 0; j < NP; j++)
             {
                if(j >= m) break;
-               // K steps of 16 that reach a coefficient < L (the last chunk is partly padding)
-               const int kSteps = min(KCH / KS, (L - (c0 + j) * KCH + KS - 1) / KS);
 #pragma unroll
-               for(int ks = 0; ks < KCH / KS; ks++)
+               for(int ks = 0; ks < KPC; ks++)
                {
-                  if(ks >= kSteps) break;
                   const uint32_t koff = ks * 32;
-                  // this K step's output columns in one MMA (<= 256) or two (256 + the rest); the
-                  // correction products over the first nCor of them (a chunk alone in its item: j = 0)
-                  const int nCol = nColK[j][ks];
+                  // this K step's output columns in one MMA (<= 256) or two (split at 256 or at the kept
+                  // tail); the correction products over the first nCor of them (a chunk alone: j = 0). K steps
+                  // past the last coefficient (the last chunk is partly padding) have no columns.
+                  const int nCol = rc[Rec::NCOL + KPC * j + ks];
                   if(nCol == 0) break;
-                  const int nCor = nCorK[ks];
+                  const int nCor = rc[Rec::NCOR + ks];
 #pragma unroll
                   for(int pass = 0; pass < NPASS; pass++)
                   {
@@ -667,7 +689,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                      const int pa = j + (NP == 1 ? 0 : (NP == 2 ? PA2[pass] : PA[pass]));
                      const int pb = j + (NP == 1 ? 0 : (NP == 2 ? PB2[pass] : PB[pass]));
                      const uint64_t da = dA + ((pa * aBytes + koff) >> 4);
-                     const uint64_t db = dB + uint64_t(bo[pb]) + (koff >> 4);
+                     const uint64_t db = dB + uint64_t(rc[Rec::BOFF + pb]) + (koff >> 4);
                      const uint32_t acc = firstMma ? 0u : 1u;
                      const uint32_t accT = keepTail ? (tailFirst ? 0u : 1u) : acc;
                      if constexpr(Lay::TF32)
@@ -748,7 +770,10 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
                if(!mbarWait(emptyBar0 + 8 * (prev % NA), (prev / NA) & 1, err, abortFlag, waitNs)) break;
             }
             if(prof) twe += clock64() - t0;
-            const int o = itemOffset[cur.oi], c0 = itemTab[5 * cur.c], m = itemTab[5 * cur.c + 1];
+            const int o = itemOffset[cur.oi];
+            Rec rc;
+            rc.load(rec4, cur.c);
+            const int c0 = rc[Rec::FIRST], m = rc[Rec::COUNT];
             const uint32_t dst = bRing + s * bStage;
             // only the operator rows (output columns) a chunk's widest K step uses: of the leading
             // piece for the hi * hi product, of the others for the correction products. A chunk alone
@@ -758,9 +783,8 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
 #pragma unroll
             for(int j = 0; j < NP; j++)
             {
-               const int g = (m == 1 ? c0 : c0 + j) * (KCH / KS);
-               bytes[j] = m == 1 ? uint32_t(j == 0 ? colTab[g] : corTab[g]) * Lay::RB
-                                 : (j < m ? uint32_t(colTab[g]) * Lay::RB : 0u);
+               bytes[j] = m == 1 ? uint32_t(j == 0 ? rc[Rec::NCOL] : rc[Rec::NCOR]) * Lay::RB
+                                 : uint32_t(rc[Rec::NCOL + KPC * j]) * Lay::RB;   // (0 for j >= m)
                tx += bytes[j];
             }
             mbarArriveExpectTx(opBar0 + 8 * s, tx);
@@ -769,7 +793,7 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
             {
                const uint8_t* src = m == 1 ? img + ((int64_t(o) * nChunks + c0) * NP + j) * bBytes
                                            : img + (int64_t(o) * nChunks + c0 + j) * NP * bBytes;
-               if(bytes[j]) bulkLoad(dst + 16u * uint32_t(itemTab[5 * cur.c + 2 + j]), src, bytes[j], opBar0 + 8 * s);
+               if(bytes[j]) bulkLoad(dst + 16u * uint32_t(rc[Rec::BOFF + j]), src, bytes[j], opBar0 + 8 * s);
             }
             issued = it + 1;
          }
@@ -984,12 +1008,14 @@ kM2LTc(const int* __restrict__ targets, int nTargets, const int* __restrict__ vt
          if(it >= NA && !mbarWait(emptyBar0 + 8 * s, cur.pha ^ 1, err, abortFlag, waitNs)) break;
          if(prof) twp += clock64() - t0;
          const uint32_t aSt = base + s * aStage;
-         const int c0 = itemTab[5 * c], m = itemTab[5 * c + 1];
+         Rec rc;
+         rc.load(rec4, c);
+         const int c0 = rc[Rec::FIRST], m = rc[Rec::COUNT];
          const uint8_t* rowp = Mbf + ((int64_t(src >= 0 ? src : 0) * 3 + comp) * NP) * Lp * Lay::ES;
          // a chunk alone: its pieces into the slots, the ones after the leading piece only when its first
          // (widest) K step has correction products; chunks sharing the stage: chunk c0 + j's leading
          // piece into slot j
-         const int nSlots = m == 1 ? (corTab[c0 * (KCH / Lay::KSTEP)] > 0 ? NP : 1) : m;
+         const int nSlots = m == 1 ? (rc[Rec::NCOR] > 0 ? NP : 1) : m;
 #pragma unroll
          for(int q = 0; q < PER / EPC; q++)
          {
