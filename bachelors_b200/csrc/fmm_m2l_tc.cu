@@ -263,9 +263,9 @@ __device__ __forceinline__ void tmemLd16(uint32_t addr, float* v)
 
 
 // Operand layout of one K chunk of KCW bf16 elements per row: 64 elements in 128-byte rows
-// (128-byte swizzle) or 32 elements in 64-byte rows (64-byte swizzle). A stage holds one chunk
-// of every piece of A (128 rows) and of T_o (N rows); the number of stages is what fits in
-// shared memory (2 with 64-wide chunks of two pieces at p = 16, 4 with 32-wide ones).
+// (128-byte swizzle) or 32 elements in 64-byte rows (64-byte swizzle). An A stage holds NP slots of
+// 128 rows, a B stage the operator rows of one pipeline item; the numbers of stages are what fits in
+// shared memory (three A and two B stages with 64-wide chunks of two pieces at p = 16).
 // ES: element bytes; KSTEP: K elements per MMA instruction (32 bytes for both element types).
 template <int KCW> struct Layout;
 template <> struct Layout<64>
