@@ -102,6 +102,7 @@ fmm_status Plan::init(const fmm_config& c)
    if(const char* e = getenv("FMM_TC_CORRLAM")) tcCorrLam = atoi(e);
    if(const char* e = getenv("FMM_TC_ASYNC")) tcAsyncArrive = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_PAIR")) tcPair = atoi(e) != 0;
+   if(const char* e = getenv("FMM_TREE_PERSISTENT")) treePersistent = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_KEEPTAIL")) tcKeepTail = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_PROF")) tcProf = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_CUTOFF")) cfg.m2l_tc_degree_cutoff = atoi(e);
@@ -142,7 +143,7 @@ void Plan::release()
    DevBuf* bufs[] = {&srcXYZb, &srcWb, &srcJb, &tgtXYZb, &rootb, &sKeys, &tKeys, &sIdx, &tIdx, &sPos, &sQ, &tPos,
                      &cubTmp, &scratch, &lvlBounds, &lvlCnt, &lvlOff, &p2pOff, &p2pList, &parList, &m2lTargets, &m2lKeys, &errb,
                      &mult, &local, &outB, &outA, &opM2M64, &opL2L64, &opM2L64, &opM2Mw, &opL2Lw, &opM2Lw, &opM2Lbf, &multBf, &tcCounters,
-                     &adjG, &adjOut, &tcPts, &tcOut, &srcSigmab, &nearCounts, &tcProfBuf, &curlTab, &vtabUp, &vtabDn, &l2lTargets, &l2lKeys, &opM2Mbf, &opL2Lbf};
+                     &adjG, &adjOut, &tcPts, &tcOut, &srcSigmab, &nearCounts, &tcProfBuf, &levelState, &curlTab, &vtabUp, &vtabDn, &l2lTargets, &l2lKeys, &opM2Mbf, &opL2Lbf};
    for(DevBuf* b : bufs) b->release();
    for(auto& b : nodeBufs) b.release();
    for(auto& b : listBufs) b.release();

@@ -224,6 +224,8 @@ struct Plan
                                          // (-1: every term the degree cutoff keeps; -2: 10)
    int tcDrainMode = 3;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1,
                                          // 3: as 2 with 32 more columns in the drain threads' registers
+   int treePersistent = 1;               // every tree level in one cooperative launch (kBuildLevels)
+   DevBuf levelState;                    // its barrier, work queues and level starts
    int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length
    int simtKc = 16;                      // its K chunk (16 or 32)
    int simtTiled = 1;                    // FP32 CUDA-core M2L: register-tiled kernel (0: the row-broadcast form)

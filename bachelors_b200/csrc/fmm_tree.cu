@@ -223,18 +223,15 @@ __device__ __forceinline__ int lowerBound(const uint64_t* __restrict__ keys, int
    return a;
 }
 
-// For nodes [a, b) of `level`: decide the split and find the 8 children's ranges.
-__global__ void kCountChildren(Tree t, int a, int b, int level, int maxLevel, int cap, int capT,
-                               const uint64_t* __restrict__ skeys, const uint64_t* __restrict__ tkeys, int* bounds,
-                               int* cnt)
+// Node i (the j-th of its level): decide the split and find the 8 children's ranges (bounds row j);
+// returns the number of non-empty children.
+__device__ int childBounds(Tree& t, int i, int j, int level, int maxLevel, int cap, int capT,
+                           const uint64_t* __restrict__ skeys, const uint64_t* __restrict__ tkeys, int* bounds)
 {
-   int i = a + blockIdx.x * blockDim.x + threadIdx.x;
-   if(i >= b) return;
-   int j = i - a;
    int s0 = t.s0[i], s1 = t.s1[i], t0 = t.t0[i], t1 = t.t1[i];
    t.child0[i] = -1;
    t.nchild[i] = 0;
-   if(!((s1 - s0 > cap || t1 - t0 > capT) && level < maxLevel)) { cnt[j] = 0; return; }
+   if(!((s1 - s0 > cap || t1 - t0 > capT) && level < maxLevel)) return 0;
    uint64_t key = t.key[i];
    int shift = 3 * (maxLevel - level - 1);
    int sb[9], tb[9];
@@ -254,27 +251,32 @@ __global__ void kCountChildren(Tree t, int a, int b, int level, int maxLevel, in
    }
    bounds[18 * j + 8] = s1;
    bounds[18 * j + 17] = t1;
-   cnt[j] = k;
+   return k;
 }
 
-__global__ void kMakeChildren(Tree t, int a, int b, int level, int next, const int* __restrict__ bounds,
-                              const int* __restrict__ cnt, const int* __restrict__ off)
+// For nodes [a, b) of `level`: decide the split and find the 8 children's ranges.
+__global__ void kCountChildren(Tree t, int a, int b, int level, int maxLevel, int cap, int capT,
+                               const uint64_t* __restrict__ skeys, const uint64_t* __restrict__ tkeys, int* bounds,
+                               int* cnt)
 {
    int i = a + blockIdx.x * blockDim.x + threadIdx.x;
    if(i >= b) return;
-   int j = i - a;
-   if(cnt[j] == 0) return;
-   int c0 = next + off[j];
+   cnt[i - a] = childBounds(t, i, i - a, level, maxLevel, cap, capT, skeys, tkeys, bounds);
+}
+
+// The k children of node i (the j-th of its level), numbered from c0.
+__device__ void makeChildrenOf(Tree& t, int i, int j, int level, int c0, int k, const int* __restrict__ bounds)
+{
    t.child0[i] = c0;
-   t.nchild[i] = cnt[j];
+   t.nchild[i] = k;
    const int* sb = bounds + 18 * j;
    const int* tb = sb + 9;
    uint64_t key = t.key[i];
-   int k = 0;
+   int n = 0;
    for(int c = 0; c < 8; c++)
    {
       if(sb[c + 1] - sb[c] + tb[c + 1] - tb[c] == 0) continue;
-      int ch = c0 + k++;
+      int ch = c0 + n++;
       t.key[ch] = (key << 3) | uint64_t(c);
       t.level[ch] = level + 1;
       t.ix[ch] = 2 * t.ix[i] + (c & 1);
@@ -286,6 +288,183 @@ __global__ void kMakeChildren(Tree t, int a, int b, int level, int next, const i
       t.child0[ch] = -1;
       t.nchild[ch] = 0;
    }
+}
+
+__global__ void kMakeChildren(Tree t, int a, int b, int level, int next, const int* __restrict__ bounds,
+                              const int* __restrict__ cnt, const int* __restrict__ off)
+{
+   int i = a + blockIdx.x * blockDim.x + threadIdx.x;
+   if(i >= b) return;
+   int j = i - a;
+   if(cnt[j] == 0) return;
+   makeChildrenOf(t, i, j, level, next + off[j], cnt[j], bounds);
+}
+
+// ------------------------------------------------------------------------------ persistent level build
+// All levels in one cooperative launch (every block resident). Per level the blocks take work items of LB_T
+// consecutive nodes from the level's queue (an atomic counter, so items start in order). An item counts its
+// nodes' children, publishes its total, finds the children numbered before it by a decoupled look-back over
+// the items before it (each has already published at least its own total), and builds its children at once.
+// One grid barrier per level; the last item publishes the next level's range, and the host reads the level
+// starts once, after the launch, instead of once per level.
+constexpr int LB_T = 256;
+
+struct LevelBuildState
+{
+   unsigned bar[64];             // grid barrier: arrivals in bar[0], generation in bar[32] (another cache line)
+   int grab[MAXLEVEL];           // per level: next work item
+   int levelStart[MAXLEVEL + 2];
+   int nLevels;
+   int overflow;                 // a level did not fit in the node arrays
+};
+
+__device__ __forceinline__ int ldAcquire(const int* p)
+{
+   int v;
+   asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+   return v;
+}
+__device__ __forceinline__ unsigned ldAcquireU(const unsigned* p)
+{
+   unsigned v;
+   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+   return v;
+}
+__device__ __forceinline__ unsigned long long ldAcquireU64(const unsigned long long* p)
+{
+   unsigned long long v;
+   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+   return v;
+}
+__device__ __forceinline__ void stReleaseU64(unsigned long long* p, unsigned long long v)
+{
+   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t treeTimer()
+{
+   uint64_t t;
+   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+   return t;
+}
+
+// Grid barrier of a cooperative launch: arrivals in bar[0], generation in bar[32] (its own cache line, so the
+// waiting blocks' polls do not contend with the arrivals). Bounded: a block that waits longer than limitNs
+// raises ERR_TIMEOUT and every thread of it returns false.
+__device__ bool gridBarrier(unsigned* bar, int* err, uint64_t limitNs)
+{
+   __shared__ int ok;
+   __syncthreads();
+   if(threadIdx.x == 0)
+   {
+      ok = 1;
+      const unsigned g = ldAcquireU(bar + 32);
+      __threadfence();
+      if(atomicAdd(bar, 1u) == gridDim.x - 1)
+      {
+         atomicExch(bar, 0u);
+         __threadfence();
+         atomicAdd(bar + 32, 1u);
+      }
+      else
+      {
+         const uint64_t t0 = treeTimer();
+         while(ldAcquireU(bar + 32) == g)
+         {
+            if(treeTimer() - t0 > limitNs)
+            {
+               atomicOr(err, ERR_TIMEOUT);
+               ok = 0;
+               break;
+            }
+            __nanosleep(200);
+         }
+      }
+      __threadfence();
+   }
+   __syncthreads();
+   return ok != 0;
+}
+
+// Look-back words, one per work item: (level + 1) << 40 | state << 32 | value, state 1 = the item's own
+// total, 2 = its total plus everything before it; a word of another level reads as "not yet".
+__device__ __forceinline__ unsigned long long lbWord(int level, int state, int value)
+{
+   return (unsigned long long)(level + 1) << 40 | (unsigned long long)state << 32 | unsigned(value);
+}
+
+__global__ void __launch_bounds__(LB_T, 6) kBuildLevels(Tree t, int maxLevel, int cap, int capT,
+                                                        const uint64_t* __restrict__ skeys,
+                                                        const uint64_t* __restrict__ tkeys, int* bounds,
+                                                        unsigned long long* look, int64_t capNodes,
+                                                        LevelBuildState* S, int* err, uint64_t limitNs)
+{
+   typedef cub::BlockScan<int, LB_T> Scan;
+   __shared__ typename Scan::TempStorage scanTmp;
+   __shared__ int item, before, failed;
+   const int tid = threadIdx.x;
+   int nLev = 1;
+   if(tid == 0) failed = 0;
+   for(int level = 0; level < maxLevel; level++)
+   {
+      const int a = ldAcquire(&S->levelStart[level]), b = ldAcquire(&S->levelStart[level + 1]);
+      if(b <= a) break;
+      const int nItems = (b - a + LB_T - 1) / LB_T;
+      while(true)
+      {
+         if(tid == 0) item = atomicAdd(&S->grab[level], 1);
+         __syncthreads();
+         const int it = item;
+         if(it >= nItems) break;
+         const int i = a + it * LB_T + tid;
+         const int k = i < b ? childBounds(t, i, i - a, level, maxLevel, cap, capT, skeys, tkeys, bounds) : 0;
+         int ex, total;
+         Scan(scanTmp).ExclusiveSum(k, ex, total);
+         if(tid == 0)
+         {
+            // publish this item's total, then add up the items before it
+            int sum = 0;
+            if(it == 0) stReleaseU64(&look[0], lbWord(level, 2, total));
+            else
+            {
+               stReleaseU64(&look[it], lbWord(level, 1, total));
+               const uint64_t t0 = treeTimer();
+               for(int j = it - 1; j >= 0;)
+               {
+                  const unsigned long long w = ldAcquireU64(&look[j]);
+                  const int st = int(w >> 32) & 0xFF;
+                  if(int(w >> 40) == level + 1 && st != 0)
+                  {
+                     sum += int(unsigned(w));
+                     if(st == 2) break;
+                     j--;
+                     continue;
+                  }
+                  if(treeTimer() - t0 > limitNs)
+                  {
+                     atomicOr(err, ERR_TIMEOUT);
+                     failed = 1;
+                     break;
+                  }
+               }
+               stReleaseU64(&look[it], lbWord(level, 2, sum + total));
+            }
+            before = sum;
+            // children that would not fit are not built; the host grows the arrays and builds again
+            if(int64_t(b) + sum + total > capNodes) S->overflow = 1;
+            if(it == nItems - 1) S->levelStart[level + 2] = int(std::min<int64_t>(int64_t(b) + sum + total, capNodes));
+         }
+         __syncthreads();
+         const int64_t c0 = int64_t(b) + before + ex;
+         if(k > 0 && c0 + k <= capNodes) makeChildrenOf(t, i, i - a, level, int(c0), k, bounds);
+         __syncthreads();
+      }
+      if(!gridBarrier(S->bar, err, limitNs) || failed) return;
+      if(ldAcquire(&S->overflow)) break;
+      const int nb = ldAcquire(&S->levelStart[level + 2]);
+      if(nb == b) break;   // no children: the tree ends here
+      nLev = level + 2;
+   }
+   if(blockIdx.x == 0 && tid == 0) S->nLevels = nLev;
 }
 
 // ------------------------------------------------------------------------------ lists
@@ -523,6 +702,78 @@ __global__ void kL2LLevelStarts(const unsigned* __restrict__ keys, int n, int nL
 }
 
 // ------------------------------------------------------------------------------ host driver
+__global__ void kInitLevelState(LevelBuildState* S, int nRoots)
+{
+   const int i = threadIdx.x;
+   S->bar[i] = 0;
+   if(i < MAXLEVEL) S->grab[i] = 0;
+   if(i < MAXLEVEL + 2) S->levelStart[i] = i == 1 ? nRoots : 0;
+   if(i == 0)
+   {
+      S->nLevels = 0;
+      S->overflow = 0;
+   }
+}
+
+// Every level of the forest in one cooperative launch (kBuildLevels), the node arrays grown and the build
+// repeated when a level would not fit; one host wait for the level starts.
+static fmm_status buildLevelsPersistent(Plan& P, cudaStream_t st, int64_t& capNodes, int K, const int* dSrcOff,
+                                        const int* dTgtOff, const uint64_t* sk, const uint64_t* tk, int capS, int capT,
+                                        int& nLevels, int64_t& total)
+{
+   int dev = 0, nSM = 0, perSM = 0;
+   FMM_CUDA(cudaGetDevice(&dev));
+   FMM_CUDA(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev));
+   FMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kBuildLevels, LB_T, 0));
+   if(perSM < 1) return setError(FMM_E_CUDA, "kBuildLevels: no resident block");
+   // up to 4 blocks per SM (measured: the batch's level build took 10.3 ms of tree phase with 4, 10.4 with all
+   // 6 resident)
+   const int grid = nSM * std::min(perSM, 4);
+   FMM_TRY(P.levelState.reserve(sizeof(LevelBuildState)));
+   LevelBuildState* S = (LevelBuildState*)P.levelState.ptr;
+   for(int attempt = 0; attempt < 8; attempt++)
+   {
+      FMM_TRY(P.ensureNodes(capNodes, st));
+      Tree& t = P.tree;
+      FMM_TRY(P.lvlBounds.reserve(sizeof(int) * 18 * size_t(capNodes)));
+      // look-back words of every item of a level (levels never hold more than capNodes nodes); a word
+      // carries its level, so the words of one level never pass for another's
+      FMM_TRY(P.lvlOff.reserve(sizeof(unsigned long long) * size_t(capNodes / LB_T + 2)));
+      FMM_CUDA(cudaMemsetAsync(P.lvlOff.ptr, 0, sizeof(unsigned long long) * size_t(capNodes / LB_T + 2), st));
+      kInitRoots<<<(K + 255) / 256, 256, 0, st>>>(t, K, dSrcOff, dTgtOff);
+      FMM_TRY(launched(P, "kInitRoots", st));
+      kInitLevelState<<<1, 64, 0, st>>>(S, K);
+      FMM_TRY(launched(P, "kInitLevelState", st));
+      FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+      int maxLevel = P.maxLevel;
+      int* bounds = (int*)P.lvlBounds.ptr;
+      unsigned long long* look = (unsigned long long*)P.lvlOff.ptr;
+      int* err = P.err;
+      uint64_t limit = P.tcWaitNs;
+      void* args[] = {&t, &maxLevel, &capS, &capT, &sk, &tk, &bounds, &look, &capNodes, &S, &err, &limit};
+      FMM_CUDA(cudaLaunchCooperativeKernel((const void*)kBuildLevels, dim3(grid), dim3(LB_T), args, 0, st));
+      FMM_TRY(launched(P, "kBuildLevels", st));
+      LevelBuildState h;
+      int herr = 0;
+      FMM_CUDA(cudaMemcpyAsync(&h, S, sizeof(h), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+      FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+      if(herr & ERR_TIMEOUT) return setError(FMM_E_TIMEOUT, "kBuildLevels: a grid barrier timed out");
+      if(h.overflow)
+      {
+         // (the arrays keep the grown size, so later builds of this plan start from it)
+         capNodes *= 2;
+         continue;
+      }
+      nLevels = h.nLevels;
+      for(int l = 0; l <= nLevels; l++) t.levelStart[l] = h.levelStart[l];
+      total = h.levelStart[nLevels];
+      return FMM_OK;
+   }
+   return setError(FMM_E_LIMIT, "kBuildLevels: node capacity did not converge");
+}
+
 template <class T>
 fmm_status buildTreeT(Plan& P, cudaStream_t st)
 {
@@ -624,16 +875,33 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    }
    FMM_CHECK_LAUNCH();
 
-   // nodes, level by level
+   // nodes, level by level (at least the capacity an earlier build of this plan grew to)
    int64_t capNodes = std::max<int64_t>(1024, 2 * (n + m) / std::max(1, P.cfg.leaf_capacity) + 64 + 2 * K);
+   capNodes = std::max<int64_t>(capNodes, P.nodeCap);
    FMM_TRY(P.ensureNodes(capNodes));
    Tree& t = P.tree;
+   const int capS = P.cfg.leaf_capacity;
+   const int capT = P.cfg.target_leaf_capacity > 0 ? P.cfg.target_leaf_capacity : P.cfg.leaf_capacity;
+   int nLevels = 1;
+   int64_t total = K;
+   bool built = false;
+   if(P.treePersistent)
+   {
+      int coop = 0, dev = 0;
+      FMM_CUDA(cudaGetDevice(&dev));
+      FMM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+      if(coop)
+      {
+         FMM_TRY(buildLevelsPersistent(P, st, capNodes, K, dSrcOff, dTgtOff, sk, tk, capS, capT, nLevels, total));
+         built = true;
+      }
+   }
+   if(!built)
+   {
    kInitRoots<<<(K + 255) / 256, 256, 0, st>>>(t, K, dSrcOff, dTgtOff);
    FMM_TRY(launched(P, "kInitRoots", st));
    t.levelStart[0] = 0;
    t.levelStart[1] = K;
-   int nLevels = 1;
-   int64_t total = K;
    for(int level = 0; level < P.maxLevel; level++)
    {
       int a = t.levelStart[level], b = t.levelStart[level + 1];
@@ -645,9 +913,8 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       int* bounds = (int*)P.lvlBounds.ptr;
       int* cc = (int*)P.lvlCnt.ptr;
       int* off = (int*)P.lvlOff.ptr;
-      kCountChildren<<<(cnt + threads - 1) / threads, threads, 0, st>>>(
-         t, a, b, level, P.maxLevel, P.cfg.leaf_capacity,
-         P.cfg.target_leaf_capacity > 0 ? P.cfg.target_leaf_capacity : P.cfg.leaf_capacity, sk, tk, bounds, cc);
+      kCountChildren<<<(cnt + threads - 1) / threads, threads, 0, st>>>(t, a, b, level, P.maxLevel, capS, capT, sk, tk,
+                                                                        bounds, cc);
       FMM_TRY(launched(P, "kCountChildren", st));
       FMM_CHECK_LAUNCH();
       tmp = 0;
@@ -673,6 +940,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       total += nextCount;
       t.levelStart[level + 2] = int(total);
       nLevels = level + 2;
+   }
    }
    t.nNodes = total;
    t.nLevels = nLevels;
