@@ -107,7 +107,7 @@ fmm_status Plan::init(const fmm_config& c)
    if(const char* e = getenv("FMM_TC_PROF")) tcProf = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_CUTOFF")) cfg.m2l_tc_degree_cutoff = atoi(e);
    if(const char* e = getenv("FMM_TC_DRAINMODE")) tcDrainMode = std::min(3, std::max(0, atoi(e)));
-   if(const char* e = getenv("FMM_TC_GROUP")) tcGroupByCount = atoi(e) != 0;
+   if(const char* e = getenv("FMM_TC_GROUP")) tcGroup = std::min(2, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_L2P_SPLIT")) l2pSplit = atoi(e) != 0;
    if(const char* e = getenv("FMM_SIMT_TILED")) simtTiled = std::min(2, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_SIMT_KC")) simtKc = atoi(e) == 32 ? 32 : 16;

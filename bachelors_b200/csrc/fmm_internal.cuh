@@ -226,7 +226,8 @@ struct Plan
                                          // 3: as 2 with 32 more columns in the drain threads' registers
    int treePersistent = 1;               // every tree level in one cooperative launch (kBuildLevels)
    DevBuf levelState;                    // its barrier, work queues and level starts
-   int tcGroupByCount = 0;               // M2L target boxes grouped by octant, then by list length
+   int tcGroup = 2;                      // M2L target boxes grouped by octant, then 0: in node order,
+                                         // 1: by list length, 2: by partner pattern (rarest offsets first)
    int simtKc = 16;                      // its K chunk (16 or 32)
    int simtTiled = 1;                    // FP32 CUDA-core M2L: register-tiled kernel (0: the row-broadcast form)
    int l2pSplit = 1;                     // 1: L2P in kL2PWarp, then the near field; 0: both in kL2PNear

@@ -647,6 +647,113 @@ __global__ void kM2LTargetKeys(Tree t, Lists L, int nNodes, int byCount, unsigne
    if(has) atomicAdd(count, 1);
 }
 
+// M2L target order by partner pattern: a tile's cost is the number of offsets any of its 42 boxes has a
+// partner at, so boxes with similar sets of offsets should share tiles. The key of a box is its octant, then
+// its offset bits with the rarest offsets first (the most telling ones): offsets counted over all boxes
+// (kOffsetCounts), ranked in one block (kOffsetRanks), and each box's bits of ranks 0-60 and 61-124 packed
+// into two 64-bit words (kM2LMaskKeys) that two stable radix sorts order (word 1, then word 0).
+__global__ void kOffsetCounts(Lists L, int nNodes, unsigned* counts)
+{
+   // one warp per box row at a time: the row's 316 entries as 10 coalesced loads in flight; lane l counts
+   // offsets l + 32 k in registers and adds them to the totals once
+   const int lane = threadIdx.x & 31;
+   const int warp = int((blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5);
+   const int nWarps = int((int64_t(gridDim.x) * blockDim.x) >> 5);
+   unsigned c[10];
+#pragma unroll
+   for(int k = 0; k < 10; k++) c[k] = 0;
+   for(int i = warp; i < nNodes; i += nWarps)
+   {
+      const int* vt = L.vtab + int64_t(i) * 316;
+      int v[10];
+#pragma unroll
+      for(int k = 0; k < 10; k++) v[k] = lane + 32 * k < 316 ? vt[lane + 32 * k] : -1;
+#pragma unroll
+      for(int k = 0; k < 10; k++) c[k] += v[k] >= 0 ? 1u : 0u;
+   }
+#pragma unroll
+   for(int k = 0; k < 10; k++)
+      if(lane + 32 * k < 316 && c[k]) atomicAdd(&counts[lane + 32 * k], c[k]);
+}
+// rank[o]: the position of offset o in increasing count order (ties by index); one block of 320 threads
+__global__ void kOffsetRanks(const unsigned* __restrict__ counts, int* rank)
+{
+   const int o = threadIdx.x;
+   if(o >= 316) return;
+   const unsigned c = counts[o];
+   int r = 0;
+   for(int q = 0; q < 316; q++)
+   {
+      const unsigned d = counts[q];
+      r += (d < c || (d == c && q < o)) ? 1 : 0;
+   }
+   rank[o] = r;
+}
+// word 0: octant (bits 63..61), ranks 0..60 (bits 60..0); word 1: ranks 61..124 (bits 63..0). Boxes without
+// M2L partners sort last. A warp per box at a time (grid-stride): the lanes read the box's table row together
+// (10 coalesced loads in flight) and OR their bits into the two words; the boxes with partners are counted
+// per block, one atomic each.
+__global__ void kM2LMaskKeys(Tree t, Lists L, int nNodes, const int* __restrict__ rank, unsigned long long* k0,
+                             unsigned long long* k1, int* vals, int* count)
+{
+   __shared__ int rk[316];
+   __shared__ int blockCount;
+   for(int o = threadIdx.x; o < 316; o += blockDim.x) rk[o] = rank[o];
+   if(threadIdx.x == 0) blockCount = 0;
+   __syncthreads();
+   const int lane = threadIdx.x & 31;
+   const int warp = int((blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5);
+   const int nWarps = int((int64_t(gridDim.x) * blockDim.x) >> 5);
+   int mine = 0;
+   for(int i = warp; i < nNodes; i += nWarps)
+   {
+      if(L.nv[i] <= 0)
+      {
+         if(lane == 0)
+         {
+            vals[i] = i;
+            k0[i] = ~0ull;
+            k1[i] = ~0ull;
+         }
+         continue;
+      }
+      unsigned long long w0 = 0, w1 = 0;
+      const int* vt = L.vtab + int64_t(i) * 316;
+      int v[10];
+#pragma unroll
+      for(int k = 0; k < 10; k++) v[k] = lane + 32 * k < 316 ? vt[lane + 32 * k] : -1;
+#pragma unroll
+      for(int k = 0; k < 10; k++)
+      {
+         if(v[k] < 0) continue;
+         const int r = rk[lane + 32 * k];
+         if(r < 61) w0 |= 1ull << (60 - r);
+         else if(r < 125) w1 |= 1ull << (124 - r);
+      }
+      for(int d = 16; d > 0; d >>= 1)
+      {
+         w0 |= __shfl_xor_sync(0xffffffffu, w0, d);
+         w1 |= __shfl_xor_sync(0xffffffffu, w1, d);
+      }
+      if(lane == 0)
+      {
+         mine++;
+         vals[i] = i;
+         k0[i] = w0 | (unsigned long long)(t.key[i] & 7) << 61;
+         k1[i] = w1;
+      }
+   }
+   if(lane == 0 && mine) atomicAdd(&blockCount, mine);
+   __syncthreads();
+   if(threadIdx.x == 0 && blockCount) atomicAdd(count, blockCount);
+}
+__global__ void kGatherKeys(const unsigned long long* __restrict__ k0, const int* __restrict__ order, int n,
+                            unsigned long long* out)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if(i < n) out[i] = k0[order[i]];
+}
+
 // Nodes with children, compacted in node order (so each level's parents are contiguous), and the
 // compacted index where each level starts.
 __global__ void kParentFlags(Tree t, int nNodes, int* flags)
@@ -1023,14 +1130,54 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       FMM_CUDA(cudaMemcpyAsync(P.parStart.data(), P.scratch.ptr, sizeof(int) * (nLevels + 1), cudaMemcpyDeviceToHost, st));
       FMM_CUDA(cudaStreamSynchronize(st));
    }
-   // M2L targets grouped by octant
+   // M2L targets grouped by octant, then (tcGroup 2) by partner pattern
+   if(P.tcGroup == 2)
+   {
+      FMM_TRY(P.m2lTargets.reserve(2 * sizeof(int) * nn));
+      // three key arrays of nn words (word 0, word 1, word 0 in word-1 order), sorted copies, and the
+      // offset counts and ranks
+      FMM_TRY(P.m2lKeys.reserve(sizeof(unsigned long long) * (4 * size_t(nn) + 2) + 2 * sizeof(int) * 320));
+      unsigned long long* k0 = (unsigned long long*)P.m2lKeys.ptr;
+      unsigned long long* k1 = k0 + nn;
+      unsigned long long* k2 = k1 + nn;
+      unsigned long long* k3 = k2 + nn;
+      unsigned* counts = (unsigned*)(k3 + nn + 2);
+      int* rank = (int*)(counts + 320);
+      int* vv = (int*)P.m2lTargets.ptr;
+      FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+      FMM_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned) * 320, st));
+      kOffsetCounts<<<148 * 4, 256, 0, st>>>(Ls, nn, counts);
+      FMM_TRY(launched(P, "kOffsetCounts", st));
+      kOffsetRanks<<<1, 320, 0, st>>>(counts, rank);
+      FMM_TRY(launched(P, "kOffsetRanks", st));
+      kM2LMaskKeys<<<148 * 8, 256, 0, st>>>(t, Ls, nn, rank, k0, k1, vv + nn, P.err);
+      FMM_TRY(launched(P, "kM2LMaskKeys", st));
+      // stable LSD order: by word 1, then by word 0
+      tmp = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, tmp, k1, k3, vv + nn, vv, nn, 0, 64, st);
+      FMM_TRY(P.cubTmp.reserve(tmp));
+      tmp = P.cubTmp.bytes;
+      FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, k1, k3, vv + nn, vv, nn, 0, 64, st));
+      kGatherKeys<<<(nn + 255) / 256, 256, 0, st>>>(k0, vv, nn, k2);
+      FMM_TRY(launched(P, "kGatherKeys", st));
+      tmp = P.cubTmp.bytes;
+      FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, k2, k3, vv, vv + nn, nn, 0, 64, st));
+      // the final order is in vv + nn: move it to the front
+      FMM_CUDA(cudaMemcpyAsync(vv, vv + nn, sizeof(int) * nn, cudaMemcpyDeviceToDevice, st));
+      int cntT = 0;
+      FMM_CUDA(cudaMemcpyAsync(&cntT, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      FMM_CUDA(cudaStreamSynchronize(st));
+      P.nM2LTargets = cntT;
+      FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
+   }
+   else
    {
       FMM_TRY(P.m2lTargets.reserve(2 * sizeof(int) * nn));
       FMM_TRY(P.m2lKeys.reserve(2 * sizeof(unsigned) * nn));
       unsigned* kk = (unsigned*)P.m2lKeys.ptr;
       int* vv = (int*)P.m2lTargets.ptr;
       FMM_CUDA(cudaMemsetAsync(P.err, 0, sizeof(int), st));
-      kM2LTargetKeys<<<(nn + 255) / 256, 256, 0, st>>>(t, Ls, nn, P.tcGroupByCount, kk + nn, vv + nn, P.err);
+      kM2LTargetKeys<<<(nn + 255) / 256, 256, 0, st>>>(t, Ls, nn, P.tcGroup == 1, kk + nn, vv + nn, P.err);
       FMM_TRY(launched(P, "kM2LTargetKeys", st));
       tmp = 0;
       cub::DeviceRadixSort::SortPairs(nullptr, tmp, kk + nn, kk, vv + nn, vv, nn, 0, 13, st);
