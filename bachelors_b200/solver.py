@@ -19,6 +19,7 @@ inputs are copied through host memory and results are numpy arrays.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from enum import IntEnum
 
 import numpy as np
@@ -113,6 +114,7 @@ class Plan:
         _lib.check(self.lib.fmm_plan_create(ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h
         self._keep = []
+        self._pinned = []   # page-locked result buffers: [torch tensor, weakref to the array handed out]
         self.device_mode = False
         self.m = 0
         # bumped whenever the plan's inputs change (sources, targets, strengths, coils), so a caller
@@ -123,6 +125,7 @@ class Plan:
         if getattr(self, "handle", None):
             self.lib.fmm_plan_destroy(self.handle)
             self.handle = None
+        self._pinned = []
 
     def __del__(self):
         try:
@@ -181,9 +184,22 @@ class Plan:
         if self.device_mode:
             return torch.empty((rows, 3), dtype=self.torch_dtype, device=f"cuda:{self.cfg.device}")
         if torch is not None and torch.cuda.is_available():
-            # page-locked host memory from torch's caching host allocator: the device-to-host copy
-            # runs at full DMA speed, and a result's block is reused once the array is released
-            return torch.empty((rows, 3), dtype=self.torch_dtype, pin_memory=True).numpy()
+            # page-locked host memory, so that the device-to-host copy runs at full DMA speed. Page-locking a
+            # large block costs ~0.1 s (201 MB); torch's host allocator keeps only a freed block, so while the
+            # caller still holds the previous result every other solve paid it. The plan keeps its own few
+            # buffers and reuses one once the array it handed out (and every view of it) is gone.
+            shape = (rows, 3)
+            for entry in self._pinned:
+                t, ref = entry
+                if tuple(t.shape) == shape and t.dtype == self.torch_dtype and (ref is None or ref() is None):
+                    arr = t.numpy()
+                    entry[1] = weakref.ref(arr)
+                    return arr
+            t = torch.empty(shape, dtype=self.torch_dtype, pin_memory=True)
+            arr = t.numpy()
+            if len(self._pinned) < 4:
+                self._pinned.append([t, weakref.ref(arr)])
+            return arr
         return np.empty((rows, 3), dtype=self.np_dtype)
 
     @staticmethod
