@@ -42,9 +42,9 @@ METRIC = "B evals/s (N=2^24, p=16) split-BF16 vs FP32 FMM at rel err<=1e-6; adjo
 UNIT = "target-evals/s"
 SEED = 20260002
 # DRAM bytes (read + write) per M2L pair of the tensor-core M2L, from an ncu capture of the
-# 128 x 32 x 64 torus at p = 16 (405.6 MB read + 54.4 MB written for 1,271,544 pairs;
+# 128 x 32 x 64 torus at p = 16 (536.6 MB read + 54.2 MB written for 1,271,544 pairs;
 # profiles/m2l_tc_bf16x3_torus2e18_p16.md)
-M2L_DRAM_BYTES_PER_PAIR = 460.03e6 / 1271544
+M2L_DRAM_BYTES_PER_PAIR = 590.78e6 / 1271544
 # bounded CPU samples of the same workload family (torus points, targets = sources): 32 x 8 x 8 = 2,048 for
 # each step of the reference arm (25 steps stay within a few minutes), 32 x 8 x 16 = 4,096 for the main
 # line's cpu_baseline (~15 s)
@@ -562,7 +562,7 @@ def main():
                      "frac_sustained": achieved / bf16_sustained, "peak_sustained": bf16_sustained,
                      "traffic": M2L_DRAM_BYTES_PER_PAIR * st["v_pairs"] if m2l == "bf16x3" else None,
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the "
-                                       "kernel on the 128x32x64 torus (362 B per M2L pair), scaled by the pairs "
+                                       "kernel on the 128x32x64 torus (465 B per M2L pair), scaled by the pairs "
                                        "of this launch",
                      "flops_per_launch": flops_m2l, "flops_per_pair": per_pair,
                      "dense_equiv_flops_per_launch": flops_dense,
