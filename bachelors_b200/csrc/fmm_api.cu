@@ -332,6 +332,7 @@ fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const
    if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
    P.bem = false;
    P.n = n;
+   P.tgtIsSrc = false;
    P.treeReady = P.upReady = P.downReady = false;
    P.dropGraph();
    return FMM_OK;
@@ -355,6 +356,7 @@ fmm_status fmm_set_bem_sources(fmm_plan* plan, const void* xyz, const void* w, c
    P.srcJ = P.srcJb.ptr;
    P.srcSigma = P.srcSigmab.ptr;
    P.n = n;
+   P.tgtIsSrc = false;
    P.hasJ = true;
    P.bem = true;
    // B and the normals (staged when on the host) become J = B x n and sigma = B . n
@@ -399,6 +401,7 @@ fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_de
    FMM_TRY(copyIn(P.tgtXYZb, xyz, es * 3 * m, on_device, st, &P.tgtXYZ));
    if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
    P.m = m;
+   P.tgtIsSrc = false;
    P.treeReady = P.upReady = P.downReady = false;
    P.dropGraph();
    return FMM_OK;
@@ -417,6 +420,7 @@ fmm_status fmm_set_targets_to_sources(fmm_plan* plan, void* stream)
    if(bytes) FMM_CUDA(cudaMemcpyAsync(P.tgtXYZb.ptr, P.srcXYZ, bytes, cudaMemcpyDeviceToDevice, st));
    P.tgtXYZ = P.tgtXYZb.ptr;
    P.m = P.n;
+   P.tgtIsSrc = true;
    P.treeReady = P.upReady = P.downReady = false;
    P.dropGraph();
    return FMM_OK;

@@ -945,7 +945,10 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
                                                                 P.maxLevel, sk + n, si + n);
       FMM_TRY(launched(P, "kKeys", st));
    }
-   if(m) {
+   // targets that are the sources (fmm_set_targets_to_sources, one coil): their keys, order and sorted
+   // positions are the sources', copied instead of computed and sorted again
+   const bool same = P.tgtIsSrc && K == 1 && m == n && !P.bem;
+   if(m && !same) {
       kKeys<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, m, P.root, dTgtOff, K,
                                                                 P.maxLevel, tk + m, ti + m);
       FMM_TRY(launched(P, "kKeys", st));
@@ -961,7 +964,12 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    tmp = P.cubTmp.bytes;
    if(n) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, sk + n, sk, si + n, si, int(n), 0, keyBits, st));
    tmp = P.cubTmp.bytes;
-   if(m) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, keyBits, st));
+   if(m && !same) FMM_CUDA(cub::DeviceRadixSort::SortPairs(P.cubTmp.ptr, tmp, tk + m, tk, ti + m, ti, int(m), 0, keyBits, st));
+   if(m && same)
+   {
+      FMM_CUDA(cudaMemcpyAsync(tk, sk, sizeof(uint64_t) * m, cudaMemcpyDeviceToDevice, st));
+      FMM_CUDA(cudaMemcpyAsync(ti, si, sizeof(int) * m, cudaMemcpyDeviceToDevice, st));
+   }
    if(P.debugSync) FMM_CUDA(cudaStreamSynchronize(st));
    // sorted point data
    typedef typename Vec4<T>::type V4;
@@ -976,7 +984,10 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
          (V4*)P.sQ.ptr);
       FMM_TRY(launched(P, "kGatherSources", st));
    }
-   if(m) {
+   if(m && same)
+      // (the sorted sources' (x, y, z, 0): the fourth lane is zero for sources that are not BEM sources)
+      FMM_CUDA(cudaMemcpyAsync(P.tPos.ptr, P.sPos.ptr, sizeof(V4) * m, cudaMemcpyDeviceToDevice, st));
+   else if(m) {
       kGatherTargets<T><<<(m + threads - 1) / threads, threads, 0, st>>>((const T*)P.tgtXYZ, ti, m, (V4*)P.tPos.ptr);
       FMM_TRY(launched(P, "kGatherTargets", st));
    }

@@ -44,3 +44,24 @@ def test_solver_with_points_is_quadratures_and_device_path():
     Bd = s2.solve(1.0, "B").cpu().numpy()
     s2.plan.close()
     np.testing.assert_array_equal(Bh, Bd)
+
+
+@pytest.mark.parametrize("m2l", ["bf16x3", "simt"])
+def test_targets_stay_the_copy_after_new_sources(m2l):
+    """The plan reuses the sources' sorted order for targets set by fmm_set_targets_to_sources; new sources set
+    afterwards leave the targets at the earlier points (the copy), as with explicit targets."""
+    xyz, w, J = (a.astype(np.float32) for a in G.torus(48, 16, 8, 2.0, 0.5))
+    xyz2 = (xyz * np.float32(1.1) + np.float32(0.05)).astype(np.float32)
+    a = Plan(order=8, leaf_capacity=32, precision="fp32", m2l=m2l)
+    a.set_sources(xyz, w, J)
+    a.set_targets_to_sources()
+    a.solve(1.0, 1)
+    a.set_sources(xyz2, w, J)
+    Ba, _ = a.solve(1.0, 1)
+    b = Plan(order=8, leaf_capacity=32, precision="fp32", m2l=m2l)
+    b.set_sources(xyz2, w, J)
+    b.set_targets(xyz)
+    Bb, _ = b.solve(1.0, 1)
+    np.testing.assert_array_equal(Ba, Bb)
+    a.close()
+    b.close()
