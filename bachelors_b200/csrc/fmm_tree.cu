@@ -543,6 +543,127 @@ __global__ void kListsLevel(Tree t, Lists L, int a, int b, int* err)
    L.nv[D] = nv;
 }
 
+// kListsLevel with one warp per node D: the lanes take the parent's colleagues (at most 27), their child counts
+// make a list of candidate slots (a leaf colleague is one slot, otherwise one per child), and each pass
+// classifies 32 candidates at once. Entries are appended by ballots in candidate order, so the colleague, A and
+// X lists come out exactly as in kListsLevel (the V table is indexed by offset).
+constexpr int LW_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * LW_WARPS) kListsLevelWarp(Tree t, Lists L, int a, int b, int* err)
+{
+   __shared__ int sC[LW_WARPS][32], sNc[LW_WARPS][32], sC0[LW_WARPS][32], sEx[LW_WARPS][33];
+   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+   const int D = a + blockIdx.x * LW_WARPS + w;
+   if(D >= b) return;
+   const int P = t.parent[D];
+   int* vt = L.vtab + int64_t(D) * 316;   // preset to -1 for the whole tree before the levels
+   const bool hasT = t.t1[D] > t.t0[D];
+   const unsigned below = (1u << lane) - 1u;
+   int ncol = 0, na = 0, nx = 0, nv = 0;
+   // append this lane's entry (if any) to a list in lane order; returns the list's new length
+   auto append = [&](bool has, int node, int* list, int cap, int count, int errBit) {
+      const unsigned m = __ballot_sync(0xffffffffu, has);
+      if(has)
+      {
+         const int pos = count + __popc(m & below);
+         if(pos < cap) list[pos] = node;
+         else atomicOr(err, errBit);
+      }
+      return count + __popc(m);
+   };
+   const int ncP = L.ncol[P];
+   int C = -1, nc = 0, c0 = 0;
+   if(lane < ncP)
+   {
+      C = L.col[int64_t(P) * COLCAP + lane];
+      nc = t.nchild[C];
+      c0 = t.child0[C];
+   }
+   const int slots = lane < ncP ? (nc > 0 ? nc : 1) : 0;
+   int incl = slots;
+   for(int d = 1; d < 32; d <<= 1)
+   {
+      const int v = __shfl_up_sync(0xffffffffu, incl, d);
+      if(lane >= d) incl += v;
+   }
+   const int total = __shfl_sync(0xffffffffu, incl, 31);
+   sC[w][lane] = C;
+   sNc[w][lane] = nc;
+   sC0[w][lane] = c0;
+   sEx[w][lane] = incl - slots;
+   if(lane == 0) sEx[w][32] = total;
+   __syncwarp();
+   int* colD = L.col + int64_t(D) * COLCAP;
+   int* aD = L.acoarse + int64_t(D) * ACAP;
+   int* xD = L.xl + int64_t(D) * XCAP;
+   for(int base = 0; base < total; base += 32)
+   {
+      const int q = base + lane;
+      bool isCol = false, isA = false, isX = false;
+      int node = -1;
+      if(q < total)
+      {
+         // the colleague owning slot q: the last lane j < ncP with sEx[j] <= q
+         int lo = 0, hi = ncP;
+         while(hi - lo > 1)
+         {
+            const int mid = (lo + hi) >> 1;
+            if(sEx[w][mid] <= q) lo = mid;
+            else hi = mid;
+         }
+         if(sNc[w][lo] == 0)
+         {
+            node = sC[w][lo];
+            isA = adjacentNodes(t, node, D);
+            isX = !isA;
+         }
+         else
+         {
+            node = sC0[w][lo] + (q - sEx[w][lo]);
+            if(adjacentNodes(t, node, D)) isCol = true;
+            else if(hasT && t.s1[node] > t.s0[node])
+            {
+               const int ox = t.ix[node] - t.ix[D], oy = t.iy[node] - t.iy[D], oz = t.iz[node] - t.iz[D];
+               const int o = d_m2lIndex[offsetIndex(ox, oy, oz)];
+               if(o >= 0)
+               {
+                  vt[o] = node;
+                  nv++;
+               }
+               else atomicOr(err, ERR_LIST_V);
+            }
+         }
+      }
+      ncol = append(isCol, node, colD, COLCAP, ncol, ERR_LIST_COL);
+      na = append(isA, node, aD, ACAP, na, ERR_LIST_A);
+      nx = append(isX, node, xD, XCAP, nx, ERR_LIST_X);
+   }
+   // the parent's coarser adjacent leaves, after the colleagues' entries (as in kListsLevel)
+   const int naP = L.na[P];
+   for(int base = 0; base < naP; base += 32)
+   {
+      const int k = base + lane;
+      bool isA = false, isX = false;
+      int node = -1;
+      if(k < naP)
+      {
+         node = L.acoarse[int64_t(P) * ACAP + k];
+         isA = adjacentNodes(t, node, D);
+         isX = !isA;
+      }
+      na = append(isA, node, aD, ACAP, na, ERR_LIST_A);
+      nx = append(isX, node, xD, XCAP, nx, ERR_LIST_X);
+   }
+   for(int d = 16; d > 0; d >>= 1) nv += __shfl_xor_sync(0xffffffffu, nv, d);
+   if(lane == 0)
+   {
+      L.ncol[D] = min(ncol, COLCAP);
+      L.na[D] = min(na, ACAP);
+      L.nx[D] = min(nx, XCAP);
+      L.nv[D] = nv;
+   }
+}
+
 // Statistics of the finished tree: out[0] += leaves, out[1] += direct (target, source) pairs the near
 // field evaluates (targets of a leaf x points of its direct-list nodes, the self pairs included).
 __global__ void kNearCounts(Tree t, int nNodes, const int* __restrict__ off, const int* __restrict__ list,
@@ -1074,8 +1195,16 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    for(int level = 1; level < nLevels; level++)
    {
       int a = t.levelStart[level], b = t.levelStart[level + 1];
-      kListsLevel<<<(b - a + 127) / 128, 128, 0, st>>>(t, Ls, a, b, P.err);
-      FMM_TRY(launched(P, "kListsLevel", st));
+      if(P.listsWarp)
+      {
+         kListsLevelWarp<<<(b - a + LW_WARPS - 1) / LW_WARPS, 32 * LW_WARPS, 0, st>>>(t, Ls, a, b, P.err);
+         FMM_TRY(launched(P, "kListsLevelWarp", st));
+      }
+      else
+      {
+         kListsLevel<<<(b - a + 127) / 128, 128, 0, st>>>(t, Ls, a, b, P.err);
+         FMM_TRY(launched(P, "kListsLevel", st));
+      }
    }
    FMM_CHECK_LAUNCH();
    int nn = int(total);

@@ -15,16 +15,16 @@ pytestmark = pytest.mark.gpu
 KEYS = ("nodes", "leaves", "levels", "v_pairs", "p2p_pairs", "p2p_interactions")
 
 
-def _solve(persistent, build):
-    old = os.environ.get("FMM_TREE_PERSISTENT")
-    os.environ["FMM_TREE_PERSISTENT"] = "1" if persistent else "0"
+def _solve(persistent, build, var="FMM_TREE_PERSISTENT"):
+    old = os.environ.get(var)
+    os.environ[var] = "1" if persistent else "0"
     try:
         plan, load = build()
     finally:
         if old is None:
-            del os.environ["FMM_TREE_PERSISTENT"]
+            del os.environ[var]
         else:
-            os.environ["FMM_TREE_PERSISTENT"] = old
+            os.environ[var] = old
     out = []
     for _ in range(2):
         load(plan)   # new inputs: the next solve builds the forest again
@@ -65,3 +65,14 @@ def test_persistent_levels_equal_level_by_level(build):
         assert sp["levels"] > 3
         assert np.all(np.isfinite(Bp))
         assert np.array_equal(Bp, Bl)
+
+
+@pytest.mark.parametrize("build", [_single, _batch], ids=["fp64-single", "fp32-batch"])
+def test_warp_lists_equal_thread_lists(build):
+    """The interaction lists built with one warp per box (ballot appends in candidate order) equal the lists
+    built with one thread per box: the same statistics and bit-identical fields."""
+    per_thread = _solve(False, build, "FMM_LISTS_WARP")
+    per_warp = _solve(True, build, "FMM_LISTS_WARP")
+    for (Bw, sw), (Bt, st) in zip(per_warp, per_thread):
+        assert sw == st
+        assert np.array_equal(Bw, Bt)
