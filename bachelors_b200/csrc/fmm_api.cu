@@ -103,7 +103,7 @@ fmm_status Plan::init(const fmm_config& c)
    if(const char* e = getenv("FMM_TC_ASYNC")) tcAsyncArrive = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_PAIR")) tcPair = atoi(e) != 0;
    if(const char* e = getenv("FMM_TREE_PERSISTENT")) treePersistent = atoi(e) != 0;
-   if(const char* e = getenv("FMM_LISTS_WARP")) listsWarp = atoi(e) != 0;
+   if(const char* e = getenv("FMM_LISTS_WARP")) listsWarp = std::min(2, std::max(0, atoi(e)));
    if(const char* e = getenv("FMM_TC_KEEPTAIL")) tcKeepTail = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_PROF")) tcProf = atoi(e) != 0;
    if(const char* e = getenv("FMM_TC_CUTOFF")) cfg.m2l_tc_degree_cutoff = atoi(e);

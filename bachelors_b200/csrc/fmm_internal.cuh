@@ -224,7 +224,8 @@ struct Plan
                                          // (-1: every term the degree cutoff keeps; -2: 10)
    int tcDrainMode = 3;                  // 0: vector atomics, 1: load-add-store, 2: running sums in TMEM + 1,
                                          // 3: as 2 with 32 more columns in the drain threads' registers
-   int listsWarp = 1;                    // interaction lists: one warp per node (kListsLevelWarp), 0: a thread
+   int listsWarp = 1;                    // interaction lists: 0 a thread per node (kListsLevel), 2 a warp per
+                                         // node (kListsLevelWarp), 1 a warp for single-coil plans
    bool tgtIsSrc = false;                // the targets are the sources (fmm_set_targets_to_sources since the
                                          // last set_sources / set_targets)
    int treePersistent = 1;               // every tree level in one cooperative launch (kBuildLevels)

@@ -1195,7 +1195,9 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    for(int level = 1; level < nLevels; level++)
    {
       int a = t.levelStart[level], b = t.levelStart[level + 1];
-      if(P.listsWarp)
+      // one warp per box pays where boxes have many candidates (a dense single coil: 11.1 -> 10.0 ms of tree
+      // phase at 2^24) and not where most have few (the 256 small coils of the batch: 11.6 -> 13.4 ms)
+      if(P.listsWarp == 2 || (P.listsWarp == 1 && K == 1))
       {
          kListsLevelWarp<<<(b - a + LW_WARPS - 1) / LW_WARPS, 32 * LW_WARPS, 0, st>>>(t, Ls, a, b, P.err);
          FMM_TRY(launched(P, "kListsLevelWarp", st));

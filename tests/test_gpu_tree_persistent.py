@@ -15,9 +15,9 @@ pytestmark = pytest.mark.gpu
 KEYS = ("nodes", "leaves", "levels", "v_pairs", "p2p_pairs", "p2p_interactions")
 
 
-def _solve(persistent, build, var="FMM_TREE_PERSISTENT"):
+def _solve(persistent, build, var="FMM_TREE_PERSISTENT", on="1"):
     old = os.environ.get(var)
-    os.environ[var] = "1" if persistent else "0"
+    os.environ[var] = on if persistent else "0"
     try:
         plan, load = build()
     finally:
@@ -72,7 +72,7 @@ def test_warp_lists_equal_thread_lists(build):
     """The interaction lists built with one warp per box (ballot appends in candidate order) equal the lists
     built with one thread per box: the same statistics and bit-identical fields."""
     per_thread = _solve(False, build, "FMM_LISTS_WARP")
-    per_warp = _solve(True, build, "FMM_LISTS_WARP")
+    per_warp = _solve(True, build, "FMM_LISTS_WARP", on="2")   # (2: a warp per box for batches as well)
     for (Bw, sw), (Bt, st) in zip(per_warp, per_thread):
         assert sw == st
         assert np.array_equal(Bw, Bt)
