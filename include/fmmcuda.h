@@ -122,7 +122,10 @@ fmm_status fmm_set_bem_sources(fmm_plan* plan, const void* xyz, const void* w, c
 fmm_status fmm_set_targets(fmm_plan* plan, const void* xyz, int64_t m, int on_device, void* stream);
 /* Targets = the current source points, in source input order (no counterpart in the reference, whose
  * FastMultipoleSolver always takes its own `points`): a device-side copy on `stream`, so a caller
- * evaluating B at its own quadrature points moves them to the GPU once. */
+ * evaluating B at its own quadrature points moves them to the GPU once. A single-coil plan's tree build
+ * then reuses the sources' sorted order for the targets (one sort instead of two). The targets stay
+ * these points until the next fmm_set_targets or fmm_set_targets_to_sources, also when new sources
+ * are set. */
 fmm_status fmm_set_targets_to_sources(fmm_plan* plan, void* stream);
 
 /* The reference's phases, for drop-in use of its call sequence
