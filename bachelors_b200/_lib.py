@@ -18,7 +18,7 @@ FMM_TREECODE_REFERENCE_NEAR, FMM_TREECODE_FD_CURL = 1, 2
 
 # Every extern "C" symbol include/fmmcuda.h declares.
 EXPORTS = [
-    "fmm_default_config", "fmm_plan_create", "fmm_plan_destroy", "fmm_set_sources", "fmm_set_bem_sources",
+    "fmm_default_config", "fmm_plan_create", "fmm_plan_destroy", "fmm_set_sources", "fmm_set_sources_async", "fmm_set_bem_sources",
     "fmm_set_targets",
     "fmm_set_targets_to_sources",
     "fmm_build_tree", "fmm_upward", "fmm_downward", "fmm_evaluate", "fmm_solve", "fmm_direct",
@@ -84,6 +84,7 @@ def load():
         "fmm_plan_create": (ctypes.c_int, [ctypes.POINTER(FmmConfig), ctypes.POINTER(vp)]),
         "fmm_plan_destroy": (ctypes.c_int, [vp]),
         "fmm_set_sources": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.c_int, vp]),
+        "fmm_set_sources_async": (ctypes.c_int, [vp, vp, vp, vp, i64, vp]),
         "fmm_set_bem_sources": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, ctypes.c_int, vp]),
         "fmm_set_targets": (ctypes.c_int, [vp, vp, i64, ctypes.c_int, vp]),
         "fmm_set_targets_to_sources": (ctypes.c_int, [vp, vp]),

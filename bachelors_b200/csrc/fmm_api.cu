@@ -135,6 +135,18 @@ fmm_status Plan::init(const fmm_config& c)
 void Plan::release()
 {
    dropGraph();
+   if(copyStream)
+   {
+      // copies of fmm_set_sources_async still in flight write into buffers freed below
+      cudaStreamSynchronize(copyStream);
+      cudaStreamDestroy(copyStream);
+      cudaEventDestroy(evPrev);
+      cudaEventDestroy(evPos);
+      cudaEventDestroy(evInputs);
+      copyStream = nullptr;
+      evPrev = evPos = evInputs = nullptr;
+   }
+   inputsAsync = false;
    if(adj)
    {
       adj->release();
@@ -326,11 +338,66 @@ fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
    size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_TRY(P.waitSourceInputs(st));   // copies of an earlier fmm_set_sources_async into the same buffers
    FMM_TRY(copyIn(P.srcXYZb, xyz, es * 3 * n, on_device, st, &P.srcXYZ));
    FMM_TRY(copyIn(P.srcWb, w, es * n, on_device, st, &P.srcW));
    P.hasJ = J != nullptr;
    if(P.hasJ) FMM_TRY(copyIn(P.srcJb, J, es * 3 * n, on_device, st, &P.srcJ));
    if(!on_device) FMM_CUDA(cudaStreamSynchronize(st));
+   P.inputsAsync = false;
+   P.bem = false;
+   P.n = n;
+   P.tgtIsSrc = false;
+   P.treeReady = P.upReady = P.downReady = false;
+   P.dropGraph();
+   return FMM_OK;
+}
+
+fmm_status fmm_set_sources_async(fmm_plan* plan, const void* xyz, const void* w, const void* J, int64_t n, void* stream)
+{
+   if(!plan) return setError(FMM_E_INVALID, "null plan");
+   if(n < 0 || n > (int64_t(1) << 31) - 1) return setError(FMM_E_INVALID, "source count %lld out of range", (long long)n);
+   if(n > 0 && (!xyz || !w)) return setError(FMM_E_INVALID, "null source coordinates or weights");
+   Plan& P = plan->P;
+   DeviceGuard g(P.cfg.device);
+   cudaStream_t st = (cudaStream_t)stream;
+   // page-locked host memory only: a pageable buffer would be copied by the driver before the call returns
+   const void* ptrs[3] = {xyz, w, J};
+   for(const void* p : ptrs)
+   {
+      if(!p || n == 0) continue;
+      cudaPointerAttributes a;
+      const cudaError_t e = cudaPointerGetAttributes(&a, p);
+      if(e != cudaSuccess || a.type != cudaMemoryTypeHost)
+      {
+         cudaGetLastError();
+         return setError(FMM_E_INVALID, "fmm_set_sources_async: the inputs must be page-locked host memory");
+      }
+   }
+   const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
+   FMM_TRY(P.srcXYZb.reserve(es * 3 * n));
+   FMM_TRY(P.srcWb.reserve(es * n));
+   P.hasJ = J != nullptr;
+   if(P.hasJ) FMM_TRY(P.srcJb.reserve(es * 3 * n));
+   if(!P.copyStream)
+   {
+      FMM_CUDA(cudaStreamCreateWithFlags(&P.copyStream, cudaStreamNonBlocking));
+      FMM_CUDA(cudaEventCreateWithFlags(&P.evPrev, cudaEventDisableTiming));
+      FMM_CUDA(cudaEventCreateWithFlags(&P.evPos, cudaEventDisableTiming));
+      FMM_CUDA(cudaEventCreateWithFlags(&P.evInputs, cudaEventDisableTiming));
+   }
+   // the copies follow the work queued on `stream` so far (it may still read the previous sources)
+   FMM_CUDA(cudaEventRecord(P.evPrev, st));
+   FMM_CUDA(cudaStreamWaitEvent(P.copyStream, P.evPrev, 0));
+   if(n) FMM_CUDA(cudaMemcpyAsync(P.srcXYZb.ptr, xyz, es * 3 * n, cudaMemcpyHostToDevice, P.copyStream));
+   FMM_CUDA(cudaEventRecord(P.evPos, P.copyStream));
+   if(n) FMM_CUDA(cudaMemcpyAsync(P.srcWb.ptr, w, es * n, cudaMemcpyHostToDevice, P.copyStream));
+   if(n && P.hasJ) FMM_CUDA(cudaMemcpyAsync(P.srcJb.ptr, J, es * 3 * n, cudaMemcpyHostToDevice, P.copyStream));
+   FMM_CUDA(cudaEventRecord(P.evInputs, P.copyStream));
+   P.srcXYZ = P.srcXYZb.ptr;
+   P.srcW = P.srcWb.ptr;
+   if(P.hasJ) P.srcJ = P.srcJb.ptr;
+   P.inputsAsync = true;
    P.bem = false;
    P.n = n;
    P.tgtIsSrc = false;
@@ -349,6 +416,7 @@ fmm_status fmm_set_bem_sources(fmm_plan* plan, const void* xyz, const void* w, c
    if(P.batch) return setError(FMM_E_INVALID, "fmm_set_bem_sources: not available on a batched plan");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
    FMM_TRY(copyIn(P.srcXYZb, xyz, es * 3 * n, on_device, st, &P.srcXYZ));
    FMM_TRY(copyIn(P.srcWb, w, es * n, on_device, st, &P.srcW));
@@ -385,6 +453,7 @@ fmm_status fmm_set_bem_sources(fmm_plan* plan, const void* xyz, const void* w, c
       if(s == FMM_OK && e != cudaSuccess) s = setError(FMM_E_CUDA, "fmm_set_bem_sources: %s", cudaGetErrorString(e));
    }
    stage.release();
+   P.inputsAsync = false;
    P.treeReady = P.upReady = P.downReady = false;
    P.dropGraph();
    return s;
@@ -415,6 +484,7 @@ fmm_status fmm_set_targets_to_sources(fmm_plan* plan, void* stream)
    if(P.n > 0 && !P.srcXYZ) return setError(FMM_E_INVALID, "fmm_set_targets_to_sources: no sources set");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourcePoints(st));   // fmm_set_sources_async copies in flight
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
    const size_t bytes = es * 3 * size_t(P.n);
    FMM_TRY(P.tgtXYZb.reserve(std::max<size_t>(bytes, 16)));
@@ -532,6 +602,7 @@ fmm_status fmm_direct(fmm_plan* plan, double current, int want, void* out_B, voi
       return setError(FMM_E_INVALID, "a plan with BEM sources sums the BEM integral into out_A (want = 2)");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    if(!P.treeReady) FMM_TRY(fmm_build_tree(plan, stream));
    size_t es = P.fp64 ? sizeof(double) : sizeof(float);
    size_t bytes = es * 3 * std::max<int64_t>(P.m, 1);
@@ -551,6 +622,7 @@ fmm_status fmm_direct_fp64_subset(fmm_plan* plan, double current, const double* 
       return setError(FMM_E_INVALID, "fmm_direct_fp64_subset: explicit targets belong to no coil of a batched plan");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = 0;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    if(!P.treeReady) FMM_TRY(fmm_build_tree(plan, nullptr));
    DevBuf t, o;
    FMM_TRY(t.reserve(sizeof(double) * 3 * std::max<int64_t>(k, 1)));
@@ -579,6 +651,7 @@ fmm_status fmm_adjoint(fmm_plan* plan, double current, const void* dL_dB, void* 
    if(!dL_dB || (!dL_dJ && !dL_dx)) return setError(FMM_E_INVALID, "fmm_adjoint: null argument");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    if(!P.adj)
    {
       fmm_config c = P.cfg;
@@ -642,6 +715,7 @@ fmm_status fmm_treecode(fmm_plan* plan, double current, int want, const void* pt
    if(m == 0) return FMM_OK;
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
    const size_t bytes = es * 3 * size_t(m);
    const void* dPts = pts;
@@ -676,6 +750,7 @@ fmm_status fmm_adjoint_direct(fmm_plan* plan, double current, const void* dL_dB,
    if(P.bem) return setError(FMM_E_INVALID, "fmm_adjoint_direct: not available for BEM sources");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
    const void* gDev = dL_dB;
    void* dJ = dL_dJ;
@@ -737,6 +812,7 @@ fmm_status fmm_autotune(fmm_plan* plan, fmm_tuning* out, void* stream)
    if(!P.downReady) return setError(FMM_E_INVALID, "fmm_autotune: run fmm_solve first (the tuner times the plan's data)");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    P.dropGraph();
    FMM_TRY(pipeBegin(P, st));
    cudaEvent_t e0, e1;
@@ -892,6 +968,7 @@ fmm_status fmm_update_sources(fmm_plan* plan, const void* w, const void* J, int 
       return setError(FMM_E_INVALID, "fmm_update_sources: J must be given exactly when the sources were set with J");
    DeviceGuard g(P.cfg.device);
    cudaStream_t st = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(st));   // fmm_set_sources_async copies in flight
    const size_t es = P.fp64 ? sizeof(double) : sizeof(float);
    if(P.n)
    {
@@ -921,6 +998,7 @@ fmm_status fmm_graph_capture(fmm_plan* plan, int want, void* stream)
    FMM_TRY(P.outA.reserve(es * 3 * std::max<int64_t>(P.m, 1)));
    // warm the lazily built state (operator image, buffers) eagerly, then capture on a private stream
    cudaStream_t user = (cudaStream_t)stream;
+   FMM_TRY(P.waitSourceInputs(user));   // fmm_set_sources_async copies in flight
    FMM_CUDA(cudaStreamSynchronize(user));
    cudaStream_t cs = nullptr;
    FMM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));

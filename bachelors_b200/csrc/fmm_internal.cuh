@@ -270,6 +270,22 @@ struct Plan
    DevBuf tcPts, tcOut;                  // fmm_treecode: staging of host query points and results
    bool adjointDone = false;
 
+   // fmm_set_sources_async: the host inputs cross the bus on copyStream while the solve runs; the
+   // source points first (evPos), then weights and current directions (evInputs). Work that reads them
+   // waits on the events (a wait on a completed event costs nothing), so the tree build starts once the
+   // points are in and the strengths are gathered at its end.
+   cudaStream_t copyStream = nullptr;
+   cudaEvent_t evPrev = nullptr, evPos = nullptr, evInputs = nullptr;
+   bool inputsAsync = false;
+   fmm_status waitSourcePoints(cudaStream_t st) { return waitCopy(st, evPos); }
+   fmm_status waitSourceInputs(cudaStream_t st) { return waitCopy(st, evInputs); }
+   fmm_status waitCopy(cudaStream_t st, cudaEvent_t ev)
+   {
+      const cudaError_t e = inputsAsync ? cudaStreamWaitEvent(st, ev, 0) : cudaSuccess;
+      if(e != cudaSuccess) return setError(FMM_E_CUDA, "waiting for the source copies: %s", cudaGetErrorString(e));
+      return FMM_OK;
+   }
+
    fmm_status init(const fmm_config& c);
    void release();
    fmm_status ensureNodes(int64_t cap, cudaStream_t st = 0);

@@ -185,8 +185,10 @@ __global__ void kGatherSources(const T* __restrict__ xyz, const T* __restrict__ 
       else { jx = T(0); jy = T(0); }
       jz = T(0);
    }
+   // (pos or q null: that half only, for strengths that arrive after the points)
+   if(pos) pos[i] = {x, y, z, T(0)};
+   if(!q) return;
    T ww = w[s];
-   pos[i] = {x, y, z, T(0)};
    // the fourth lane carries w sigma for BEM sources (fmm_bem.cu), zero otherwise
    q[i] = {ww * jx, ww * jy, ww * jz, sigma ? ww * sigma[s] : T(0)};
 }
@@ -1021,6 +1023,7 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    P.coilBits = 0;
    while((int64_t(1) << P.coilBits) < K) P.coilBits++;
    P.maxLevel = std::min(MAXLEVEL, (63 - P.coilBits) / 3);
+   FMM_TRY(P.waitSourcePoints(st));   // points copied by fmm_set_sources_async
    FMM_TRY(P.segb.reserve(sizeof(int) * 2 * (K + 1)));
    int* dSrcOff = (int*)P.segb.ptr;
    int* dTgtOff = dSrcOff + K + 1;
@@ -1099,10 +1102,11 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
    FMM_TRY(P.tPos.reserve(sizeof(V4) * std::max<int64_t>(m, 1)));
    if(n)
    {
+      // strengths still crossing the bus (fmm_set_sources_async): gathered at the end of the build
       kGatherSources<T><<<(n + threads - 1) / threads, threads, 0, st>>>(
          (const T*)P.srcXYZ, (const T*)P.srcW, (const T*)(P.hasJ ? P.srcJ : nullptr),
          (const T*)(P.bem ? P.srcSigma : nullptr), si, n, (V4*)P.sPos.ptr,
-         (V4*)P.sQ.ptr);
+         P.inputsAsync ? nullptr : (V4*)P.sQ.ptr);
       FMM_TRY(launched(P, "kGatherSources", st));
    }
    if(m && same)
@@ -1362,6 +1366,16 @@ fmm_status buildTreeT(Plan& P, cudaStream_t st)
       P.l2lStart.assign(8 * nLevels + 1, 0);
       FMM_CUDA(cudaMemcpyAsync(P.l2lStart.data(), P.scratch.ptr, sizeof(int) * (8 * nLevels + 1), cudaMemcpyDeviceToHost, st));
       FMM_CUDA(cudaStreamSynchronize(st));
+      FMM_CHECK_LAUNCH();
+   }
+   if(P.inputsAsync && n)
+   {
+      typedef typename Vec4<T>::type V4;
+      FMM_TRY(P.waitSourceInputs(st));
+      kGatherSources<T><<<(n + threads - 1) / threads, threads, 0, st>>>(
+         (const T*)P.srcXYZ, (const T*)P.srcW, (const T*)(P.hasJ ? P.srcJ : nullptr), nullptr,
+         (const int*)P.sIdx.ptr, n, nullptr, (V4*)P.sQ.ptr);
+      FMM_TRY(launched(P, "kGatherSources", st));
       FMM_CHECK_LAUNCH();
    }
    return FMM_OK;

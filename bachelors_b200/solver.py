@@ -138,15 +138,27 @@ class Plan:
             return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         return ctypes.c_void_p(0)
 
-    def set_sources(self, xyz, w, J=None):
+    def set_sources(self, xyz, w, J=None, asynchronous=False):
+        """Source points, weights and current directions (J None: the azimuthal direction).
+
+        asynchronous=True (host arrays in page-locked memory, e.g. from torch's pin_memory(), of the plan's
+        element type): fmm_set_sources_async, which returns before the copies end and lets the next tree
+        build run while the weights and directions cross the bus. The arrays must stay unchanged until the
+        next solve has returned; the plan keeps references to them until then."""
         x = _Buffer(xyz, self.np_dtype, self.torch_dtype, (3,))
         wb = _Buffer(w, self.np_dtype, self.torch_dtype, ())
         jb = _Buffer(J, self.np_dtype, self.torch_dtype, (3,)) if J is not None else None
+        if asynchronous and x.device:
+            raise ValueError("asynchronous=True takes host arrays; device inputs are copied on the stream anyway")
         self.device_mode = x.device
         self.n = x.n
-        _lib.check(self.lib.fmm_set_sources(self.handle, ctypes.c_void_p(x.ptr), ctypes.c_void_p(wb.ptr),
-                                            ctypes.c_void_p(jb.ptr) if jb else None, x.n, int(x.device),
-                                            self._stream()))
+        if asynchronous:
+            _lib.check(self.lib.fmm_set_sources_async(self.handle, ctypes.c_void_p(x.ptr), ctypes.c_void_p(wb.ptr),
+                                                      ctypes.c_void_p(jb.ptr) if jb else None, x.n, self._stream()))
+        else:
+            _lib.check(self.lib.fmm_set_sources(self.handle, ctypes.c_void_p(x.ptr), ctypes.c_void_p(wb.ptr),
+                                                ctypes.c_void_p(jb.ptr) if jb else None, x.n, int(x.device),
+                                                self._stream()))
         self._keep = [x, wb, jb]
         self.generation += 1
 

@@ -105,6 +105,16 @@ fmm_status fmm_plan_destroy(fmm_plan* plan);
  * copied; the caller's buffers may be released after the call returns. */
 fmm_status fmm_set_sources(fmm_plan* plan, const void* xyz, const void* w, const void* J, int64_t n,
                            int on_device, void* stream);
+/* fmm_set_sources for page-locked host buffers (cudaHostAlloc / cudaHostRegister; anything else is
+ * FMM_E_INVALID), without waiting for the copies: the points, then the weights and directions, cross the
+ * bus on a copy stream of the plan, after the work queued on `stream` so far. The next tree build
+ * (fmm_build_tree / fmm_solve) starts once the points are in and takes the strengths at its end, so
+ * their copy runs under the build; every other call that reads the sources waits for the copies on
+ * its stream. The caller keeps the buffers alive and unchanged until the next fmm_solve (or
+ * fmm_build_tree) on this plan has returned. No counterpart in the reference, whose sources live in
+ * host memory. */
+fmm_status fmm_set_sources_async(fmm_plan* plan, const void* xyz, const void* w, const void* J, int64_t n,
+                                 void* stream);
 /* BEM sources (the reference's Problem::BEM, FMM/FMMGPU/multipole_solver_enums.hpp:26-30, BEMQuadrature
  * bem_quadrature.hpp): points xyz[3n], weights w[n], field values B[3n] and surface normals normal[3n]. The
  * plan then computes the reference's BEM integral (math::calcBEMIntegral, integration.cpp:191-215)
