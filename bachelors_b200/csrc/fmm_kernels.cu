@@ -335,6 +335,16 @@ __device__ __forceinline__ void load4(const double* p, double* v)
    const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
    v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
 }
+__device__ __forceinline__ void load2(const float* p, float* v)
+{
+   const float2 x = *reinterpret_cast<const float2*>(p);
+   v[0] = x.x; v[1] = x.y;
+}
+__device__ __forceinline__ void load2(const double* p, double* v)
+{
+   const double2 x = *reinterpret_cast<const double2*>(p);
+   v[0] = x.x; v[1] = x.y;
+}
 
 __device__ __forceinline__ int degreeOf(int k)
 {
@@ -814,7 +824,9 @@ __global__ void __launch_bounds__(256, 2) kL2LChild(Tree t, const int* __restric
    const int o = blockIdx.z;
    const int s0 = seg.start[o] + blockIdx.x * TG_P, s1 = seg.start[o + 1];
    if(s0 >= s1) return;
-   __shared__ __align__(16) T As[TG_K][TG_ROWS + 1];
+   // rows padded by two: the transposed stores meet two-way bank conflicts, and each thread reads its
+   // six rows as three aligned pairs
+   __shared__ __align__(16) T As[TG_K][TG_ROWS + 2];
    __shared__ __align__(16) T Bs[TG_K][TG_N];
    __shared__ int childOf[TG_P], parentOf[TG_P];
    const int tid = threadIdx.x;
@@ -875,7 +887,7 @@ __global__ void __launch_bounds__(256, 2) kL2LChild(Tree t, const int* __restric
       {
          T a[6], b[4];
 #pragma unroll
-         for(int i = 0; i < 6; i++) a[i] = As[kk][tr * 6 + i];
+         for(int i = 0; i < 6; i += 2) load2(&As[kk][tr * 6 + i], a + i);
          load4(&Bs[kk][tc * 4], b);
 #pragma unroll
          for(int i = 0; i < 6; i++)
