@@ -684,7 +684,9 @@ def main():
         e2e_ms = max_over_ranks(e2e_ms, world)
         line["e2e"] = {"value": world * n / (e2e_ms / 1000.0), "unit": UNIT,
                        "h2d_bytes_per_step": int(xyz.nbytes + w.nbytes + J.nbytes),
-                       "d2h_bytes_per_step": int(Bh2.nbytes), "ms_per_step": e2e_ms}
+                       "d2h_bytes_per_step": int(Bh2.nbytes), "ms_per_step": e2e_ms,
+                       "note": "page-locked inputs through fmm_set_sources_async: the points cross first, the "
+                               "weights and directions under the tree build; B back into page-locked memory"}
         s.plan.close()
 
     extras = [e for e in args.extra.split(",") if e]
